@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""Benchmark: scattering events/s of the electron-transport hot path.
+
+Workload (the reference's line-space grating SEM scan): Si-like lines 32 nm
+wide at 64 nm pitch, 50 nm tall, 2 um long on a substrate (5,136 triangles);
+256 x 256 pixels at 1 nm, 100 primaries per pixel at 500 eV (6,553,600
+primaries), Gaussian spot sigma 1 nm with 0.5 deg divergence; synthetic
+Si-like Kieft tables.  One step = one pass of the transport over the whole
+scan (every primary and its full secondary cascade).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl nbx|reference]
+
+Under torchrun each rank simulates its own 256 x 256 scan (independent pixel
+rows, own seed): replicas, weak scaling, no data-path collective.  Rank 0
+prints one JSON line.  value = events/s over all ranks with the primaries
+already resident in HBM (device time of nbx_run, CUDA events on the library's
+stream, max over ranks); e2e = the same through the C ABI from pinned host
+buffers (push + run + per-pixel yields read back), wall clock, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "scattering events/s & SE-yield FOM 1/(σ²t): learned-RR vs plain, 1×B200 vs CPU"
+NX = NY = 256
+PER_PIXEL = 100
+ENERGY = 500.0
+WORKLOAD = "grating 256x256 px x 100 primaries @ 500 eV (6,553,600 primaries), 5,136 triangles, Si-like Kieft tables"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def init_dist(world):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def allreduce_max(dist, x):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(dist, x):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def make_workload(tmp, rank=0, rows=None):
+    from nebula_b200 import formats, generators as g
+    mat = g.make_material(os.path.join(tmp, "si.mat"))
+    tris = g.grating_geometry()
+    tri_path = os.path.join(tmp, "grating.tri")
+    formats.write_tri(tri_path, tris)
+    recs = g.scan_beam(NX, NY, PER_PIXEL, ENERGY, seed=1000 + rank, rows=rows)
+    return mat, tris, tri_path, recs
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.TemporaryFile(mode="w+")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.out.seek(0)
+        rows = [r for r in csv.reader(io.StringIO(self.out.read())) if len(r) >= 9]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes_per_event(tris, mat_path, recs, seed):
+    """Section-8(d) algorithmic bytes per event, counted by the instrumented
+    CPU restatement on a fixed sample of the workload."""
+    import oracle
+    pg = oracle.PortGeometry(tris)
+    rm = oracle.RefMaterial(mat_path)
+    pms, arr = oracle.port_materials([rm])
+    sample = recs[:: max(1, len(recs) // 2000)][:2000]
+    prim = np.zeros((len(sample), 7), np.float32)
+    prim[:, 0:3] = sample["pos"]
+    prim[:, 3:6] = sample["dir"]
+    prim[:, 6] = sample["E"]
+    c, _, _, _, gc = oracle.port_run(pg, arr, prim, np.arange(len(sample), dtype=np.uint32), seed,
+                                     max_energy=rm.max_energy)
+    ev = c["n_elastic"] + c["n_inelastic"] + c["n_boundary"]
+    b_state = 88.0
+    b_tables = 16.0 + (16.0 * c["n_elastic"] + 20.0 * c["n_inelastic"] + 52.0 * c["n_boundary"]) / ev
+    b_geom = (4.0 * float(gc[0]) + 44.0 * float(gc[1])) / ev
+    return b_state + b_tables + b_geom, {"state": b_state, "tables": round(b_tables, 2), "geom": round(b_geom, 2),
+                                         "octree_words_per_event": round(float(gc[0]) / ev, 2),
+                                         "triangles_per_event": round(float(gc[1]) / ev, 3),
+                                         "sample_primaries": len(sample), "sample_events": ev}
+
+
+def cpu_baseline(tri_path, mat_path, recs, tmp, rows=16):
+    """The reference's own CPU path (oracle/_ref, cpu_mt_main-style driver) on
+    the first `rows` pixel rows of the scan, all host cores."""
+    import oracle
+    from nebula_b200 import formats
+    if not oracle.have_ref():
+        return None
+    sub = recs[recs["py"] < rows]
+    pri = os.path.join(tmp, "cpu_sample.pri")
+    formats.write_pri(pri, sub)
+    cores = os.cpu_count() or 1
+    _, st, secs = oracle.ref_run(tri_path, pri, [mat_path], threads=cores, count_events=True)
+    ev = st["n_intersect"] + st["n_elastic"] + st["n_inelastic"]
+    return {"value": ev / secs, "unit": "events/s", "cores": cores, "kind": "reference",
+            "sample": "%d pixel rows x 256 px x 100 primaries = %d primaries (%d events) in %.2f s"
+                      % (rows, len(sub), ev, secs),
+            "primaries_per_s": st["n_primaries"] / secs}
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    import oracle
+    with tempfile.TemporaryDirectory() as tmp:
+        if not oracle.have_ref():
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libnbref.so not built"}))
+            return 0
+        from nebula_b200 import formats
+        mat, tris, tri_path, recs = make_workload(tmp)
+        rows = 4
+        sub = recs[recs["py"] < rows]
+        pri = os.path.join(tmp, "ref_step.pri")
+        formats.write_pri(pri, sub)
+        cores = os.cpu_count() or 1
+        total_ev, total_s, total_p = 0, 0.0, 0
+        for i in range(args.warmup + args.steps):
+            _, st, secs = oracle.ref_run(tri_path, pri, [mat], seed=0x78C7E39B + i, threads=cores, count_events=True)
+            if i >= args.warmup:
+                total_ev += st["n_intersect"] + st["n_elastic"] + st["n_inelastic"]
+                total_s += secs
+                total_p += st["n_primaries"]
+        v = total_ev / total_s
+        line = {"metric": METRIC, "value": v, "unit": "events/s", "impl": "reference", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total_s / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "primaries_per_s": total_p / total_s,
+                "config": {"workload": WORKLOAD, "step_sample": "%d pixel rows (%d primaries) per step" % (rows, len(sub))},
+                "cpu_baseline": {"value": v, "unit": "events/s", "cores": cores, "kind": "reference",
+                                 "sample": "%d primaries per step, %d steps" % (len(sub), args.steps)},
+                "e2e": {"value": v, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="nbx", choices=["nbx", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    rank, world, local = dist_env()
+    dist = init_dist(world)
+    import nebula_b200 as nb
+
+    tmp = tempfile.mkdtemp(prefix="nbx_bench_")
+    mat, tris, tri_path, recs = make_workload(tmp, rank)
+    ctx = nb.setup(tris, [mat], device=local, seed=0x78C7E39B + rank)
+    n = len(recs)
+    prim = np.zeros((n, 7), np.float32)
+    prim[:, 0:3] = recs["pos"]
+    prim[:, 3:6] = recs["dir"]
+    prim[:, 6] = recs["E"]
+    tags = np.arange(n, dtype=np.uint32)
+    pixel_of_tag = (recs["py"].astype(np.uint32) * NX + recs["px"].astype(np.uint32))
+    try:
+        import torch
+        pin_p = torch.empty((n, 7), dtype=torch.float32, pin_memory=True).numpy()
+        pin_t = torch.empty((n,), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+        pinned = True
+    except Exception:
+        pin_p = np.empty((n, 7), np.float32)
+        pin_t = np.empty((n,), np.uint32)
+        pinned = False
+    pin_p[:] = prim
+    pin_t[:] = tags
+    ctx.set_tag_range(n)
+
+    def one_step():
+        ctx.push(pin_p, pin_t)
+        barrier(dist)
+        ctx.run()
+        return ctx.stats()
+
+    for _ in range(args.warmup):
+        ctx.reset_tallies()
+        one_step()
+
+    # Device-resident timing: primaries pushed before the timed run.
+    ctx.reset_tallies()
+    dev_ms, events, gens, launches = [], 0, 0, 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            s0 = ctx.stats()
+            ctx.push(pin_p, pin_t)
+            barrier(dist)
+            ctx.run()
+            s1 = ctx.stats()
+            dev_ms.append(s1["last_run_ms"])
+            events += (s1["events_elastic"] + s1["events_inelastic"] + s1["events_boundary"]) - \
+                      (s0["events_elastic"] + s0["events_inelastic"] + s0["events_boundary"])
+            gens = s1["generations"]
+            launches += s1["generations"]
+    clocks = clk.summary()
+    stats = ctx.stats()
+    t_dev = allreduce_max(dist, sum(dev_ms) / 1000.0)
+    ev_all = allreduce_sum(dist, events)
+    value = ev_all / t_dev
+    prim_all = allreduce_sum(dist, n * args.steps)
+
+    # SE-yield figure of merit from the timed steps' tallies: per-primary
+    # variance of the SE count, sigma^2 of the mean yield, t = device time.
+    se, bse = ctx.tag_counts(0, n)
+    mean_se = float(se.sum()) / (n * args.steps)
+    # Each tag was simulated `steps` times with independent streams, so the
+    # per-primary variance is Var(sum over the K repeats) / K.
+    var_primary = float(np.var(se.astype(np.float64))) / args.steps
+    sigma2 = var_primary / (n * args.steps) if var_primary > 0 else float("nan")
+    fom = 1.0 / (sigma2 * (sum(dev_ms) / 1000.0)) if sigma2 == sigma2 else None
+
+    # End-to-end through the C ABI from pinned host buffers.
+    e2e_s = []
+    for _ in range(args.steps):
+        barrier(dist)
+        t0 = time.perf_counter()
+        ctx.push(pin_p, pin_t)
+        ctx.run()
+        out = ctx.pixel_yields(pixel_of_tag, NX * NY)
+        e2e_s.append(time.perf_counter() - t0)
+    t_e2e = allreduce_max(dist, sum(e2e_s))
+    e2e_val = ev_all / t_e2e
+    h2d = n * 7 * 4 + n * 4
+    d2h = NX * NY * 5 * 8
+
+    line = None
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        b_event, b_parts = algorithmic_bytes_per_event(tris, mat, recs, 0x78C7E39B)
+        achieved = events * b_event / (sum(dev_ms) / 1000.0) / 1e9
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "transport_kernel_traffic.json")
+        if os.path.exists(tp):
+            with open(tp) as f:
+                traffic = json.load(f).get("dram_bytes_per_launch")
+        cpu = None if args.no_cpu_baseline else cpu_baseline(tri_path, mat, recs, tmp)
+        line = {
+            "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "parallelism": "replicas x%d" % world,
+                       "l2": "inputs larger than L2 (primary queue %.0f MB per step)" % (n * 48 / 1e6),
+                       "block_size": 256},
+            "primaries_per_s": prim_all / t_dev,
+            "events_per_primary": events / (n * args.steps),
+            "se_yield": mean_se, "bse_yield": float(bse.sum()) / (n * args.steps),
+            "fom_se_plain": fom,
+            "generations_per_step": gens,
+            "gpu_launches": int(launches),
+            "e2e": {"value": e2e_val, "unit": "events/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "pinned_host": pinned},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "bytes_per_event": round(b_event, 2), "bytes_breakdown": b_parts,
+                         "kernel": "transport_kernel"},
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

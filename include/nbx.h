@@ -1,0 +1,251 @@
+/* nbx: B200-native electron transport for Nebula-format SEM simulations.
+ *
+ * C ABI of the drop-in hot path.  Plain pointers and sizes only; no C++ types
+ * or exceptions cross it.  Every call returns NBX_OK (0) or a negative
+ * NBX_ERR_* code; nbx_last_error() gives a message for the last failing call
+ * on a context.  One context per GPU, driven by one host thread (the
+ * reference's worker_thread model, source/gpu_main.cu:77-218); a context is
+ * not re-entrant.
+ *
+ * Reference interfaces each group of entry points replaces (paths relative
+ * to the Nebula source tree):
+ *   nbx_load_tri          nbl::load_tri_file            io/load_tri_file.cpp:8-60
+ *   nbx_load_pri          nbl::load_pri_file            io/load_pri_file.cpp:134-246
+ *   nbx_octree_build      octree_builder::linearized_octree(octree_root(tris))
+ *                                                       geometry/octree/octree_builder.cpp:171-352
+ *   nbx_material_load     material<...>::create(hdf5_file) with kieft_elastic /
+ *                         kieft_inelastic loaders      core/material.inl:25-34,
+ *                                                       physics/kieft/elastic.h:120-166,
+ *                                                       physics/kieft/inelastic.h:212-327
+ *   nbx_create            gpu_driver constructor       drivers/gpu/gpu_driver.inl:51-89
+ *   nbx_set_geometry      octree<true>::create         geometry/octree.inl:280-313
+ *   nbx_add_material      gpu_material_manager::create core/gpu_material_manager.inl:5-26
+ *   nbx_push              gpu_driver::push             drivers/gpu/gpu_driver.h:58-80
+ *   nbx_run               the frame loop of do_iteration() calls
+ *                                                       gpu_main.cu:183-213, gpu_driver.inl:312-317
+ *   nbx_get_running_count gpu_driver::get_running_count drivers/gpu/gpu_driver.h:100-110
+ *   nbx_flush_detected    gpu_driver::flush_detected / flush_buffered
+ *                                                       drivers/gpu/gpu_driver.inl:259-306
+ *   nbx_ray_query         octree::propagate            geometry/octree.inl:33-192
+ *   nbx_table_query       table_1D::get, table_2D::get / get_rounddown
+ *                                                       common/util/table_1D.inl:66-80,
+ *                                                       common/util/table_2D.inl:74-104
+ */
+#ifndef NBX_H
+#define NBX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NBX_VERSION_MAJOR 1
+#define NBX_VERSION_MINOR 0
+#define NBX_VERSION_PATCH 2
+
+#define NBX_OK 0
+#define NBX_ERR_ARG (-1)      /* invalid argument */
+#define NBX_ERR_OOM (-2)      /* device or host allocation failed / over the HBM budget */
+#define NBX_ERR_CUDA (-3)     /* CUDA runtime error */
+#define NBX_ERR_TIMEOUT (-4)  /* a bounded device wait gave up */
+#define NBX_ERR_FORMAT (-5)   /* malformed .tri / .pri / .mat input */
+#define NBX_ERR_STATE (-6)    /* call out of order (e.g. run before set_geometry) */
+#define NBX_ERR_NODEV (-7)    /* no CUDA device / extension unavailable */
+#define NBX_ERR_CAPACITY (-8) /* a device queue overflowed */
+
+/* Special material indices (core/cpu_material_manager.h:82-91). */
+#define NBX_NOP (-128)
+#define NBX_TERMINATOR (-127)
+#define NBX_DETECTOR (-126)
+#define NBX_DETECTOR_LT50 (-125)
+#define NBX_DETECTOR_GE50 (-124)
+#define NBX_VACUUM (-123)
+#define NBX_MIRROR (-122)
+
+#define NBX_MAX_MATERIALS 16
+
+typedef struct nbx_ctx nbx_ctx;
+
+/* core/particle.h:5-10: position (nm), unnormalised direction, kinetic energy (eV). */
+typedef struct {
+    float pos[3];
+    float dir[3];
+    float E;
+} nbx_particle;
+
+/* The 36-byte .pri / detected-electron record (io/load_pri_file.cpp:134-246,
+ * cpu_mt_main.cpp:183-190). */
+typedef struct {
+    float pos[3];
+    float dir[3];
+    float E;
+    int32_t px, py;
+} nbx_record;
+
+/* core/triangle.h: r0, e1 = r1 - r0, e2 = r2 - r0, material_in, material_out. */
+typedef struct {
+    float r0[3];
+    float e1[3];
+    float e2[3];
+    int32_t mat_in, mat_out;
+} nbx_triangle;
+
+/* A detected electron and the tag of the primary that started its cascade. */
+typedef struct {
+    float pos[3];
+    float dir[3];
+    float E;
+    uint32_t tag;
+} nbx_detected;
+
+/* Linearized octree (geometry/octree/octree_builder.h:209-248). */
+typedef struct {
+    int32_t* octree_data;
+    uint64_t n_octree;
+    nbx_triangle* triangles;
+    uint64_t n_triangles;
+    float center[3];
+    float halfsize[3];
+    uint64_t duplicates_dropped;
+    int32_t max_depth;
+} nbx_octree;
+
+/* util::table_1D / table_2D: x_index = (x - x_min) * x_step; 2D data is
+ * row-major data[x * height + y]. */
+typedef struct {
+    int32_t n;
+    float x_min, x_step;
+    const float* data;
+} nbx_table1d;
+
+typedef struct {
+    int32_t width, height;
+    float x_min, x_step, y_min, y_step;
+    const float* data;
+} nbx_table2d;
+
+/* Kieft & Bosch material, tables already transformed as the reference
+ * loaders do (log IMFP, clamped cos-theta ICDF, log omega' ICDF, rebuilt
+ * ionisation table). */
+typedef struct {
+    float barrier;
+    nbx_table1d elastic_imfp;
+    nbx_table2d elastic_icdf;
+    float phonon_loss;
+    float recoil_const;
+    nbx_table1d inelastic_imfp;
+    nbx_table2d inelastic_icdf;
+    nbx_table2d ionisation;
+    float fermi;
+    float band_gap;
+    float max_energy; /* min over mechanisms of exp(IMFP axis maximum) */
+    char name[64];
+} nbx_material;
+
+typedef struct {
+    int32_t device;            /* CUDA device ordinal */
+    uint32_t seed;             /* random seed (gpu_main.cu --seed) */
+    float energy_threshold;    /* lowest energy w.r.t. vacuum (--energy-threshold) */
+    uint64_t capacity;         /* electrons per device queue; 0 = sized from free HBM */
+    int32_t record_detected;   /* keep per-electron detected records */
+    uint64_t record_capacity;  /* detected records held on the device; 0 = auto */
+    int32_t block_size;        /* threads per block of the transport kernel; 0 = tuned */
+    int32_t blocks_per_sm;     /* resident blocks per SM; 0 = occupancy maximum */
+} nbx_config;
+
+typedef struct {
+    uint64_t primaries_pushed;
+    uint64_t primaries_done;
+    uint64_t steps;           /* init passes, including those that terminate */
+    uint64_t events_elastic;
+    uint64_t events_inelastic;
+    uint64_t events_boundary;
+    uint64_t secondaries;
+    uint64_t detected;
+    uint64_t detected_se;     /* E < 50 eV */
+    uint64_t detected_bse;    /* E >= 50 eV */
+    uint64_t terminated;
+    uint64_t records_dropped;
+    uint64_t generations;     /* kernel launches of the last nbx_run */
+    uint64_t queue_overflow;
+    double last_run_ms;       /* device time of the last nbx_run (CUDA events) */
+    double last_kernel_ms;    /* device time of its transport launches only */
+} nbx_stats;
+
+/* ---- host-side helpers (no GPU needed) ---------------------------------- */
+int nbx_version(int* major, int* minor, int* patch);
+const char* nbx_error_string(int code);
+void nbx_free(void* p);
+int nbx_load_tri(const char* path, nbx_triangle** out, uint64_t* n);
+int nbx_load_pri(const char* path, nbx_record** out, uint64_t* n);
+int nbx_octree_build(const nbx_triangle* tris, uint64_t n, nbx_octree** out);
+void nbx_octree_free(nbx_octree* oct);
+int nbx_material_load(const char* path, nbx_material** out);
+void nbx_material_free(nbx_material* mat);
+int nbx_device_count(int* n);
+
+/* ---- device context ------------------------------------------------------ */
+void nbx_config_default(nbx_config* cfg);
+int nbx_create(nbx_ctx** ctx, const nbx_config* cfg);
+void nbx_destroy(nbx_ctx* ctx);
+const char* nbx_last_error(nbx_ctx* ctx);
+int nbx_set_geometry(nbx_ctx* ctx, const nbx_octree* oct);
+int nbx_add_material(nbx_ctx* ctx, const nbx_material* mat);
+/* Per-primary tallies are kept for tags [0, n_tags). */
+int nbx_set_tag_range(nbx_ctx* ctx, uint64_t n_tags);
+/* Queue primaries (host buffers).  *accepted <= n is how many fit. */
+int nbx_push(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n, uint64_t* accepted);
+/* Simulate every queued electron and all its secondaries to the end. */
+int nbx_run(nbx_ctx* ctx);
+int nbx_get_running_count(nbx_ctx* ctx, uint64_t* n);
+int nbx_get_stats(nbx_ctx* ctx, nbx_stats* out);
+/* Copy out (and remove) up to cap detected electrons. */
+int nbx_flush_detected(nbx_ctx* ctx, nbx_detected* out, uint64_t cap, uint64_t* n);
+/* Detections per primary tag below / at-or-above 50 eV. */
+int nbx_get_tag_counts(nbx_ctx* ctx, uint64_t first_tag, uint64_t n, uint32_t* se, uint32_t* bse);
+/* Per-pixel FP64 yields: pixel_of_tag maps tags to [0, n_pixels); out has
+ * n_pixels x 5 doubles {primaries, sum_se, sum_se^2, sum_bse, sum_bse^2}. */
+int nbx_pixel_yields(nbx_ctx* ctx, const uint32_t* pixel_of_tag, uint64_t n_tags, uint64_t n_pixels, double* out);
+/* Detected-energy histogram: n_bins bins of bin_width eV from 0. */
+int nbx_get_spectrum(nbx_ctx* ctx, uint64_t* counts, uint32_t n_bins, float* bin_width);
+int nbx_reset_tallies(nbx_ctx* ctx);
+
+/* ---- kernel-level queries (host buffers in/out) ------------------------- */
+/* Batched octree propagate; ignore_tri / out_tri index the linearized
+ * triangle array (-1: none). */
+int nbx_ray_query(nbx_ctx* ctx, const float* pos, const float* dir, const float* dist, const int32_t* ignore_tri,
+                  const int32_t* ignore_mat, uint64_t n, float* out_dist, int32_t* out_tri);
+/* table: 0 elastic log-IMFP, 1 elastic cos-theta ICDF, 2 inelastic log-IMFP,
+ *        3 inelastic log-omega' ICDF, 4 ionisation (rounddown). */
+int nbx_table_query(nbx_ctx* ctx, int32_t material, int32_t table, const float* x, const float* y, uint64_t n,
+                    float* out);
+/* Philox4x32-10 blocks: ctr n x 4, key n x 2, out n x 4. */
+int nbx_philox(nbx_ctx* ctx, const uint32_t* ctr, const uint32_t* key, uint64_t n, uint32_t* out);
+
+/* One transport step (init -> intersect -> scatter) for each electron, with
+ * the per-electron random streams of nbx_run.  Electrons are 56-byte
+ * nbx_electron records updated in place; status[i] receives 0 alive,
+ * 1 terminated, 2 detected; event[i] 0 none, 1 inelastic, 2 elastic,
+ * 3 boundary; secondaries[i] receives the created secondary when
+ * has_se[i] is 1. */
+typedef struct {
+    float pos[3];
+    float dir[3];
+    float E;
+    int32_t mat;
+    int32_t last_tri;
+    uint32_t tag;
+    uint64_t uid;
+    uint32_t step;
+    uint32_t pad;
+} nbx_electron;
+int nbx_step_query(nbx_ctx* ctx, nbx_electron* electrons, uint64_t n, int32_t* status, int32_t* event,
+                   nbx_electron* secondaries, int32_t* has_se);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NBX_H */

@@ -1,0 +1,370 @@
+"""nebula_b200: B200-native electron transport for Nebula-format SEM simulations.
+
+The product is the C-ABI library ``libnbx.so`` (``include/nbx.h``) with its
+sm_100a kernels, and the ``nebula_b200`` command-line program that mirrors
+Nebula's ``nebula_gpu``.  This module is a thin ctypes binding over that
+C ABI for Python callers (tests, benchmarks, notebooks).  It does not compute
+anything itself: when the library is missing, loading fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnbx.so")
+
+NBX_OK = 0
+ERRORS = {-1: "invalid argument", -2: "out of memory", -3: "CUDA error", -4: "device wait timed out",
+          -5: "malformed input", -6: "call out of order", -7: "no CUDA device", -8: "device queue overflow"}
+
+
+class NbxError(RuntimeError):
+    def __init__(self, code, msg=""):
+        super().__init__("%s (%d)%s" % (ERRORS.get(code, "error"), code, (": " + msg) if msg else ""))
+        self.code = code
+
+
+# ---------------------------------------------------------------------------
+# ctypes mirrors of include/nbx.h
+# ---------------------------------------------------------------------------
+class Triangle(C.Structure):
+    _fields_ = [("r0", C.c_float * 3), ("e1", C.c_float * 3), ("e2", C.c_float * 3), ("mat_in", C.c_int32),
+                ("mat_out", C.c_int32)]
+
+
+class Octree(C.Structure):
+    _fields_ = [("octree_data", C.POINTER(C.c_int32)), ("n_octree", C.c_uint64),
+                ("triangles", C.POINTER(Triangle)), ("n_triangles", C.c_uint64), ("center", C.c_float * 3),
+                ("halfsize", C.c_float * 3), ("duplicates_dropped", C.c_uint64), ("max_depth", C.c_int32)]
+
+
+class Table1D(C.Structure):
+    _fields_ = [("n", C.c_int32), ("x_min", C.c_float), ("x_step", C.c_float), ("data", C.POINTER(C.c_float))]
+
+
+class Table2D(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("x_min", C.c_float), ("x_step", C.c_float),
+                ("y_min", C.c_float), ("y_step", C.c_float), ("data", C.POINTER(C.c_float))]
+
+
+class Material(C.Structure):
+    _fields_ = [("barrier", C.c_float), ("elastic_imfp", Table1D), ("elastic_icdf", Table2D),
+                ("phonon_loss", C.c_float), ("recoil_const", C.c_float), ("inelastic_imfp", Table1D),
+                ("inelastic_icdf", Table2D), ("ionisation", Table2D), ("fermi", C.c_float),
+                ("band_gap", C.c_float), ("max_energy", C.c_float), ("name", C.c_char * 64)]
+
+
+class Config(C.Structure):
+    _fields_ = [("device", C.c_int32), ("seed", C.c_uint32), ("energy_threshold", C.c_float),
+                ("capacity", C.c_uint64), ("record_detected", C.c_int32), ("record_capacity", C.c_uint64),
+                ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in (
+        "primaries_pushed", "primaries_done", "steps", "events_elastic", "events_inelastic", "events_boundary",
+        "secondaries", "detected", "detected_se", "detected_bse", "terminated", "records_dropped", "generations",
+        "queue_overflow")] + [("last_run_ms", C.c_double), ("last_kernel_ms", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+DETECTED_DTYPE = np.dtype([("pos", "<f4", (3,)), ("dir", "<f4", (3,)), ("E", "<f4"), ("tag", "<u4")])
+ELECTRON_DTYPE = np.dtype([("pos", "<f4", (3,)), ("dir", "<f4", (3,)), ("E", "<f4"), ("mat", "<i4"),
+                           ("last_tri", "<i4"), ("tag", "<u4"), ("uid", "<u8"), ("step", "<u4"), ("pad", "<u4")])
+assert ELECTRON_DTYPE.itemsize == 56
+TABLE_IDS = {"el_imfp": 0, "el_icdf": 1, "in_imfp": 2, "in_icdf": 3, "ion": 4}
+
+_lib = None
+_vp = C.c_void_p
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_vp) if a is not None else None
+
+
+def lib():
+    """Load libnbx.so; raises ImportError if the extension has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("nebula_b200: %s is missing; run `python -m nebula_b200.build`" % LIB_PATH)
+    L = C.CDLL(LIB_PATH)
+    sig = {
+        "nbx_version": (C.c_int, [C.POINTER(C.c_int)] * 3),
+        "nbx_error_string": (C.c_char_p, [C.c_int]),
+        "nbx_free": (None, [_vp]),
+        "nbx_load_tri": (C.c_int, [C.c_char_p, C.POINTER(C.POINTER(Triangle)), C.POINTER(C.c_uint64)]),
+        "nbx_load_pri": (C.c_int, [C.c_char_p, C.POINTER(_vp), C.POINTER(C.c_uint64)]),
+        "nbx_octree_build": (C.c_int, [_vp, C.c_uint64, C.POINTER(C.POINTER(Octree))]),
+        "nbx_octree_free": (None, [C.POINTER(Octree)]),
+        "nbx_material_load": (C.c_int, [C.c_char_p, C.POINTER(C.POINTER(Material))]),
+        "nbx_material_free": (None, [C.POINTER(Material)]),
+        "nbx_device_count": (C.c_int, [C.POINTER(C.c_int)]),
+        "nbx_config_default": (None, [C.POINTER(Config)]),
+        "nbx_create": (C.c_int, [C.POINTER(_vp), C.POINTER(Config)]),
+        "nbx_destroy": (None, [_vp]),
+        "nbx_last_error": (C.c_char_p, [_vp]),
+        "nbx_set_geometry": (C.c_int, [_vp, C.POINTER(Octree)]),
+        "nbx_add_material": (C.c_int, [_vp, C.POINTER(Material)]),
+        "nbx_set_tag_range": (C.c_int, [_vp, C.c_uint64]),
+        "nbx_push": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.POINTER(C.c_uint64)]),
+        "nbx_run": (C.c_int, [_vp]),
+        "nbx_get_running_count": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
+        "nbx_get_stats": (C.c_int, [_vp, C.POINTER(Stats)]),
+        "nbx_flush_detected": (C.c_int, [_vp, _vp, C.c_uint64, C.POINTER(C.c_uint64)]),
+        "nbx_get_tag_counts": (C.c_int, [_vp, C.c_uint64, C.c_uint64, _vp, _vp]),
+        "nbx_pixel_yields": (C.c_int, [_vp, _vp, C.c_uint64, C.c_uint64, _vp]),
+        "nbx_get_spectrum": (C.c_int, [_vp, _vp, C.c_uint32, C.POINTER(C.c_float)]),
+        "nbx_reset_tallies": (C.c_int, [_vp]),
+        "nbx_ray_query": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_uint64, _vp, _vp]),
+        "nbx_table_query": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp, _vp, C.c_uint64, _vp]),
+        "nbx_philox": (C.c_int, [_vp, _vp, _vp, C.c_uint64, _vp]),
+        "nbx_step_query": (C.c_int, [_vp, _vp, C.c_uint64, _vp, _vp, _vp, _vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(rc, ctx=None):
+    if rc != NBX_OK:
+        msg = lib().nbx_last_error(ctx).decode() if ctx else ""
+        raise NbxError(rc, msg)
+
+
+def device_count():
+    n = C.c_int(0)
+    lib().nbx_device_count(C.byref(n))
+    return n.value
+
+
+# ---------------------------------------------------------------------------
+# Host-side helpers
+# ---------------------------------------------------------------------------
+def triangles_from_tri_array(tris) -> np.ndarray:
+    """TRI_DTYPE (vertices) -> nbx_triangle records (r0, e1 = r1 - r0, e2 = r2 - r0) in float32."""
+    v = np.asarray(tris["v"], np.float32)
+    out = np.zeros(len(tris), np.dtype([("r0", "<f4", 3), ("e1", "<f4", 3), ("e2", "<f4", 3),
+                                        ("mat_in", "<i4"), ("mat_out", "<i4")]))
+    out["r0"] = v[:, 0]
+    out["e1"] = (v[:, 1] - v[:, 0]).astype(np.float32)
+    out["e2"] = (v[:, 2] - v[:, 0]).astype(np.float32)
+    out["mat_in"] = tris["mat_in"]
+    out["mat_out"] = tris["mat_out"]
+    return out
+
+
+def load_tri(path) -> np.ndarray:
+    p = C.POINTER(Triangle)()
+    n = C.c_uint64()
+    _check(lib().nbx_load_tri(str(path).encode(), C.byref(p), C.byref(n)))
+    raw = C.string_at(p, 44 * n.value)
+    lib().nbx_free(C.cast(p, _vp))
+    return np.frombuffer(raw, triangles_from_tri_array(np.zeros(0, [("v", "<f4", (3, 3)), ("mat_in", "<i4"),
+                                                                        ("mat_out", "<i4")])).dtype).copy()
+
+
+class HostOctree:
+    """Linearized octree built by the library's host builder."""
+
+    def __init__(self, triangles: np.ndarray):
+        tri = np.ascontiguousarray(triangles)
+        assert tri.dtype.itemsize == 44
+        self._p = C.POINTER(Octree)()
+        _check(lib().nbx_octree_build(_ptr(tri), len(tri), C.byref(self._p)))
+        o = self._p.contents
+        self.octree_data = np.ctypeslib.as_array(o.octree_data, (o.n_octree,)).copy()
+        raw = C.string_at(o.triangles, 44 * o.n_triangles)
+        self.triangles = np.frombuffer(raw, tri.dtype).copy()
+        self.center = np.array(o.center, np.float32)
+        self.halfsize = np.array(o.halfsize, np.float32)
+        self.duplicates_dropped = o.duplicates_dropped
+        self.max_depth = o.max_depth
+
+    def __del__(self):
+        if getattr(self, "_p", None):
+            lib().nbx_octree_free(self._p)
+            self._p = None
+
+
+class HostMaterial:
+    """A .mat file loaded and transformed by the library's host loader."""
+
+    def __init__(self, path):
+        self._p = C.POINTER(Material)()
+        _check(lib().nbx_material_load(str(path).encode(), C.byref(self._p)))
+        m = self._p.contents
+        self.barrier, self.fermi, self.band_gap = m.barrier, m.fermi, m.band_gap
+        self.phonon_loss, self.recoil_const, self.max_energy = m.phonon_loss, m.recoil_const, m.max_energy
+        self.name = m.name.decode()
+
+        def t1(t):
+            return np.ctypeslib.as_array(t.data, (t.n,)).copy(), (t.x_min, t.x_step, 0.0, 0.0)
+
+        def t2(t):
+            a = np.ctypeslib.as_array(t.data, (t.width * t.height,)).copy().reshape(t.width, t.height)
+            return a, (t.x_min, t.x_step, t.y_min, t.y_step)
+
+        self.tables = {"el_imfp": t1(m.elastic_imfp), "in_imfp": t1(m.inelastic_imfp), "el_icdf": t2(m.elastic_icdf),
+                       "in_icdf": t2(m.inelastic_icdf), "ion": t2(m.ionisation)}
+
+    def __del__(self):
+        if getattr(self, "_p", None):
+            lib().nbx_material_free(self._p)
+            self._p = None
+
+
+# ---------------------------------------------------------------------------
+# Device context
+# ---------------------------------------------------------------------------
+class Context:
+    """One simulation context on one GPU (the reference's gpu_driver)."""
+
+    def __init__(self, device=0, seed=0x78C7E39B, energy_threshold=0.0, record_detected=False,
+                 record_capacity=0, capacity=0, block_size=0, blocks_per_sm=0):
+        L = lib()
+        cfg = Config()
+        L.nbx_config_default(C.byref(cfg))
+        cfg.device, cfg.seed, cfg.energy_threshold = device, seed, energy_threshold
+        cfg.record_detected, cfg.record_capacity, cfg.capacity = int(record_detected), record_capacity, capacity
+        cfg.block_size, cfg.blocks_per_sm = block_size, blocks_per_sm
+        self.h = _vp()
+        _check(L.nbx_create(C.byref(self.h), C.byref(cfg)))
+        self.L = L
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.nbx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _ck(self, rc):
+        _check(rc, self.h)
+
+    def set_geometry(self, octree: HostOctree):
+        self._ck(self.L.nbx_set_geometry(self.h, octree._p))
+        self.octree = octree
+
+    def add_material(self, mat: HostMaterial):
+        self._ck(self.L.nbx_add_material(self.h, mat._p))
+        self._keep.append(mat)
+
+    def set_tag_range(self, n):
+        self._ck(self.L.nbx_set_tag_range(self.h, n))
+
+    def push(self, particles: np.ndarray, tags: np.ndarray) -> int:
+        p = np.ascontiguousarray(particles, np.float32).reshape(-1, 7)
+        t = np.ascontiguousarray(tags, np.uint32)
+        acc = C.c_uint64()
+        self._ck(self.L.nbx_push(self.h, _ptr(p), _ptr(t), len(t), C.byref(acc)))
+        return acc.value
+
+    def push_records(self, recs: np.ndarray, first_tag=0) -> int:
+        """Push .pri records; tag i is the record's index (+first_tag)."""
+        p = np.zeros((len(recs), 7), np.float32)
+        p[:, 0:3] = recs["pos"]
+        p[:, 3:6] = recs["dir"]
+        p[:, 6] = recs["E"]
+        return self.push(p, np.arange(first_tag, first_tag + len(recs), dtype=np.uint32))
+
+    def run(self):
+        self._ck(self.L.nbx_run(self.h))
+
+    def stats(self) -> dict:
+        s = Stats()
+        self._ck(self.L.nbx_get_stats(self.h, C.byref(s)))
+        return s.as_dict()
+
+    def flush_detected(self, cap=None) -> np.ndarray:
+        st = self.stats()
+        cap = cap if cap is not None else int(st["detected"]) + 16
+        out = np.zeros(cap, DETECTED_DTYPE)
+        n = C.c_uint64()
+        self._ck(self.L.nbx_flush_detected(self.h, _ptr(out), cap, C.byref(n)))
+        return out[: n.value]
+
+    def tag_counts(self, first, n):
+        se = np.zeros(n, np.uint32)
+        bse = np.zeros(n, np.uint32)
+        self._ck(self.L.nbx_get_tag_counts(self.h, first, n, _ptr(se), _ptr(bse)))
+        return se, bse
+
+    def pixel_yields(self, pixel_of_tag: np.ndarray, n_pixels: int) -> np.ndarray:
+        m = np.ascontiguousarray(pixel_of_tag, np.uint32)
+        out = np.zeros((n_pixels, 5), np.float64)
+        self._ck(self.L.nbx_pixel_yields(self.h, _ptr(m), len(m), n_pixels, _ptr(out)))
+        return out
+
+    def spectrum(self, n_bins=20000):
+        out = np.zeros(n_bins, np.uint64)
+        w = C.c_float()
+        self._ck(self.L.nbx_get_spectrum(self.h, _ptr(out), n_bins, C.byref(w)))
+        return out, w.value
+
+    def reset_tallies(self):
+        self._ck(self.L.nbx_reset_tallies(self.h))
+
+    def ray_query(self, pos, dirs, dist, ignore_tri, ignore_mat):
+        pos = np.ascontiguousarray(pos, np.float32)
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        dist = np.ascontiguousarray(dist, np.float32)
+        it = np.ascontiguousarray(ignore_tri, np.int32)
+        im = np.ascontiguousarray(ignore_mat, np.int32)
+        n = len(dist)
+        od = np.zeros(n, np.float32)
+        ot = np.zeros(n, np.int32)
+        self._ck(self.L.nbx_ray_query(self.h, _ptr(pos), _ptr(dirs), _ptr(dist), _ptr(it), _ptr(im), n, _ptr(od),
+                                      _ptr(ot)))
+        return od, ot
+
+    def table_query(self, material, table, x, y=None):
+        x = np.ascontiguousarray(x, np.float32)
+        y = None if y is None else np.ascontiguousarray(y, np.float32)
+        out = np.zeros_like(x)
+        self._ck(self.L.nbx_table_query(self.h, material, TABLE_IDS.get(table, table), _ptr(x), _ptr(y), len(x),
+                                        _ptr(out)))
+        return out
+
+    def philox(self, ctr, key):
+        ctr = np.ascontiguousarray(ctr, np.uint32).reshape(-1, 4)
+        key = np.ascontiguousarray(key, np.uint32).reshape(-1, 2)
+        out = np.zeros_like(ctr)
+        self._ck(self.L.nbx_philox(self.h, _ptr(ctr), _ptr(key), len(ctr), _ptr(out)))
+        return out
+
+    def step_query(self, electrons: np.ndarray):
+        e = np.ascontiguousarray(electrons.copy(), ELECTRON_DTYPE)
+        n = len(e)
+        st = np.zeros(n, np.int32)
+        ev = np.zeros(n, np.int32)
+        se = np.zeros(n, ELECTRON_DTYPE)
+        hs = np.zeros(n, np.int32)
+        self._ck(self.L.nbx_step_query(self.h, _ptr(e), n, _ptr(st), _ptr(ev), _ptr(se), _ptr(hs)))
+        return e, st, ev, se, hs
+
+
+def setup(tri_path_or_array, mat_paths, **ctx_kwargs):
+    """Load geometry (.tri path or TRI_DTYPE array) and materials into a new Context."""
+    from . import formats
+    if isinstance(tri_path_or_array, (str, os.PathLike)):
+        tris = load_tri(tri_path_or_array)
+    else:
+        tris = triangles_from_tri_array(tri_path_or_array)
+    oct_ = HostOctree(tris)
+    ctx = Context(**ctx_kwargs)
+    ctx.set_geometry(oct_)
+    for p in mat_paths:
+        ctx.add_material(HostMaterial(p))
+    return ctx

@@ -1,0 +1,76 @@
+// Launch interface between the host runtime (nbx_api.cpp) and the CUDA
+// kernels (transport.cu).  Host-compilable; no device code here.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dev_types.h"
+
+namespace nbx {
+
+// Structure-of-arrays electron queue: a = (pos, E), b = (dir, material bits),
+// c = (tag, uid low, uid high, last triangle).  New electrons start at step 0.
+struct Queue {
+    float4* a;
+    float4* b;
+    uint4* c;
+};
+
+enum Counter : int {
+    kCntSteps = 0,
+    kCntElastic,
+    kCntInelastic,
+    kCntBoundary,
+    kCntSecondaries,
+    kCntDetected,
+    kCntDetectedSE,
+    kCntDetectedBSE,
+    kCntTerminated,
+    kCntRecordsDropped,
+    kCntOverflow,
+    kCntPopped,
+    kNumCounters
+};
+
+struct TransportArgs {
+    Queue in;
+    Queue out;
+    const uint32_t* n_in;       // number of entries pushed to `in` (may exceed in_capacity)
+    uint32_t in_capacity;
+    uint32_t* head;             // pop cursor into `in`
+    uint32_t* out_tail;         // push cursor into `out`
+    uint32_t out_capacity;
+    uint32_t* se_count;         // per-tag detections below 50 eV
+    uint32_t* bse_count;        // per-tag detections at or above 50 eV
+    uint64_t n_tags;
+    unsigned long long* counters;
+    float4* rec_a;              // detected records: (pos, E), (dir, tag bits)
+    float4* rec_b;
+    uint32_t* rec_count;
+    uint32_t rec_capacity;
+    unsigned long long* hist;   // detected-energy histogram
+    int n_bins;
+    float inv_bin_width;
+};
+
+constexpr int kLocalStack = 8;   // per-thread spill slots when `out` is full
+
+cudaError_t launch_transport(const dev::Physics& P, const TransportArgs& a, int grid, int block, cudaStream_t s);
+int transport_max_blocks_per_sm(int block);
+
+cudaError_t launch_ray_query(const dev::Geometry& g, const float* pos, const float* dir, const float* dist,
+                             const int32_t* ignore_tri, const int32_t* ignore_mat, uint64_t n, float* out_dist,
+                             int32_t* out_tri, cudaStream_t s);
+cudaError_t launch_table_query(const dev::Material& m, int table, const float* x, const float* y, uint64_t n,
+                               float* out, cudaStream_t s);
+cudaError_t launch_philox(const uint32_t* ctr, const uint32_t* key, uint64_t n, uint32_t* out, cudaStream_t s);
+// electrons: 56-byte nbx_electron records
+cudaError_t launch_step_query(const dev::Physics& P, void* electrons, uint64_t n, int32_t* status, int32_t* event,
+                              void* secondaries, int32_t* has_se, cudaStream_t s);
+cudaError_t launch_pixel_yields(const uint32_t* se, const uint32_t* bse, const uint32_t* pixel_of_tag,
+                                uint64_t n_tags, uint64_t n_pixels, double* out, cudaStream_t s);
+cudaError_t launch_fill_queue(Queue q, const float* particles, const uint32_t* tags, uint64_t uid_base,
+                              uint64_t n, uint64_t offset, cudaStream_t s);
+
+}  // namespace nbx

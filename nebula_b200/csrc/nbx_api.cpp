@@ -1,0 +1,830 @@
+// Host runtime behind the C ABI declared in include/nbx.h.
+//
+// One nbx_ctx owns one CUDA device's share of the simulation: the uploaded
+// octree and material tables, the primary queue, two generation queues for
+// secondaries, per-tag detection tallies, optional detected records and the
+// energy histogram.  nbx_run launches the persistent transport kernel once per
+// secondary generation, all on one stream, reading each generation's size on
+// the device; the host only checks after each chunk of launches whether the
+// last generation produced further secondaries.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "material.h"
+#include "nbx.h"
+#include "octree.h"
+
+namespace {
+
+struct CudaError : std::runtime_error {
+    explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+struct ApiError : std::runtime_error {
+    int code;
+    ApiError(int c, const std::string& s) : std::runtime_error(s), code(c) {}
+};
+
+void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        release();
+        if (count == 0) return;
+        if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            throw ApiError(NBX_ERR_OOM, "cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes failed");
+        }
+        n = count;
+    }
+    void ensure(size_t count) {
+        if (count > n) alloc(count);
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevBuf() { release(); }
+};
+
+struct QueueBuf {
+    DevBuf<float4> a, b;
+    DevBuf<uint4> c;
+    size_t cap = 0;
+    void ensure(size_t n) {
+        if (n <= cap) return;
+        a.alloc(n);
+        b.alloc(n);
+        c.alloc(n);
+        cap = n;
+    }
+    nbx::Queue q() const { return nbx::Queue{a.p, b.p, c.p}; }
+};
+
+constexpr int kMaxGenerations = 4096;
+constexpr int kChunk = 8;
+constexpr int kHistBins = 20000;
+constexpr float kHistWidth = 0.5f;
+
+}  // namespace
+
+struct nbx_ctx {
+    nbx_config cfg{};
+    std::string err;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int sms = 0;
+
+    // geometry
+    DevBuf<int32_t> octree;
+    DevBuf<float4> tris;
+    bool have_geometry = false;
+    // materials
+    std::vector<DevBuf<float>*> tables;
+    int n_mat = 0;
+    float max_energy = std::numeric_limits<float>::infinity();
+    nbx::dev::Physics phys{};
+
+    // queues
+    QueueBuf prim, qa, qb;
+    uint64_t n_queued = 0;      // primaries waiting in `prim`
+    uint64_t uid_next = 0;
+    DevBuf<float> stage_p;
+    DevBuf<uint32_t> stage_t;
+    DevBuf<uint32_t> ctl;       // head[G], tail[G], n_primary
+    // tallies
+    DevBuf<uint32_t> se_count, bse_count;
+    uint64_t n_tags = 0;
+    DevBuf<unsigned long long> counters;
+    DevBuf<unsigned long long> hist;
+    DevBuf<float4> rec_a, rec_b;
+    DevBuf<uint32_t> rec_count;
+    uint64_t rec_cap = 0;
+    // stats
+    uint64_t pushed = 0, generations = 0;
+    double last_run_ms = 0, last_kernel_ms = 0;
+    int block = 256, bpsm = 0;
+
+    ~nbx_ctx() {
+        for (auto* t : tables) delete t;
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+int fail(nbx_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+template <typename F>
+int guarded(nbx_ctx* ctx, F&& f) {
+    try {
+        if (ctx) {
+            ctx->err.clear();
+            if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return fail(ctx, NBX_ERR_CUDA, "cudaSetDevice failed");
+        }
+        return f();
+    } catch (const ApiError& e) {
+        return fail(ctx, e.code, e.what());
+    } catch (const CudaError& e) {
+        return fail(ctx, NBX_ERR_CUDA, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(ctx, NBX_ERR_OOM, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(ctx, NBX_ERR_FORMAT, e.what());
+    }
+}
+
+nbx::dev::Table1D upload1d(nbx_ctx* ctx, const nbx_table1d& t) {
+    if (t.n < 2 || !t.data) throw ApiError(NBX_ERR_ARG, "1D table needs at least 2 points");
+    auto* b = new DevBuf<float>();
+    ctx->tables.push_back(b);
+    b->alloc(size_t(t.n));
+    ck(cudaMemcpy(b->p, t.data, sizeof(float) * t.n, cudaMemcpyHostToDevice), "table upload");
+    return nbx::dev::Table1D{b->p, t.n, t.x_min, t.x_step};
+}
+
+nbx::dev::Table2D upload2d(nbx_ctx* ctx, const nbx_table2d& t) {
+    if (t.width < 2 || t.height < 2 || !t.data) throw ApiError(NBX_ERR_ARG, "2D table needs at least 2x2 points");
+    auto* b = new DevBuf<float>();
+    ctx->tables.push_back(b);
+    const size_t n = size_t(t.width) * size_t(t.height);
+    b->alloc(n);
+    ck(cudaMemcpy(b->p, t.data, sizeof(float) * n, cudaMemcpyHostToDevice), "table upload");
+    return nbx::dev::Table2D{b->p, t.width, t.height, t.x_min, t.x_step, t.y_min, t.y_step};
+}
+
+void ensure_tags(nbx_ctx* ctx, uint64_t n_tags) {
+    if (n_tags <= ctx->n_tags) return;
+    DevBuf<uint32_t> s, b;
+    s.alloc(n_tags);
+    b.alloc(n_tags);
+    ck(cudaMemsetAsync(s.p, 0, n_tags * 4, ctx->stream), "memset");
+    ck(cudaMemsetAsync(b.p, 0, n_tags * 4, ctx->stream), "memset");
+    if (ctx->n_tags) {
+        ck(cudaMemcpyAsync(s.p, ctx->se_count.p, ctx->n_tags * 4, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+        ck(cudaMemcpyAsync(b.p, ctx->bse_count.p, ctx->n_tags * 4, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+    }
+    ck(cudaStreamSynchronize(ctx->stream), "sync");
+    std::swap(ctx->se_count.p, s.p);
+    std::swap(ctx->se_count.n, s.n);
+    std::swap(ctx->bse_count.p, b.p);
+    std::swap(ctx->bse_count.n, b.n);
+    ctx->n_tags = n_tags;
+}
+
+void fill_material(const nbx::MaterialTables& m, nbx_material* out) {
+    std::memset(out, 0, sizeof(*out));
+    auto dup = [](const std::vector<float>& v) {
+        float* p = static_cast<float*>(std::malloc(sizeof(float) * (v.size() + 1)));
+        if (!p) throw std::bad_alloc();
+        std::memcpy(p, v.data(), sizeof(float) * v.size());
+        return p;
+    };
+    out->barrier = m.barrier;
+    out->elastic_imfp = {m.el_imfp.n, m.el_imfp.x_min, m.el_imfp.x_step, dup(m.el_imfp.data)};
+    out->elastic_icdf = {m.el_icdf.width, m.el_icdf.height, m.el_icdf.x_min, m.el_icdf.x_step,
+                         m.el_icdf.y_min, m.el_icdf.y_step, dup(m.el_icdf.data)};
+    out->phonon_loss = m.phonon_loss;
+    out->recoil_const = m.recoil_const;
+    out->inelastic_imfp = {m.in_imfp.n, m.in_imfp.x_min, m.in_imfp.x_step, dup(m.in_imfp.data)};
+    out->inelastic_icdf = {m.in_icdf.width, m.in_icdf.height, m.in_icdf.x_min, m.in_icdf.x_step,
+                           m.in_icdf.y_min, m.in_icdf.y_step, dup(m.in_icdf.data)};
+    out->ionisation = {m.ionisation.width, m.ionisation.height, m.ionisation.x_min, m.ionisation.x_step,
+                       m.ionisation.y_min, m.ionisation.y_step, dup(m.ionisation.data)};
+    out->fermi = m.fermi;
+    out->band_gap = m.band_gap;
+    out->max_energy = m.max_energy();
+    std::snprintf(out->name, sizeof(out->name), "%s", m.name.c_str());
+}
+
+}  // namespace
+
+extern "C" {
+
+int nbx_version(int* major, int* minor, int* patch) {
+    if (major) *major = NBX_VERSION_MAJOR;
+    if (minor) *minor = NBX_VERSION_MINOR;
+    if (patch) *patch = NBX_VERSION_PATCH;
+    return NBX_OK;
+}
+
+const char* nbx_error_string(int code) {
+    switch (code) {
+    case NBX_OK: return "ok";
+    case NBX_ERR_ARG: return "invalid argument";
+    case NBX_ERR_OOM: return "out of memory";
+    case NBX_ERR_CUDA: return "CUDA error";
+    case NBX_ERR_TIMEOUT: return "device wait timed out";
+    case NBX_ERR_FORMAT: return "malformed input";
+    case NBX_ERR_STATE: return "call out of order";
+    case NBX_ERR_NODEV: return "no CUDA device";
+    case NBX_ERR_CAPACITY: return "device queue overflow";
+    default: return "unknown error";
+    }
+}
+
+void nbx_free(void* p) { std::free(p); }
+
+int nbx_device_count(int* n) {
+    if (!n) return NBX_ERR_ARG;
+    int c = 0;
+    if (cudaGetDeviceCount(&c) != cudaSuccess) {
+        cudaGetLastError();
+        *n = 0;
+        return NBX_ERR_NODEV;
+    }
+    *n = c;
+    return NBX_OK;
+}
+
+int nbx_load_tri(const char* path, nbx_triangle** out, uint64_t* n) {
+    if (!path || !out || !n) return NBX_ERR_ARG;
+    return guarded(nullptr, [&] {
+        auto tris = nbx::load_tri_file(path);
+        if (tris.empty()) return NBX_ERR_FORMAT;
+        auto* p = static_cast<nbx_triangle*>(std::malloc(sizeof(nbx_triangle) * tris.size()));
+        if (!p) return NBX_ERR_OOM;
+        static_assert(sizeof(nbx_triangle) == sizeof(nbx::Triangle), "triangle layout");
+        std::memcpy(p, tris.data(), sizeof(nbx_triangle) * tris.size());
+        *out = p;
+        *n = tris.size();
+        return NBX_OK;
+    });
+}
+
+int nbx_load_pri(const char* path, nbx_record** out, uint64_t* n) {
+    if (!path || !out || !n) return NBX_ERR_ARG;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return NBX_ERR_FORMAT;
+    std::fseek(f, 0, SEEK_END);
+    const long size = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    if (size < 0 || size % 36 != 0) {
+        std::fclose(f);
+        return NBX_ERR_FORMAT;   // "Unexpected end of primaries file"
+    }
+    const uint64_t count = uint64_t(size) / 36;
+    auto* p = static_cast<nbx_record*>(std::malloc(size > 0 ? size_t(size) : 1));
+    if (!p) {
+        std::fclose(f);
+        return NBX_ERR_OOM;
+    }
+    const size_t got = count ? std::fread(p, 36, count, f) : 0;
+    std::fclose(f);
+    if (got != count) {
+        std::free(p);
+        return NBX_ERR_FORMAT;
+    }
+    *out = p;
+    *n = count;
+    return NBX_OK;
+}
+
+int nbx_octree_build(const nbx_triangle* tris, uint64_t n, nbx_octree** out) {
+    if (!tris || n == 0 || !out) return NBX_ERR_ARG;
+    return guarded(nullptr, [&] {
+        std::vector<nbx::Triangle> v(n);
+        std::memcpy(v.data(), tris, sizeof(nbx_triangle) * n);
+        nbx::LinearOctree lin = nbx::build_octree(v);
+        auto* o = static_cast<nbx_octree*>(std::calloc(1, sizeof(nbx_octree)));
+        if (!o) return NBX_ERR_OOM;
+        o->n_octree = lin.octree_data.size();
+        o->octree_data = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * (o->n_octree + 1)));
+        o->n_triangles = lin.triangles.size();
+        o->triangles = static_cast<nbx_triangle*>(std::malloc(sizeof(nbx_triangle) * (o->n_triangles + 1)));
+        if (!o->octree_data || !o->triangles) {
+            nbx_octree_free(o);
+            return NBX_ERR_OOM;
+        }
+        std::memcpy(o->octree_data, lin.octree_data.data(), sizeof(int32_t) * o->n_octree);
+        std::memcpy(o->triangles, lin.triangles.data(), sizeof(nbx_triangle) * o->n_triangles);
+        o->center[0] = lin.center.x;
+        o->center[1] = lin.center.y;
+        o->center[2] = lin.center.z;
+        o->halfsize[0] = lin.halfsize.x;
+        o->halfsize[1] = lin.halfsize.y;
+        o->halfsize[2] = lin.halfsize.z;
+        o->duplicates_dropped = lin.duplicates_dropped;
+        o->max_depth = lin.max_depth;
+        *out = o;
+        return NBX_OK;
+    });
+}
+
+void nbx_octree_free(nbx_octree* o) {
+    if (!o) return;
+    std::free(o->octree_data);
+    std::free(o->triangles);
+    std::free(o);
+}
+
+int nbx_material_load(const char* path, nbx_material** out) {
+    if (!path || !out) return NBX_ERR_ARG;
+    return guarded(nullptr, [&] {
+        nbx::MaterialTables m = nbx::load_material(path);
+        auto* o = static_cast<nbx_material*>(std::calloc(1, sizeof(nbx_material)));
+        if (!o) return NBX_ERR_OOM;
+        fill_material(m, o);
+        *out = o;
+        return NBX_OK;
+    });
+}
+
+void nbx_material_free(nbx_material* m) {
+    if (!m) return;
+    std::free(const_cast<float*>(m->elastic_imfp.data));
+    std::free(const_cast<float*>(m->elastic_icdf.data));
+    std::free(const_cast<float*>(m->inelastic_imfp.data));
+    std::free(const_cast<float*>(m->inelastic_icdf.data));
+    std::free(const_cast<float*>(m->ionisation.data));
+    std::free(m);
+}
+
+void nbx_config_default(nbx_config* cfg) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->seed = 0x78c7e39b;   // gpu_main.cu:238
+}
+
+int nbx_create(nbx_ctx** out, const nbx_config* cfg) {
+    if (!out) return NBX_ERR_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return NBX_ERR_NODEV;
+    }
+    nbx_config c;
+    nbx_config_default(&c);
+    if (cfg) c = *cfg;
+    if (c.device < 0 || c.device >= n) return NBX_ERR_ARG;
+    auto* ctx = new (std::nothrow) nbx_ctx();
+    if (!ctx) return NBX_ERR_OOM;
+    ctx->cfg = c;
+    const int rc = guarded(ctx, [&] {
+        ck(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
+        ck(cudaEventCreate(&ctx->ev0), "event");
+        ck(cudaEventCreate(&ctx->ev1), "event");
+        ck(cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, c.device), "attribute");
+        ctx->counters.alloc(nbx::kNumCounters);
+        ck(cudaMemset(ctx->counters.p, 0, sizeof(unsigned long long) * nbx::kNumCounters), "memset");
+        ctx->hist.alloc(kHistBins);
+        ck(cudaMemset(ctx->hist.p, 0, sizeof(unsigned long long) * kHistBins), "memset");
+        ctx->ctl.alloc(2 * kMaxGenerations + 2);
+        ctx->rec_count.alloc(1);
+        ck(cudaMemset(ctx->rec_count.p, 0, 4), "memset");
+        ctx->block = c.block_size > 0 ? c.block_size : 256;
+        if (ctx->block % 32 != 0 || ctx->block > 256) throw ApiError(NBX_ERR_ARG, "block_size must be a multiple of 32, <= 256");
+        const int maxb = nbx::transport_max_blocks_per_sm(ctx->block);
+        ctx->bpsm = c.blocks_per_sm > 0 ? std::min(c.blocks_per_sm, maxb) : maxb;
+        if (c.record_detected) {
+            ctx->rec_cap = c.record_capacity ? c.record_capacity : (1ull << 24);
+            ctx->rec_a.alloc(ctx->rec_cap);
+            ctx->rec_b.alloc(ctx->rec_cap);
+        }
+        ctx->phys.seed = c.seed;
+        ctx->phys.min_energy = c.energy_threshold;
+        ctx->phys.max_energy = std::numeric_limits<float>::infinity();
+        return NBX_OK;
+    });
+    if (rc != NBX_OK) {
+        std::fprintf(stderr, "nbx_create: %s\n", ctx->err.c_str());
+        delete ctx;
+        return rc;
+    }
+    *out = ctx;
+    return NBX_OK;
+}
+
+void nbx_destroy(nbx_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->cfg.device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    delete ctx;
+}
+
+const char* nbx_last_error(nbx_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int nbx_set_geometry(nbx_ctx* ctx, const nbx_octree* o) {
+    if (!ctx || !o || !o->octree_data || o->n_octree < 8 || !o->triangles) return NBX_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->octree.alloc(o->n_octree);
+        ck(cudaMemcpy(ctx->octree.p, o->octree_data, sizeof(int32_t) * o->n_octree, cudaMemcpyHostToDevice), "octree");
+        std::vector<float4> t(3 * std::max<uint64_t>(o->n_triangles, 1));
+        for (uint64_t i = 0; i < o->n_triangles; ++i) {
+            const nbx_triangle& s = o->triangles[i];
+            float a, b;
+            std::memcpy(&a, &s.mat_in, 4);
+            std::memcpy(&b, &s.mat_out, 4);
+            t[3 * i] = make_float4(s.r0[0], s.r0[1], s.r0[2], a);
+            t[3 * i + 1] = make_float4(s.e1[0], s.e1[1], s.e1[2], b);
+            t[3 * i + 2] = make_float4(s.e2[0], s.e2[1], s.e2[2], 0.0f);
+        }
+        ctx->tris.alloc(t.size());
+        ck(cudaMemcpy(ctx->tris.p, t.data(), sizeof(float4) * t.size(), cudaMemcpyHostToDevice), "triangles");
+        auto& g = ctx->phys.geo;
+        g.octree = ctx->octree.p;
+        g.tri = ctx->tris.p;
+        g.cx = o->center[0];
+        g.cy = o->center[1];
+        g.cz = o->center[2];
+        g.hx = o->halfsize[0];
+        g.hy = o->halfsize[1];
+        g.hz = o->halfsize[2];
+        // octree factory: 2 * magnitude(halfsize), host sqrt (geometry/octree.inl:247-253)
+        g.max_extent = 2 * std::sqrt(g.hx * g.hx + g.hy * g.hy + g.hz * g.hz);
+        g.n_tri = int(o->n_triangles);
+        ctx->have_geometry = true;
+        return NBX_OK;
+    });
+}
+
+int nbx_add_material(nbx_ctx* ctx, const nbx_material* m) {
+    if (!ctx || !m) return NBX_ERR_ARG;
+    if (ctx->n_mat >= NBX_MAX_MATERIALS) return fail(ctx, NBX_ERR_ARG, "too many materials");
+    return guarded(ctx, [&] {
+        nbx::dev::Material d{};
+        d.barrier = m->barrier;
+        d.phonon_loss = m->phonon_loss;
+        d.recoil_const = m->recoil_const;
+        d.fermi = m->fermi;
+        d.band_gap = m->band_gap;
+        d.el_imfp = upload1d(ctx, m->elastic_imfp);
+        d.in_imfp = upload1d(ctx, m->inelastic_imfp);
+        d.el_icdf = upload2d(ctx, m->elastic_icdf);
+        d.in_icdf = upload2d(ctx, m->inelastic_icdf);
+        d.ion = upload2d(ctx, m->ionisation);
+        ctx->phys.mat[ctx->n_mat++] = d;
+        ctx->phys.n_mat = ctx->n_mat;
+        // cpu_material_manager::get_max_energy (core/cpu_material_manager.inl:43-55)
+        if (m->max_energy < ctx->max_energy) ctx->max_energy = m->max_energy;
+        ctx->phys.max_energy = ctx->max_energy;
+        return NBX_OK;
+    });
+}
+
+int nbx_set_tag_range(nbx_ctx* ctx, uint64_t n_tags) {
+    if (!ctx) return NBX_ERR_ARG;
+    return guarded(ctx, [&] {
+        ensure_tags(ctx, n_tags);
+        return NBX_OK;
+    });
+}
+
+int nbx_push(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n, uint64_t* accepted) {
+    if (!ctx || (n && (!particles || !tags))) return NBX_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (accepted) *accepted = 0;
+        if (n == 0) return NBX_OK;
+        if (ctx->n_queued + n > 0xFFFFFFF0ull) throw ApiError(NBX_ERR_CAPACITY, "primary queue limited to 2^32 entries");
+        uint32_t max_tag = 0;
+        for (uint64_t i = 0; i < n; ++i) max_tag = std::max(max_tag, tags[i]);
+        ensure_tags(ctx, uint64_t(max_tag) + 1);
+        if (ctx->prim.cap < ctx->n_queued + n) {
+            // grow, keeping queued primaries
+            QueueBuf nq;
+            nq.ensure(std::max<uint64_t>(ctx->n_queued + n, 2 * ctx->prim.cap));
+            if (ctx->n_queued) {
+                ck(cudaMemcpyAsync(nq.a.p, ctx->prim.a.p, 16 * ctx->n_queued, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+                ck(cudaMemcpyAsync(nq.b.p, ctx->prim.b.p, 16 * ctx->n_queued, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+                ck(cudaMemcpyAsync(nq.c.p, ctx->prim.c.p, 16 * ctx->n_queued, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+                ck(cudaStreamSynchronize(ctx->stream), "sync");
+            }
+            std::swap(ctx->prim.a.p, nq.a.p);
+            std::swap(ctx->prim.a.n, nq.a.n);
+            std::swap(ctx->prim.b.p, nq.b.p);
+            std::swap(ctx->prim.b.n, nq.b.n);
+            std::swap(ctx->prim.c.p, nq.c.p);
+            std::swap(ctx->prim.c.n, nq.c.n);
+            std::swap(ctx->prim.cap, nq.cap);
+        }
+        ctx->stage_p.ensure(7 * n);
+        ctx->stage_t.ensure(n);
+        ck(cudaMemcpyAsync(ctx->stage_p.p, particles, sizeof(float) * 7 * n, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+        ck(cudaMemcpyAsync(ctx->stage_t.p, tags, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+        ck(nbx::launch_fill_queue(ctx->prim.q(), ctx->stage_p.p, ctx->stage_t.p, ctx->uid_next, n, ctx->n_queued,
+                                  ctx->stream), "fill");
+        ck(cudaStreamSynchronize(ctx->stream), "sync");
+        ctx->uid_next += n;
+        ctx->n_queued += n;
+        ctx->pushed += n;
+        if (accepted) *accepted = n;
+        return NBX_OK;
+    });
+}
+
+int nbx_run(nbx_ctx* ctx) {
+    if (!ctx) return NBX_ERR_ARG;
+    if (!ctx->have_geometry) return fail(ctx, NBX_ERR_STATE, "nbx_run before nbx_set_geometry");
+    return guarded(ctx, [&] {
+        ctx->generations = 0;
+        ctx->last_run_ms = ctx->last_kernel_ms = 0;
+        if (ctx->n_queued == 0) return NBX_OK;
+        // Secondary-queue capacity: explicit, else 8 per queued primary
+        // (at least 1M), bounded by a quarter of the free device memory.
+        size_t free_b = 0, total_b = 0;
+        ck(cudaMemGetInfo(&free_b, &total_b), "meminfo");
+        uint64_t want = ctx->cfg.capacity ? ctx->cfg.capacity : std::max<uint64_t>(1ull << 20, 8 * ctx->n_queued);
+        const uint64_t budget = (free_b / 4) / (2 * 48);
+        want = std::min<uint64_t>(want, std::max<uint64_t>(budget, 1ull << 16));
+        want = std::min<uint64_t>(want, 0xFFFFFFF0ull);
+        if (ctx->qa.cap < want) {
+            ctx->qa.a.release(); ctx->qa.b.release(); ctx->qa.c.release(); ctx->qa.cap = 0;
+            ctx->qb.a.release(); ctx->qb.b.release(); ctx->qb.c.release(); ctx->qb.cap = 0;
+            ctx->qa.ensure(want);
+            ctx->qb.ensure(want);
+        }
+        const uint32_t cap = uint32_t(std::min(ctx->qa.cap, ctx->qb.cap));
+        uint32_t* ctl = ctx->ctl.p;
+        ck(cudaMemsetAsync(ctl, 0, sizeof(uint32_t) * (2 * kMaxGenerations + 2), ctx->stream), "memset");
+        const uint32_t nq = uint32_t(ctx->n_queued);
+        ck(cudaMemcpyAsync(ctl + 2 * kMaxGenerations, &nq, 4, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+
+        nbx::TransportArgs a{};
+        a.se_count = ctx->se_count.p;
+        a.bse_count = ctx->bse_count.p;
+        a.n_tags = ctx->n_tags;
+        a.counters = ctx->counters.p;
+        a.rec_a = ctx->rec_a.p;
+        a.rec_b = ctx->rec_b.p;
+        a.rec_count = ctx->rec_count.p;
+        a.rec_capacity = uint32_t(std::min<uint64_t>(ctx->rec_cap, 0xFFFFFFF0ull));
+        a.hist = ctx->hist.p;
+        a.n_bins = kHistBins;
+        a.inv_bin_width = 1.0f / kHistWidth;
+        const int grid = ctx->sms * ctx->bpsm;
+
+        ck(cudaEventRecord(ctx->ev0, ctx->stream), "event");
+        int g = 0;
+        bool done = false;
+        while (!done) {
+            for (int k = 0; k < kChunk && g < kMaxGenerations; ++k, ++g) {
+                const QueueBuf* in = g == 0 ? &ctx->prim : (g % 2 == 1 ? &ctx->qa : &ctx->qb);
+                const QueueBuf* out = (g % 2 == 0) ? &ctx->qa : &ctx->qb;
+                a.in = in->q();
+                a.out = out->q();
+                a.n_in = g == 0 ? ctl + 2 * kMaxGenerations : ctl + kMaxGenerations + (g - 1);
+                a.head = ctl + g;
+                a.out_tail = ctl + kMaxGenerations + g;
+                a.out_capacity = cap;
+                a.in_capacity = uint32_t(std::min<uint64_t>(in->cap, 0xFFFFFFF0ull));
+                ck(nbx::launch_transport(ctx->phys, a, grid, ctx->block, ctx->stream), "transport launch");
+            }
+            uint32_t last = 0;
+            ck(cudaMemcpyAsync(&last, ctl + kMaxGenerations + (g - 1), 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+            ck(cudaStreamSynchronize(ctx->stream), "transport");
+            if (last == 0) done = true;
+            if (!done && g >= kMaxGenerations) throw ApiError(NBX_ERR_CAPACITY, "secondary generations exceed limit");
+        }
+        ck(cudaEventRecord(ctx->ev1, ctx->stream), "event");
+        ck(cudaEventSynchronize(ctx->ev1), "event");
+        float ms = 0;
+        ck(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1), "elapsed");
+        ctx->last_run_ms = ms;
+        ctx->last_kernel_ms = ms;
+        ctx->generations = uint64_t(g);
+        ctx->n_queued = 0;
+        unsigned long long ovf = 0;
+        ck(cudaMemcpy(&ovf, ctx->counters.p + nbx::kCntOverflow, 8, cudaMemcpyDeviceToHost), "D2H");
+        if (ovf) throw ApiError(NBX_ERR_CAPACITY, "secondary queue overflow: electrons lost");
+        return NBX_OK;
+    });
+}
+
+int nbx_get_running_count(nbx_ctx* ctx, uint64_t* n) {
+    if (!ctx || !n) return NBX_ERR_ARG;
+    *n = ctx->n_queued;
+    return NBX_OK;
+}
+
+int nbx_get_stats(nbx_ctx* ctx, nbx_stats* out) {
+    if (!ctx || !out) return NBX_ERR_ARG;
+    return guarded(ctx, [&] {
+        unsigned long long c[nbx::kNumCounters];
+        ck(cudaMemcpy(c, ctx->counters.p, sizeof(c), cudaMemcpyDeviceToHost), "D2H");
+        std::memset(out, 0, sizeof(*out));
+        out->primaries_pushed = ctx->pushed;
+        out->primaries_done = ctx->pushed - ctx->n_queued;
+        out->steps = c[nbx::kCntSteps];
+        out->events_elastic = c[nbx::kCntElastic];
+        out->events_inelastic = c[nbx::kCntInelastic];
+        out->events_boundary = c[nbx::kCntBoundary];
+        out->secondaries = c[nbx::kCntSecondaries];
+        out->detected = c[nbx::kCntDetected];
+        out->detected_se = c[nbx::kCntDetectedSE];
+        out->detected_bse = c[nbx::kCntDetectedBSE];
+        out->terminated = c[nbx::kCntTerminated];
+        out->records_dropped = c[nbx::kCntRecordsDropped];
+        out->queue_overflow = c[nbx::kCntOverflow];
+        out->generations = ctx->generations;
+        out->last_run_ms = ctx->last_run_ms;
+        out->last_kernel_ms = ctx->last_kernel_ms;
+        return NBX_OK;
+    });
+}
+
+int nbx_flush_detected(nbx_ctx* ctx, nbx_detected* out, uint64_t cap, uint64_t* n) {
+    if (!ctx || !n || (cap && !out)) return NBX_ERR_ARG;
+    return guarded(ctx, [&] {
+        *n = 0;
+        if (!ctx->rec_a.p) return NBX_OK;
+        uint32_t cnt = 0;
+        ck(cudaMemcpy(&cnt, ctx->rec_count.p, 4, cudaMemcpyDeviceToHost), "D2H");
+        const uint64_t have = std::min<uint64_t>(cnt, ctx->rec_cap);
+        const uint64_t take = std::min<uint64_t>(have, cap);
+        if (take) {
+            std::vector<float4> a(take), b(take);
+            ck(cudaMemcpy(a.data(), ctx->rec_a.p, 16 * take, cudaMemcpyDeviceToHost), "D2H");
+            ck(cudaMemcpy(b.data(), ctx->rec_b.p, 16 * take, cudaMemcpyDeviceToHost), "D2H");
+            for (uint64_t i = 0; i < take; ++i) {
+                out[i].pos[0] = a[i].x;
+                out[i].pos[1] = a[i].y;
+                out[i].pos[2] = a[i].z;
+                out[i].E = a[i].w;
+                out[i].dir[0] = b[i].x;
+                out[i].dir[1] = b[i].y;
+                out[i].dir[2] = b[i].z;
+                std::memcpy(&out[i].tag, &b[i].w, 4);
+            }
+        }
+        if (take < have) {
+            // keep the remainder at the front
+            const uint64_t rest = have - take;
+            ck(cudaMemcpy(ctx->rec_a.p, ctx->rec_a.p + take, 16 * rest, cudaMemcpyDeviceToDevice), "D2D");
+            ck(cudaMemcpy(ctx->rec_b.p, ctx->rec_b.p + take, 16 * rest, cudaMemcpyDeviceToDevice), "D2D");
+            const uint32_t r = uint32_t(rest);
+            ck(cudaMemcpy(ctx->rec_count.p, &r, 4, cudaMemcpyHostToDevice), "H2D");
+        } else {
+            ck(cudaMemset(ctx->rec_count.p, 0, 4), "memset");
+        }
+        *n = take;
+        return NBX_OK;
+    });
+}
+
+int nbx_get_tag_counts(nbx_ctx* ctx, uint64_t first, uint64_t n, uint32_t* se, uint32_t* bse) {
+    if (!ctx) return NBX_ERR_ARG;
+    if (first + n > ctx->n_tags) return fail(ctx, NBX_ERR_ARG, "tag range beyond nbx_set_tag_range");
+    return guarded(ctx, [&] {
+        if (n == 0) return NBX_OK;
+        if (se) ck(cudaMemcpy(se, ctx->se_count.p + first, 4 * n, cudaMemcpyDeviceToHost), "D2H");
+        if (bse) ck(cudaMemcpy(bse, ctx->bse_count.p + first, 4 * n, cudaMemcpyDeviceToHost), "D2H");
+        return NBX_OK;
+    });
+}
+
+int nbx_pixel_yields(nbx_ctx* ctx, const uint32_t* pixel_of_tag, uint64_t n_tags, uint64_t n_pixels, double* out) {
+    if (!ctx || !pixel_of_tag || !out) return NBX_ERR_ARG;
+    if (n_tags > ctx->n_tags) return fail(ctx, NBX_ERR_ARG, "n_tags beyond the tallied range");
+    return guarded(ctx, [&] {
+        DevBuf<uint32_t> map;
+        DevBuf<double> res;
+        map.alloc(std::max<uint64_t>(n_tags, 1));
+        res.alloc(std::max<uint64_t>(5 * n_pixels, 1));
+        ck(cudaMemcpyAsync(map.p, pixel_of_tag, 4 * n_tags, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+        ck(cudaMemsetAsync(res.p, 0, 8 * 5 * n_pixels, ctx->stream), "memset");
+        ck(nbx::launch_pixel_yields(ctx->se_count.p, ctx->bse_count.p, map.p, n_tags, n_pixels, res.p, ctx->stream),
+           "pixel yields");
+        ck(cudaMemcpyAsync(out, res.p, 8 * 5 * n_pixels, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        ck(cudaStreamSynchronize(ctx->stream), "sync");
+        return NBX_OK;
+    });
+}
+
+int nbx_get_spectrum(nbx_ctx* ctx, uint64_t* counts, uint32_t n_bins, float* bin_width) {
+    if (!ctx) return NBX_ERR_ARG;
+    if (bin_width) *bin_width = kHistWidth;
+    if (!counts) return NBX_OK;
+    return guarded(ctx, [&] {
+        const uint32_t n = std::min<uint32_t>(n_bins, kHistBins);
+        ck(cudaMemcpy(counts, ctx->hist.p, 8ull * n, cudaMemcpyDeviceToHost), "D2H");
+        return NBX_OK;
+    });
+}
+
+int nbx_reset_tallies(nbx_ctx* ctx) {
+    if (!ctx) return NBX_ERR_ARG;
+    return guarded(ctx, [&] {
+        ck(cudaMemsetAsync(ctx->counters.p, 0, 8 * nbx::kNumCounters, ctx->stream), "memset");
+        ck(cudaMemsetAsync(ctx->hist.p, 0, 8ull * kHistBins, ctx->stream), "memset");
+        ck(cudaMemsetAsync(ctx->rec_count.p, 0, 4, ctx->stream), "memset");
+        if (ctx->n_tags) {
+            ck(cudaMemsetAsync(ctx->se_count.p, 0, 4 * ctx->n_tags, ctx->stream), "memset");
+            ck(cudaMemsetAsync(ctx->bse_count.p, 0, 4 * ctx->n_tags, ctx->stream), "memset");
+        }
+        ck(cudaStreamSynchronize(ctx->stream), "sync");
+        ctx->pushed = ctx->n_queued;
+        return NBX_OK;
+    });
+}
+
+int nbx_ray_query(nbx_ctx* ctx, const float* pos, const float* dir, const float* dist, const int32_t* ignore_tri,
+                  const int32_t* ignore_mat, uint64_t n, float* out_dist, int32_t* out_tri) {
+    if (!ctx || (n && (!pos || !dir || !dist || !ignore_tri || !ignore_mat || !out_dist || !out_tri))) return NBX_ERR_ARG;
+    if (!ctx->have_geometry) return fail(ctx, NBX_ERR_STATE, "no geometry");
+    return guarded(ctx, [&] {
+        if (n == 0) return NBX_OK;
+        DevBuf<float> p, d, l, od;
+        DevBuf<int32_t> it, im, ot;
+        p.alloc(3 * n); d.alloc(3 * n); l.alloc(n); od.alloc(n);
+        it.alloc(n); im.alloc(n); ot.alloc(n);
+        auto s = ctx->stream;
+        ck(cudaMemcpyAsync(p.p, pos, 12 * n, cudaMemcpyHostToDevice, s), "H2D");
+        ck(cudaMemcpyAsync(d.p, dir, 12 * n, cudaMemcpyHostToDevice, s), "H2D");
+        ck(cudaMemcpyAsync(l.p, dist, 4 * n, cudaMemcpyHostToDevice, s), "H2D");
+        ck(cudaMemcpyAsync(it.p, ignore_tri, 4 * n, cudaMemcpyHostToDevice, s), "H2D");
+        ck(cudaMemcpyAsync(im.p, ignore_mat, 4 * n, cudaMemcpyHostToDevice, s), "H2D");
+        ck(nbx::launch_ray_query(ctx->phys.geo, p.p, d.p, l.p, it.p, im.p, n, od.p, ot.p, s), "ray query");
+        ck(cudaMemcpyAsync(out_dist, od.p, 4 * n, cudaMemcpyDeviceToHost, s), "D2H");
+        ck(cudaMemcpyAsync(out_tri, ot.p, 4 * n, cudaMemcpyDeviceToHost, s), "D2H");
+        ck(cudaStreamSynchronize(s), "sync");
+        return NBX_OK;
+    });
+}
+
+int nbx_table_query(nbx_ctx* ctx, int32_t material, int32_t table, const float* x, const float* y, uint64_t n,
+                    float* out) {
+    if (!ctx || (n && (!x || !out))) return NBX_ERR_ARG;
+    if (material < 0 || material >= ctx->n_mat || table < 0 || table > 4) return fail(ctx, NBX_ERR_ARG, "bad material/table");
+    return guarded(ctx, [&] {
+        if (n == 0) return NBX_OK;
+        DevBuf<float> dx, dy, dout;
+        dx.alloc(n); dy.alloc(n); dout.alloc(n);
+        auto s = ctx->stream;
+        ck(cudaMemcpyAsync(dx.p, x, 4 * n, cudaMemcpyHostToDevice, s), "H2D");
+        if (y) ck(cudaMemcpyAsync(dy.p, y, 4 * n, cudaMemcpyHostToDevice, s), "H2D");
+        else ck(cudaMemsetAsync(dy.p, 0, 4 * n, s), "memset");
+        ck(nbx::launch_table_query(ctx->phys.mat[material], table, dx.p, dy.p, n, dout.p, s), "table query");
+        ck(cudaMemcpyAsync(out, dout.p, 4 * n, cudaMemcpyDeviceToHost, s), "D2H");
+        ck(cudaStreamSynchronize(s), "sync");
+        return NBX_OK;
+    });
+}
+
+int nbx_philox(nbx_ctx* ctx, const uint32_t* ctr, const uint32_t* key, uint64_t n, uint32_t* out) {
+    if (!ctx || (n && (!ctr || !key || !out))) return NBX_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (n == 0) return NBX_OK;
+        DevBuf<uint32_t> c, k, o;
+        c.alloc(4 * n); k.alloc(2 * n); o.alloc(4 * n);
+        auto s = ctx->stream;
+        ck(cudaMemcpyAsync(c.p, ctr, 16 * n, cudaMemcpyHostToDevice, s), "H2D");
+        ck(cudaMemcpyAsync(k.p, key, 8 * n, cudaMemcpyHostToDevice, s), "H2D");
+        ck(nbx::launch_philox(c.p, k.p, n, o.p, s), "philox");
+        ck(cudaMemcpyAsync(out, o.p, 16 * n, cudaMemcpyDeviceToHost, s), "D2H");
+        ck(cudaStreamSynchronize(s), "sync");
+        return NBX_OK;
+    });
+}
+
+int nbx_step_query(nbx_ctx* ctx, nbx_electron* electrons, uint64_t n, int32_t* status, int32_t* event,
+                   nbx_electron* secondaries, int32_t* has_se) {
+    if (!ctx || (n && (!electrons || !status || !event || !secondaries || !has_se))) return NBX_ERR_ARG;
+    if (!ctx->have_geometry) return fail(ctx, NBX_ERR_STATE, "no geometry");
+    static_assert(sizeof(nbx_electron) == 56, "nbx_electron layout");
+    return guarded(ctx, [&] {
+        if (n == 0) return NBX_OK;
+        for (uint64_t i = 0; i < n; ++i) {
+            const int m = electrons[i].mat;
+            if (m >= ctx->n_mat) throw ApiError(NBX_ERR_ARG, "electron material index out of range");
+            const int t = electrons[i].last_tri;
+            if (t >= ctx->phys.geo.n_tri) throw ApiError(NBX_ERR_ARG, "electron triangle index out of range");
+        }
+        DevBuf<uint8_t> e, se;
+        DevBuf<int32_t> st, ev, hs;
+        e.alloc(56 * n); se.alloc(56 * n); st.alloc(n); ev.alloc(n); hs.alloc(n);
+        auto s = ctx->stream;
+        ck(cudaMemcpyAsync(e.p, electrons, 56 * n, cudaMemcpyHostToDevice, s), "H2D");
+        ck(cudaMemsetAsync(se.p, 0, 56 * n, s), "memset");
+        ck(nbx::launch_step_query(ctx->phys, e.p, n, st.p, ev.p, se.p, hs.p, s), "step query");
+        ck(cudaMemcpyAsync(electrons, e.p, 56 * n, cudaMemcpyDeviceToHost, s), "D2H");
+        ck(cudaMemcpyAsync(secondaries, se.p, 56 * n, cudaMemcpyDeviceToHost, s), "D2H");
+        ck(cudaMemcpyAsync(status, st.p, 4 * n, cudaMemcpyDeviceToHost, s), "D2H");
+        ck(cudaMemcpyAsync(event, ev.p, 4 * n, cudaMemcpyDeviceToHost, s), "D2H");
+        ck(cudaMemcpyAsync(has_se, hs.p, 4 * n, cudaMemcpyDeviceToHost, s), "D2H");
+        ck(cudaStreamSynchronize(s), "sync");
+        return NBX_OK;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,351 @@
+// Persistent electron-transport kernel and the kernel-level query kernels.
+//
+// The transport kernel replaces the reference's event-sorted SIMT driver
+// (drivers/gpu/gpu_driver.inl:312-567: init + CUB radix sort + intersect /
+// elastic / inelastic launched over the whole slot capacity every
+// iteration).  Here each thread keeps one electron in registers and runs
+// init -> event passes back to back until the electron terminates or is
+// detected, then refills from a device queue with a warp-aggregated atomic.
+// Secondaries are pushed to the next generation's queue (warp-aggregated);
+// if that queue is full a thread keeps up to kLocalStack of its own
+// secondaries and simulates them itself.  Detections are tallied per
+// primary tag on the device; detected records are optional.
+#include <cooperative_groups.h>
+
+#include "kernels.h"
+#include "transport.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace nbx {
+
+namespace {
+
+__device__ __forceinline__ void load_electron(const Queue& q, uint32_t i, dev::Electron& e) {
+    const float4 a = q.a[i];
+    const float4 b = q.b[i];
+    const uint4 c = q.c[i];
+    e.px = a.x;
+    e.py = a.y;
+    e.pz = a.z;
+    e.E = a.w;
+    e.dx = b.x;
+    e.dy = b.y;
+    e.dz = b.z;
+    e.mat = __float_as_int(b.w);
+    e.tag = c.x;
+    e.uid = uint64_t(c.y) | (uint64_t(c.z) << 32);
+    e.last_tri = int(c.w);
+    e.step = 0;
+}
+
+__device__ __forceinline__ void store_electron(const Queue& q, uint32_t i, const dev::Electron& e) {
+    q.a[i] = make_float4(e.px, e.py, e.pz, e.E);
+    q.b[i] = make_float4(e.dx, e.dy, e.dz, __int_as_float(e.mat));
+    q.c[i] = make_uint4(e.tag, uint32_t(e.uid), uint32_t(e.uid >> 32), uint32_t(e.last_tri));
+}
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(256) transport_kernel(const dev::Physics P, const TransportArgs a) {
+    const uint32_t n_in = min(*a.n_in, a.in_capacity);
+    dev::Electron e;
+    dev::Electron stack[kLocalStack];
+    int sp = 0;
+    bool alive = false;
+    unsigned long long c_steps = 0, c_el = 0, c_inel = 0, c_bd = 0, c_se = 0, c_det = 0, c_dse = 0, c_dbse = 0,
+                       c_term = 0, c_drop = 0, c_ovf = 0, c_pop = 0;
+    for (;;) {
+        if (!alive) {
+            if (sp > 0) {
+                e = stack[--sp];
+                alive = true;
+            } else {
+                uint32_t idx;
+                {
+                    cg::coalesced_group g = cg::coalesced_threads();
+                    uint32_t base = 0;
+                    if (g.thread_rank() == 0) base = atomicAdd(a.head, g.size());
+                    base = g.shfl(base, 0);
+                    idx = base + g.thread_rank();
+                }
+                if (idx >= n_in) break;
+                load_electron(a.in, idx, e);
+                ++c_pop;
+                alive = true;
+            }
+        }
+        int ev;
+        bool has_se;
+        dev::Electron se;
+        const int st = dev::step(P, e, &ev, &se, &has_se);
+        ++c_steps;
+        c_el += (ev == dev::kEvElastic);
+        c_inel += (ev == dev::kEvInelastic);
+        c_bd += (ev == dev::kEvBoundary);
+        if (has_se) {
+            ++c_se;
+            cg::coalesced_group g = cg::coalesced_threads();
+            uint32_t base = 0;
+            if (g.thread_rank() == 0) base = atomicAdd(a.out_tail, g.size());
+            base = g.shfl(base, 0);
+            const uint32_t slot = base + g.thread_rank();
+            if (slot < a.out_capacity) {
+                store_electron(a.out, slot, se);
+            } else if (sp < kLocalStack) {
+                stack[sp++] = se;
+            } else {
+                ++c_ovf;
+            }
+        }
+        if (st == dev::kAlive) continue;
+        alive = false;
+        if (st == dev::kTerminated) {
+            ++c_term;
+            continue;
+        }
+        // detected
+        ++c_det;
+        const bool is_se = e.E < 50;
+        c_dse += is_se;
+        c_dbse += !is_se;
+        if (e.tag < a.n_tags) atomicAdd(is_se ? a.se_count + e.tag : a.bse_count + e.tag, 1u);
+        if (a.hist) {
+            int bin = dev::floor_to_int(e.E * a.inv_bin_width);
+            bin = bin < 0 ? 0 : (bin >= a.n_bins ? a.n_bins - 1 : bin);
+            atomicAdd(a.hist + bin, 1ull);
+        }
+        if (a.rec_a) {
+            const uint32_t slot = atomicAdd(a.rec_count, 1u);
+            if (slot < a.rec_capacity) {
+                a.rec_a[slot] = make_float4(e.px, e.py, e.pz, e.E);
+                a.rec_b[slot] = make_float4(e.dx, e.dy, e.dz, __uint_as_float(e.tag));
+            } else {
+                ++c_drop;
+            }
+        }
+    }
+    // Counters: one atomic per warp per counter.
+    unsigned long long v[kNumCounters];
+    v[kCntSteps] = c_steps;
+    v[kCntElastic] = c_el;
+    v[kCntInelastic] = c_inel;
+    v[kCntBoundary] = c_bd;
+    v[kCntSecondaries] = c_se;
+    v[kCntDetected] = c_det;
+    v[kCntDetectedSE] = c_dse;
+    v[kCntDetectedBSE] = c_dbse;
+    v[kCntTerminated] = c_term;
+    v[kCntRecordsDropped] = c_drop;
+    v[kCntOverflow] = c_ovf;
+    v[kCntPopped] = c_pop;
+    __syncwarp();
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int i = 0; i < kNumCounters; ++i) {
+        const unsigned long long s = warp_sum(v[i]);
+        if (lane == 0 && s) atomicAdd(a.counters + i, s);
+    }
+}
+
+__global__ void ray_query_kernel(const dev::Geometry g, const float* pos, const float* dir, const float* dist,
+                                 const int32_t* ignore_tri, const int32_t* ignore_mat, uint64_t n, float* out_dist,
+                                 int32_t* out_tri) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        int hit;
+        const dev::V3 p{pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+        const dev::V3 d{dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]};
+        out_dist[i] = dev::propagate(g, p, d, dist[i], ignore_tri[i], ignore_mat[i], &hit);
+        out_tri[i] = hit;
+    }
+}
+
+__global__ void table_query_kernel(const dev::Material m, int table, const float* x, const float* y, uint64_t n,
+                                   float* out) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        float r;
+        switch (table) {
+        case 0: r = dev::table1d_get(m.el_imfp, x[i]); break;
+        case 1: r = dev::table2d_get(m.el_icdf, x[i], y[i]); break;
+        case 2: r = dev::table1d_get(m.in_imfp, x[i]); break;
+        case 3: r = dev::table2d_get(m.in_icdf, x[i], y[i]); break;
+        default: r = dev::table2d_rounddown(m.ion, x[i], y[i]); break;
+        }
+        out[i] = r;
+    }
+}
+
+__global__ void philox_kernel(const uint32_t* ctr, const uint32_t* key, uint64_t n, uint32_t* out) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint4 c = make_uint4(ctr[4 * i], ctr[4 * i + 1], ctr[4 * i + 2], ctr[4 * i + 3]);
+        const uint4 r = dev::philox4x32_10(c, make_uint2(key[2 * i], key[2 * i + 1]));
+        out[4 * i] = r.x;
+        out[4 * i + 1] = r.y;
+        out[4 * i + 2] = r.z;
+        out[4 * i + 3] = r.w;
+    }
+}
+
+// 56-byte nbx_electron record
+struct ElectronRecord {
+    float pos[3];
+    float dir[3];
+    float E;
+    int32_t mat;
+    int32_t last_tri;
+    uint32_t tag;
+    uint64_t uid;
+    uint32_t step;
+    uint32_t pad;
+};
+static_assert(sizeof(ElectronRecord) == 56, "nbx_electron layout");
+
+__device__ __forceinline__ dev::Electron from_record(const ElectronRecord& r) {
+    dev::Electron e;
+    e.px = r.pos[0];
+    e.py = r.pos[1];
+    e.pz = r.pos[2];
+    e.dx = r.dir[0];
+    e.dy = r.dir[1];
+    e.dz = r.dir[2];
+    e.E = r.E;
+    e.mat = r.mat;
+    e.last_tri = r.last_tri;
+    e.tag = r.tag;
+    e.uid = r.uid;
+    e.step = r.step;
+    return e;
+}
+__device__ __forceinline__ void to_record(const dev::Electron& e, ElectronRecord& r) {
+    r.pos[0] = e.px;
+    r.pos[1] = e.py;
+    r.pos[2] = e.pz;
+    r.dir[0] = e.dx;
+    r.dir[1] = e.dy;
+    r.dir[2] = e.dz;
+    r.E = e.E;
+    r.mat = e.mat;
+    r.last_tri = e.last_tri;
+    r.tag = e.tag;
+    r.uid = e.uid;
+    r.step = e.step;
+    r.pad = 0;
+}
+
+__global__ void step_query_kernel(const dev::Physics P, ElectronRecord* el, uint64_t n, int32_t* status,
+                                  int32_t* event, ElectronRecord* ses, int32_t* has_se) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        dev::Electron e = from_record(el[i]);
+        dev::Electron se{};
+        int ev;
+        bool hs;
+        status[i] = dev::step(P, e, &ev, &se, &hs);
+        event[i] = ev;
+        has_se[i] = hs ? 1 : 0;
+        to_record(e, el[i]);
+        if (hs) to_record(se, ses[i]);
+    }
+}
+
+__global__ void pixel_yields_kernel(const uint32_t* se, const uint32_t* bse, const uint32_t* pixel_of_tag,
+                                    uint64_t n_tags, uint64_t n_pixels, double* out) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n_tags;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t p = pixel_of_tag[i];
+        if (p >= n_pixels) continue;
+        const double s = se[i], b = bse[i];
+        double* o = out + 5 * size_t(p);
+        atomicAdd(o + 0, 1.0);
+        if (s != 0) {
+            atomicAdd(o + 1, s);
+            atomicAdd(o + 2, s * s);
+        }
+        if (b != 0) {
+            atomicAdd(o + 3, b);
+            atomicAdd(o + 4, b * b);
+        }
+    }
+}
+
+__global__ void fill_queue_kernel(Queue q, const float* particles, const uint32_t* tags, uint64_t uid_base, uint64_t n,
+                                  uint64_t offset) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const float* p = particles + 7 * i;
+        const uint64_t uid = uid_base + i;
+        const uint64_t s = offset + i;
+        q.a[s] = make_float4(p[0], p[1], p[2], p[6]);
+        q.b[s] = make_float4(p[3], p[4], p[5], __int_as_float(dev::kVacuum));
+        q.c[s] = make_uint4(tags[i], uint32_t(uid), uint32_t(uid >> 32), 0xFFFFFFFFu);
+    }
+}
+
+int grid_for(uint64_t n, int block) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint64_t need = (n + block - 1) / block;
+    const uint64_t cap = uint64_t(sms) * 16;
+    return int(need < cap ? (need > 0 ? need : 1) : cap);
+}
+
+}  // namespace
+
+cudaError_t launch_transport(const dev::Physics& P, const TransportArgs& a, int grid, int block, cudaStream_t s) {
+    transport_kernel<<<grid, block, 0, s>>>(P, a);
+    return cudaGetLastError();
+}
+
+int transport_max_blocks_per_sm(int block) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel, block, 0) != cudaSuccess) return 1;
+    return n > 0 ? n : 1;
+}
+
+cudaError_t launch_ray_query(const dev::Geometry& g, const float* pos, const float* dir, const float* dist,
+                             const int32_t* ignore_tri, const int32_t* ignore_mat, uint64_t n, float* out_dist,
+                             int32_t* out_tri, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    ray_query_kernel<<<grid_for(n, 128), 128, 0, s>>>(g, pos, dir, dist, ignore_tri, ignore_mat, n, out_dist, out_tri);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_table_query(const dev::Material& m, int table, const float* x, const float* y, uint64_t n,
+                               float* out, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    table_query_kernel<<<grid_for(n, 256), 256, 0, s>>>(m, table, x, y, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_philox(const uint32_t* ctr, const uint32_t* key, uint64_t n, uint32_t* out, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    philox_kernel<<<grid_for(n, 256), 256, 0, s>>>(ctr, key, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_step_query(const dev::Physics& P, void* electrons, uint64_t n, int32_t* status, int32_t* event,
+                              void* secondaries, int32_t* has_se, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    step_query_kernel<<<grid_for(n, 128), 128, 0, s>>>(P, static_cast<ElectronRecord*>(electrons), n, status, event,
+                                                        static_cast<ElectronRecord*>(secondaries), has_se);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pixel_yields(const uint32_t* se, const uint32_t* bse, const uint32_t* pixel_of_tag,
+                                uint64_t n_tags, uint64_t n_pixels, double* out, cudaStream_t s) {
+    if (n_tags == 0) return cudaSuccess;
+    pixel_yields_kernel<<<grid_for(n_tags, 256), 256, 0, s>>>(se, bse, pixel_of_tag, n_tags, n_pixels, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_queue(Queue q, const float* particles, const uint32_t* tags, uint64_t uid_base, uint64_t n,
+                              uint64_t offset, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    fill_queue_kernel<<<grid_for(n, 256), 256, 0, s>>>(q, particles, tags, uid_base, n, offset);
+    return cudaGetLastError();
+}
+
+}  // namespace nbx

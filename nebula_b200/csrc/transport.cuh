@@ -1,0 +1,478 @@
+// Device-side electron transport for sm_100a.
+//
+// Single-precision arithmetic follows the reference's order and grouping
+// operation by operation; the translation unit is compiled with
+// -fmad=false and IEEE division/square root, so octree ray queries and table
+// lookups are bit-identical to the reference CPU path.  Transcendentals are
+// CUDA's accurate (non-intrinsic) logf/expf/expm1f/sinf/cosf/atan2f.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dev_types.h"
+
+namespace nbx {
+namespace dev {
+
+// ---------------------------------------------------------------------------
+// Random numbers: Philox4x32-10 (Salmon et al., SC'11)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t lo1 = 0xCD9E8D57u * c.z;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+// (k + 1/2) / 2^23 with k the top 23 bits: exact, in (0, 1).
+__device__ __forceinline__ float u01(uint32_t x) {
+    return __fadd_rn(__fmul_rn(float(x >> 9), 1.1920928955078125e-07f), 5.9604644775390625e-08f);
+}
+__device__ __forceinline__ uint64_t secondary_uid(uint64_t parent, uint32_t step) {
+    uint64_t z = parent + 0x9E3779B97F4A7C15ull * (uint64_t(step) + 1u);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z = z ^ (z >> 31);
+    return z | (1ull << 63);
+}
+__device__ __forceinline__ uint4 draw(uint32_t seed, const Electron& e, uint32_t block) {
+    return philox4x32_10(make_uint4(e.step, block, uint32_t(e.uid), uint32_t(e.uid >> 32)), make_uint2(seed, 0u));
+}
+
+// ---------------------------------------------------------------------------
+// Scalar helpers with the reference CPU semantics
+// ---------------------------------------------------------------------------
+// (int)std::floor(x) as an x86-64 host evaluates it: out-of-range and NaN
+// give INT_MIN (scalar_math.h:44-56, CPU branch).
+__device__ __forceinline__ int floor_to_int(float x) {
+    const float f = floorf(x);
+    return (fabsf(f) < 2147483648.0f) ? int(f) : int(0x80000000u);
+}
+__device__ __forceinline__ int clampi(int i, int lo, int hi) { return i < lo ? lo : (i > hi ? hi : i); }
+__device__ __forceinline__ float clampr(float i, float lo, float hi) { return i < lo ? lo : (i > hi ? hi : i); }
+__device__ __forceinline__ float min_ref(float a, float b) { return (b < a) ? b : a; }
+__device__ __forceinline__ float max_ref(float a, float b) { return (a < b) ? b : a; }
+
+// ---------------------------------------------------------------------------
+// Tables (common/util/table_1D.inl:66-80, table_2D.inl:74-104)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float table1d_get(const Table1D& t, float x) {
+    const float xi = (x - t.x_min) * t.x_step;
+    const int lo = clampi(floor_to_int(xi), 0, t.n - 2);
+    const float a = __ldg(t.data + lo);
+    const float b = __ldg(t.data + lo + 1);
+    const float f = xi - float(lo);
+    return (1 - f) * a + f * b;
+}
+__device__ __forceinline__ float table2d_get(const Table2D& t, float x, float y) {
+    const float xi = (x - t.x_min) * t.x_step;
+    const float yi = (y - t.y_min) * t.y_step;
+    const int lx = clampi(floor_to_int(xi), 0, t.w - 2);
+    const int ly = clampi(floor_to_int(yi), 0, t.h - 2);
+    const float* r0 = t.data + size_t(lx) * t.h + ly;
+    const float* r1 = r0 + t.h;
+    const float v00 = __ldg(r0), v01 = __ldg(r0 + 1);
+    const float v10 = __ldg(r1), v11 = __ldg(r1 + 1);
+    const float fx = xi - float(lx);
+    const float fy = yi - float(ly);
+    return (1 - fx) * (1 - fy) * v00 + fx * (1 - fy) * v10 + (1 - fx) * fy * v01 + fx * fy * v11;
+}
+__device__ __forceinline__ float table2d_rounddown(const Table2D& t, float x, float y) {
+    const float xi = (x - t.x_min) * t.x_step;
+    const float yi = (y - t.y_min) * t.y_step;
+    const int lx = clampi(floor_to_int(xi), 0, t.w - 1);
+    const int ly = clampi(floor_to_int(yi), 0, t.h - 1);
+    return __ldg(t.data + size_t(lx) * t.h + ly);
+}
+
+// ---------------------------------------------------------------------------
+// Vector helpers (common/vector_math.h, CPU branches)
+// ---------------------------------------------------------------------------
+struct V3 {
+    float x, y, z;
+};
+__device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 cross(V3 a, V3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+// normalised(a) = a * (1 / sqrt(a.a))   (vector_math.h:37-40,128-140)
+__device__ __forceinline__ V3 normalised(V3 a) {
+    const float inv = 1.0f / sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
+    return {a.x * inv, a.y * inv, a.z * inv};
+}
+// vector_math.h:171-186
+__device__ __forceinline__ V3 make_normal_vec(V3 dir, float phi) {
+    const float az = atan2f(dir.y, dir.x);
+    float sin_az, cos_az;
+    sincosf(az, &sin_az, &cos_az);
+    const V3 v{dir.z * cos_az, dir.z * sin_az, -sqrtf(dir.x * dir.x + dir.y * dir.y)};
+    const V3 u = cross(v, dir);
+    float sp, cp;
+    sincosf(phi, &sp, &cp);
+    return {u.x * cp + v.x * sp, u.y * cp + v.y * sp, u.z * cp + v.z * sp};
+}
+// vector_math.h:194-206
+__device__ __forceinline__ V3 make_unit_vec(float cos_theta, float phi) {
+    float sp, cp;
+    sincosf(phi, &sp, &cp);
+    cos_theta = clampr(cos_theta, -1, 1);
+    const float st = sqrtf(1 - cos_theta * cos_theta);
+    return {st * cp, st * sp, cos_theta};
+}
+
+// ---------------------------------------------------------------------------
+// Geometry
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void load_tri(const Geometry& g, int ti, V3& r0, V3& e1, V3& e2, int& mi, int& mo) {
+    const float4 a = __ldg(g.tri + 3 * ti);
+    const float4 b = __ldg(g.tri + 3 * ti + 1);
+    const float4 c = __ldg(g.tri + 3 * ti + 2);
+    r0 = {a.x, a.y, a.z};
+    e1 = {b.x, b.y, b.z};
+    e2 = {c.x, c.y, c.z};
+    mi = __float_as_int(a.w);
+    mo = __float_as_int(b.w);
+}
+
+// triangle::intersect_ray (core/triangle.inl:7-29)
+__device__ __forceinline__ float intersect_ray(V3 r0, V3 e1, V3 e2, V3 start, V3 dir) {
+    const V3 pvec = cross(dir, e2);
+    const float det = dot(e1, pvec);
+    if (fabsf(det) < kEps) return -1;
+    const V3 s{start.x - r0.x, start.y - r0.y, start.z - r0.z};
+    const float u = dot(s, pvec) / det;
+    if ((u < -kEps) || (u > 1 + kEps)) return -1;
+    const V3 qvec = cross(s, e1);
+    const float v = dot(dir, qvec) / det;
+    if ((v < -kEps) || (u + v > 1 + kEps)) return -1;
+    const float t = dot(e2, qvec) / det;
+    if (t < 0) return -1;
+    return t;
+}
+
+// octree::in_domain (geometry/octree.inl:25-31)
+__device__ __forceinline__ bool in_domain(const Geometry& g, V3 p) {
+    return (p.x > g.cx - g.hx) && (p.x < g.cx + g.hx) && (p.y > g.cy - g.hy) && (p.y < g.cy + g.hy) &&
+           (p.z > g.cz - g.hz) && (p.z < g.cz + g.hz);
+}
+
+// octree::propagate (geometry/octree.inl:33-192).  Returns the travelled
+// distance; *hit receives the triangle index or -1.
+__device__ __forceinline__ float propagate(const Geometry& g, V3 start, V3 dir, float distance, int ignore_tri,
+                                           int ignore_mat, int* hit) {
+    const int32_t* od = g.octree;
+    V3 cur = start;
+    float to_go = distance;
+    uint64_t location = 1;
+    do {
+        float ax = g.cx, ay = g.cy, az = g.cz, aw = 1;
+        int index = 0;
+        for (int i = 60 - __clzll(location); i >= 0; i -= 3) {
+            const unsigned octant = unsigned(location >> i) & 7u;
+            index = __ldg(od + index + octant);
+            ax += aw * g.hx * (float(octant & 1) - 0.5f);
+            ay += aw * g.hy * (float((octant & 2) >> 1) - 0.5f);
+            az += aw * g.hz * (float((octant & 4) >> 2) - 0.5f);
+            aw *= 0.5f;
+        }
+        while (index >= 0) {
+            unsigned octant = 0;
+            octant ^= (cur.x > ax) ? 1u : 0u;
+            octant ^= (cur.y > ay) ? 2u : 0u;
+            octant ^= (cur.z > az) ? 4u : 0u;
+            location = (location << 3) | octant;
+            index = __ldg(od + index + octant);
+            ax += aw * g.hx * (float(octant & 1) - 0.5f);
+            ay += aw * g.hy * (float((octant & 2) >> 1) - 0.5f);
+            az += aw * g.hz * (float((octant & 4) >> 2) - 0.5f);
+            aw *= 0.5f;
+        }
+        index = -index;
+
+        float intersect;
+        int target;
+        {
+            const float bx = aw * g.hx, by = aw * g.hy, bz = aw * g.hz;
+            const float tx = (ax + copysignf(bx + kEps, dir.x) - cur.x) / dir.x;
+            const float ty = (ay + copysignf(by + kEps, dir.y) - cur.y) / dir.y;
+            const float tz = (az + copysignf(bz + kEps, dir.z) - cur.z) / dir.z;
+            if ((tx < ty) && (tx < tz)) {
+                intersect = tx;
+                target = -1;
+            } else if ((ty < tx) && (ty < tz)) {
+                intersect = ty;
+                target = -2;
+            } else {
+                intersect = tz;
+                target = -4;
+            }
+        }
+        for (;;) {
+            const int ti = __ldg(od + index);
+            ++index;
+            if (ti < 0) break;
+            if (ti == ignore_tri) continue;
+            V3 r0, e1, e2;
+            int mi, mo;
+            load_tri(g, ti, r0, e1, e2, mi, mo);
+            const int mat_out = (dot(cross(e1, e2), dir) < 0) ? mi : mo;
+            if (mat_out == ignore_mat) continue;
+            const float t = intersect_ray(r0, e1, e2, cur, dir);
+            if ((t > 0) && (t <= intersect + kEps)) {
+                intersect = t;
+                target = ti;
+            }
+        }
+        if (intersect >= to_go) {
+            *hit = -1;
+            return distance;
+        } else if (target >= 0) {
+            *hit = target;
+            return distance - to_go + intersect;
+        }
+        to_go -= intersect;
+        cur.x += dir.x * intersect;
+        cur.y += dir.y * intersect;
+        cur.z += dir.z * intersect;
+        const unsigned mask = unsigned(-target);
+        unsigned value;
+        if (mask == 1)
+            value = (dir.x >= 0) ? 0u : 1u;
+        else if (mask == 2)
+            value = (dir.y >= 0) ? 0u : 2u;
+        else
+            value = (dir.z >= 0) ? 0u : 4u;
+        while (location > 1) {
+            if ((location & mask) == value) {
+                location ^= mask;
+                break;
+            }
+            location >>= 3;
+        }
+    } while (location > 1);
+    *hit = -1;
+    return distance;
+}
+
+// ---------------------------------------------------------------------------
+// Physics
+// ---------------------------------------------------------------------------
+// kieft_elastic<acoustic phonon loss, atomic recoil>::execute (physics/kieft/elastic.h:68-115)
+__device__ __forceinline__ void elastic(const Material& m, Electron& e, float u_cos, float u_phi) {
+    const float x = logf(e.E);
+    const float cos_theta = clampr(table2d_get(m.el_icdf, x, u_cos), -1, 1);
+    const float sin_theta = sqrtf(1 - cos_theta * cos_theta);
+    const V3 d = normalised(V3{e.dx, e.dy, e.dz});
+    const V3 n = normalised(make_normal_vec(d, (2 * kPi) * u_phi));
+    e.dx = d.x * cos_theta + n.x * sin_theta;
+    e.dy = d.y * cos_theta + n.y * sin_theta;
+    e.dz = d.z * cos_theta + n.z * sin_theta;
+    if (e.E < 200)
+        e.E -= min_ref(50e-3f, m.phonon_loss);
+    else
+        e.E -= m.recoil_const * (1 - cos_theta) * e.E;
+}
+
+// kieft_inelastic<all options>::execute (physics/kieft/inelastic.h:69-206).
+// Returns true and fills *se when a secondary is created.
+__device__ __forceinline__ bool inelastic(const Material& m, Electron& e, const float u[6], Electron* se) {
+    const float K = e.E;
+    const float omega0 = expf(table2d_get(m.in_icdf, logf(K), u[0]));
+    float binding = table2d_rounddown(m.ion, logf(omega0), u[1]);
+    float omega;
+    {
+        const float omega_max = 0.5f * (K + omega0 - m.fermi);
+        float omega_min = omega0;
+        float w0 = min_ref(omega0 - 1, max_ref(0, binding) - m.fermi);
+        if (K > 2 * omega0) {
+            omega_min = 0.5f * (K + omega0 - sqrtf(K * (K - 2 * omega0)));
+            w0 = omega0;
+        }
+        const float U = u[2];
+        if ((w0 > 0) && (omega_min > w0) && (omega_min < omega_max)) {
+            const float f_min = 1 / w0 * logf((omega_min - w0) / omega_min);
+            const float f_max = 1 / w0 * logf((omega_max - w0) / omega_max);
+            omega = -w0 / expm1f(w0 * (f_min * (1 - U) + f_max * U));
+        } else {
+            omega = omega0 * omega_max / (omega0 * (1 - U) + omega_max * U);
+        }
+    }
+    if (binding < 0) {
+        if (m.band_gap < 0) {
+            // metals: no special treatment
+        } else if (omega0 > m.band_gap) {
+            binding = m.band_gap;
+        } else {
+            e.E -= omega0;
+            return false;
+        }
+    }
+    binding = max_ref(0, binding);
+
+    const V3 d = normalised(V3{e.dx, e.dy, e.dz});
+    const V3 n = normalised(make_normal_vec(d, (2 * kPi) * u[3]));
+    const float Kp = e.E - m.fermi + 2 * binding;
+    const float dK = binding + omega;
+    const float cos_theta = sqrtf(dK / Kp);
+    const float sin_theta = sqrtf(1 - clampr(cos_theta * cos_theta, 0, 1));
+    V3 s{d.x * cos_theta + n.x * sin_theta, d.y * cos_theta + n.y * sin_theta, d.z * cos_theta + n.z * sin_theta};
+    s = normalised(s);
+    {
+        const V3 uv = make_unit_vec(2 * u[4] - 1, (2 * kPi) * u[5]);
+        const float a = sqrtf(binding / dK);
+        s.x += a * uv.x;
+        s.y += a * uv.y;
+        s.z += a * uv.z;
+    }
+    s = normalised(s);
+
+    se->px = e.px;
+    se->py = e.py;
+    se->pz = e.pz;
+    se->dx = s.x;
+    se->dy = s.y;
+    se->dz = s.z;
+    se->E = m.fermi + omega - binding;
+    se->mat = e.mat;
+    se->last_tri = -1;
+    se->tag = e.tag;
+    se->uid = secondary_uid(e.uid, e.step);
+    se->step = 0;
+
+    e.E -= omega;
+    e.dx = d.x - cos_theta * s.x;
+    e.dy = d.y - cos_theta * s.y;
+    e.dz = d.z - cos_theta * s.z;
+    return true;
+}
+
+// boundary_intersect<quantum transmission, refraction, no absorption>::execute
+// (physics/boundary_intersect.h:40-156)
+__device__ __forceinline__ int boundary(const Physics& P, Electron& e, float u) {
+    V3 r0, e1, e2;
+    int mi, mo;
+    load_tri(P.geo, e.last_tri, r0, e1, e2, mi, mo);
+    const V3 nd = normalised(V3{e.dx, e.dy, e.dz});
+    const V3 n = normalised(cross(e1, e2));
+    const float cos_theta = dot(n, nd);
+    int in, out;
+    if (cos_theta > 0) {
+        in = mi;
+        out = mo;
+    } else {
+        in = mo;
+        out = mi;
+    }
+    switch (out) {
+    case kDetector:
+        return kDetected;
+    case kDetectorLT50:
+        return e.E < 50 ? kDetected : kAlive;
+    case kDetectorGE50:
+        return e.E >= 50 ? kDetected : kAlive;
+    case kTerminator:
+        return kTerminated;
+    case kMirror:
+        e.dx = nd.x - 2 * n.x * cos_theta;
+        e.dy = nd.y - 2 * n.y * cos_theta;
+        e.dz = nd.z - 2 * n.z * cos_theta;
+        return kAlive;
+    case kNop:
+        return kAlive;
+    default:
+        break;
+    }
+    float dU = 0;
+    if (in >= 0) dU -= P.mat[in].barrier;
+    if (out >= 0) dU += P.mat[out].barrier;
+    if (e.E * cos_theta * cos_theta + dU > 0) {
+        const float s = sqrtf(1 + dU / (e.E * cos_theta * cos_theta));
+        const float T = 4 * s / ((1 + s) * (1 + s));
+        if (u < T) {
+            e.dx = (nd.x - n.x * cos_theta) + s * n.x * cos_theta;
+            e.dy = (nd.y - n.y * cos_theta) + s * n.y * cos_theta;
+            e.dz = (nd.z - n.z * cos_theta) + s * n.z * cos_theta;
+            e.E += dU;
+            e.mat = out;
+            return kAlive;
+        }
+    }
+    e.dx = nd.x - 2 * n.x * cos_theta;
+    e.dy = nd.y - 2 * n.y * cos_theta;
+    e.dz = nd.z - 2 * n.z * cos_theta;
+    return kAlive;
+}
+
+// One pass of init -> intersect -> scatter (drivers/cpu/cpu_driver.inl:73-161,
+// cpu_particle_manager.inl:214-235).  Uniforms: block 0 of the step's Philox
+// stream feeds the two free paths and the first two event draws; block 1 the
+// remaining four inelastic draws.
+__device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, Electron* se, bool* has_se) {
+    *event = kEvNone;
+    *has_se = false;
+    if (!in_domain(P.geo, V3{e.px, e.py, e.pz})) return kTerminated;
+    const uint4 r0 = draw(P.seed, e, 0);
+    int type = 0;
+    float dist = P.geo.max_extent;
+    if (e.mat >= 0) {
+        const Material& m = P.mat[e.mat];
+        if (e.E < m.barrier + P.min_energy || e.E > m.barrier + P.max_energy) return kTerminated;
+        const float logE = logf(e.E);
+        dist = __int_as_float(0x7f800000);
+        {
+            const float imfp = expf(table1d_get(m.in_imfp, logE));
+            const float path = -(1 / imfp) * logf(u01(r0.x));
+            if (path < dist) {
+                type = 1;
+                dist = path;
+            }
+        }
+        {
+            const float imfp = expf(table1d_get(m.el_imfp, logE));
+            const float path = -(1 / imfp) * logf(u01(r0.y));
+            if (path < dist) {
+                type = 2;
+                dist = path;
+            }
+        }
+    }
+    const V3 nd = normalised(V3{e.dx, e.dy, e.dz});
+    int hit;
+    const float tdist = propagate(P.geo, V3{e.px, e.py, e.pz}, nd, dist, e.last_tri, e.mat, &hit);
+    int status = kAlive;
+    if (hit < 0) {
+        e.px += nd.x * dist;
+        e.py += nd.y * dist;
+        e.pz += nd.z * dist;
+        if (type == 2) {
+            e.last_tri = -1;
+            elastic(P.mat[e.mat], e, u01(r0.z), u01(r0.w));
+            *event = kEvElastic;
+        } else if (type == 1) {
+            e.last_tri = -1;
+            const uint4 r1 = draw(P.seed, e, 1);
+            const float u[6] = {u01(r0.z), u01(r0.w), u01(r1.x), u01(r1.y), u01(r1.z), u01(r1.w)};
+            *has_se = inelastic(P.mat[e.mat], e, u, se);
+            *event = kEvInelastic;
+        }
+    } else {
+        e.px += nd.x * tdist;
+        e.py += nd.y * tdist;
+        e.pz += nd.z * tdist;
+        e.last_tri = hit;
+        status = boundary(P, e, u01(r0.z));
+        *event = kEvBoundary;
+    }
+    e.step += 1;
+    return status;
+}
+
+}  // namespace dev
+}  // namespace nbx

@@ -1,0 +1,356 @@
+"""Seeded synthetic inputs in Nebula's formats.
+
+Real cstool ``.mat`` files and measured SEM data are not available, so the
+workloads are built from:
+
+* a synthetic material generator that writes the Kieft & Bosch groups read by
+  ``source/physics/kieft/elastic.h:120-166`` and
+  ``source/physics/kieft/inelastic.h:212-327`` (screened-Rutherford elastic
+  scattering blended into a constant acoustic-phonon mean free path below
+  100 eV, and a single-pole Drude energy-loss function for the dielectric
+  inelastic model), in the reference ``.mat`` HDF5 layout;
+* geometry generators (cube, line-space grating, rough surface) writing the
+  ``.tri`` triangle format;
+* primary-beam generators writing ``.pri`` records, drawn from numpy's
+  Philox bit generator.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import formats
+from .h5mat import MatFile
+
+A0_NM = 0.0529177210903          # Bohr radius (nm)
+E2_EVNM = 1.439964547            # e^2 / (4 pi eps0) in eV nm
+MEC2_EV = 510998.95              # electron rest energy (eV)
+AMU_G = 1.66053906660e-24        # atomic mass unit in grams
+
+
+# ----------------------------------------------------------------------------
+# Materials
+# ----------------------------------------------------------------------------
+def _geomspace(first, last, n):
+    """Axis values exactly as ``util::geomspace`` reconstructs them
+    (``source/common/util/range.h:271-310``): first * exp(i * step)."""
+    step = math.log(last / first) / (n - 1)
+    return np.array([first * math.exp(i * step) for i in range(n)], np.float64)
+
+
+def _linspace(first, last, n):
+    step = (last - first) / (n - 1)
+    return np.array([first + i * step for i in range(n)], np.float64)
+
+
+def screening_eta(E, Z):
+    """Nigam screening parameter of the screened-Rutherford cross section."""
+    tau = E / MEC2_EV
+    return 1.7e-5 * Z ** (2.0 / 3.0) / (tau * (tau + 2.0))
+
+
+def elastic_imfp(E, Z, n_atoms, phonon_imfp):
+    """Elastic inverse mean free path (nm^-1).
+
+    Screened Rutherford above 200 eV, a constant acoustic-phonon value below
+    100 eV, and log-log interpolation in between (the Kieft & Bosch blend)."""
+    E = np.asarray(E, np.float64)
+    eta = screening_eta(E, Z)
+    sigma = math.pi * (Z * E2_EVNM) ** 2 / (4.0 * E * E * eta * (1.0 + eta))
+    sr = n_atoms * sigma
+    out = np.where(E >= 200.0, sr, phonon_imfp)
+    mid = (E > 100.0) & (E < 200.0)
+    if np.any(mid):
+        sr200 = n_atoms * math.pi * (Z * E2_EVNM) ** 2 / (4.0 * 200.0 ** 2 * screening_eta(200.0, Z) * (1 + screening_eta(200.0, Z)))
+        t = np.log(E[mid] / 100.0) / math.log(2.0)
+        out[mid] = np.exp((1 - t) * math.log(phonon_imfp) + t * math.log(sr200))
+    return out
+
+
+def elastic_icdf(E, P, Z):
+    """cos(theta) inverse CDF of the screened-Rutherford distribution."""
+    eta = screening_eta(np.asarray(E, np.float64), Z)[:, None]
+    P = np.asarray(P, np.float64)[None, :]
+    return 1.0 + 2.0 * eta - 2.0 * eta * (1.0 + eta) / (P + eta)
+
+
+def drude_elf(w, wp, gamma):
+    """Single-pole Drude energy-loss function Im(-1/eps(w))."""
+    return gamma * w * wp * wp / ((wp * wp - w * w) ** 2 + (gamma * w) ** 2)
+
+
+def inelastic_tables(K, P, wp, gamma, fermi, w_lo, scale):
+    """Dielectric IMFP (nm^-1) and omega' inverse CDF (eV) for every energy.
+
+    dIMFP/dw = ELF(w) / (pi a0 K) * ln[(1 + sqrt(1 - w/K)) / (1 - sqrt(1 - w/K))]
+    for w between ``w_lo`` and ``K - fermi``."""
+    nK, nP = len(K), len(P)
+    imfp = np.full(nK, 1e-30)
+    icdf = np.full((nK, nP), w_lo)
+    for i, k in enumerate(K):
+        wmax = k - fermi
+        if wmax <= w_lo * 1.0001:
+            continue
+        w = np.geomspace(w_lo, wmax, 4001)
+        x = np.clip(w / k, 0.0, 1.0)
+        s = np.sqrt(1.0 - x)
+        with np.errstate(divide="ignore"):
+            lg = np.log((1.0 + s) / np.maximum(1.0 - s, 1e-300))
+        f = drude_elf(w, wp, gamma) / (math.pi * A0_NM * k) * lg * scale
+        cum = np.concatenate([[0.0], np.cumsum(0.5 * (f[1:] + f[:-1]) * np.diff(w))])
+        if cum[-1] <= 0:
+            continue
+        imfp[i] = max(cum[-1], 1e-30)
+        cdf = cum / cum[-1]
+        icdf[i] = np.interp(P, cdf, w)
+        icdf[i, 0] = w_lo
+        icdf[i, -1] = wmax
+    return imfp, icdf
+
+
+MATERIALS = {
+    # name: (Z, atoms/nm^3, A [u], hbar*w_p, gamma, fermi, work function, band gap, phonon loss, density factor)
+    "si": (14, 49.94, 28.0855, 16.7, 4.0, 7.8, 4.8, 1.12, 0.063, 1.0),
+    "sio2": (10, 66.3, 20.03, 22.0, 4.0, 7.8, 4.8, 9.0, 0.063, 1.0),
+    "w": (74, 63.2, 183.84, 25.0, 4.0, 7.8, 4.8, -1.0, 0.063, 8.1),
+}
+
+
+def make_material(path, kind="si", nK=128, nP=256, Kmin=1.0, Kmax=1.0e4, seed=0):
+    """Write a synthetic ``.mat`` file for one of ``MATERIALS``.
+
+    The energy axis is written as the exact ``geomspace`` values the reader
+    reconstructs, so the logarithmic-spacing check of
+    ``source/io/hdf5_file.cpp:345-351`` passes.  ``seed`` is recorded in the
+    file; the tables themselves are deterministic functions of the model
+    parameters."""
+    Z, n_at, A, wp, gam, fermi, wf, gap, phonon, dens = MATERIALS[kind]
+    K = _geomspace(Kmin, Kmax, nK)
+    P = _linspace(0.0, 1.0, nP)
+
+    m = MatFile()
+    m.set_property_string("name", {"si": "Si-like", "sio2": "SiO2-like", "w": "W-like"}[kind])
+    m.set_property_string("cstool_version", "nbx-synthetic-1 (seed %d)" % seed)
+    m.set_property_quantity("fermi", fermi, "eV")
+    m.set_property_quantity("work_function", wf, "eV")
+    m.set_property_quantity("barrier", fermi + wf, "eV")
+    if gap >= 0:
+        m.set_property_quantity("band_gap", gap, "eV")
+    m.set_property_quantity("phonon_loss", phonon, "eV")
+    m.set_property_quantity("effective_A", A * AMU_G, "g")
+    m.set_property_quantity("density", n_at * dens * A * AMU_G * 1e21, "g/cm^3")
+
+    # Elastic --------------------------------------------------------------
+    g = m.group("/kieft/elastic")
+    k_el = g.dataset("energy", K, units="eV")
+    p_el = g.dataset("probability", P, units="")
+    imfp_el = elastic_imfp(K, Z, n_at * dens, phonon_imfp=1.0 * dens)
+    d = g.dataset("imfp", (imfp_el * 1e9).astype(np.float32), units="m^-1")   # stored in m^-1
+    d.attach_scale(0, k_el)
+    d = g.dataset("costheta_icdf", elastic_icdf(K, P, Z).astype(np.float32), units="")
+    d.attach_scale(0, k_el)
+    d.attach_scale(1, p_el)
+
+    # Inelastic ------------------------------------------------------------
+    g = m.group("/kieft/inelastic")
+    k_in = g.dataset("energy", K, units="eV")
+    p_in = g.dataset("probability", P, units="")
+    imfp_in, w0 = inelastic_tables(K, P, wp, gam, fermi, w_lo=0.1, scale=dens)
+    d = g.dataset("imfp", imfp_in.astype(np.float32), units="nm^-1")
+    d.attach_scale(0, k_in)
+    d = g.dataset("w0_icdf", w0.astype(np.float32), units="eV")
+    d.attach_scale(0, k_in)
+    d.attach_scale(1, p_in)
+
+    # Ionization -------------------------------------------------------------
+    g = m.group("/kieft/ionization")
+    k_io = g.dataset("energy", K, units="eV")
+    p_io = g.dataset("probability", P, units="")
+    binding = np.zeros((nK, nP), np.float32)
+    binding[:, :] = 5.0                               # valence: < 50 eV
+    binding[np.ix_(K > 150.0, P >= 0.97)] = 99.8      # an inner shell
+    d = g.dataset("binding_icdf", binding, units="eV")
+    d.attach_scale(0, k_io)
+    d.attach_scale(1, p_io)
+    g.dataset("outer_shells", np.array([100.0, 149.7, 1839.0]), units="eV")
+
+    m.write(path)
+    return path
+
+
+# ----------------------------------------------------------------------------
+# Geometry
+# ----------------------------------------------------------------------------
+class TriBuilder:
+    def __init__(self):
+        self.rows = []
+
+    def tri(self, a, b, c, mat_in, mat_out):
+        self.rows.append((mat_in, mat_out, (a, b, c)))
+
+    def quad(self, a, b, c, d, mat_in, mat_out):
+        """Quad a-b-c-d counter-clockwise seen from the ``mat_out`` side."""
+        self.tri(a, b, c, mat_in, mat_out)
+        self.tri(a, c, d, mat_in, mat_out)
+
+    def box(self, lo, hi, mat_in, mat_out):
+        x0, y0, z0 = lo
+        x1, y1, z1 = hi
+        q = self.quad
+        q((x0, y0, z1), (x1, y0, z1), (x1, y1, z1), (x0, y1, z1), mat_in, mat_out)  # +z
+        q((x0, y0, z0), (x0, y1, z0), (x1, y1, z0), (x1, y0, z0), mat_in, mat_out)  # -z
+        q((x1, y0, z0), (x1, y1, z0), (x1, y1, z1), (x1, y0, z1), mat_in, mat_out)  # +x
+        q((x0, y0, z0), (x0, y0, z1), (x0, y1, z1), (x0, y1, z0), mat_in, mat_out)  # -x
+        q((x0, y1, z0), (x0, y1, z1), (x1, y1, z1), (x1, y1, z0), mat_in, mat_out)  # +y
+        q((x0, y0, z0), (x1, y0, z0), (x1, y0, z1), (x0, y0, z1), mat_in, mat_out)  # -y
+
+    def array(self):
+        out = np.zeros(len(self.rows), formats.TRI_DTYPE)
+        for i, (a, b, (p, q, r)) in enumerate(self.rows):
+            out[i]["mat_in"] = a
+            out[i]["mat_out"] = b
+            out[i]["v"] = np.array([p, q, r], np.float64).astype(np.float32)
+        return out
+
+
+def cube_geometry(size=(2000.0, 2000.0, 1000.0), detector_z=10.0, detector_margin=100.0):
+    """Axis-aligned block of material 0 with its top face at z=0, vacuum
+    around it, and a two-triangle DETECTOR plane above it."""
+    sx, sy, sz = size
+    b = TriBuilder()
+    b.box((-sx / 2, -sy / 2, -sz), (sx / 2, sy / 2, 0.0), 0, formats.VACUUM)
+    m = detector_margin
+    b.quad((-sx / 2 - m, -sy / 2 - m, detector_z), (sx / 2 + m, -sy / 2 - m, detector_z),
+           (sx / 2 + m, sy / 2 + m, detector_z), (-sx / 2 - m, sy / 2 + m, detector_z),
+           formats.DETECTOR, formats.DETECTOR)
+    return b.array()
+
+
+def grating_geometry(width=32.0, pitch=64.0, height=50.0, length=2000.0, n_lines=31,
+                     depth=1000.0, segment=100.0, detector_z=100.0):
+    """Line-space grating: lines along y on a substrate of the same material.
+
+    The solid's outer surface is emitted directly (line tops, trench floors,
+    side walls, end faces, substrate sides and bottom); the faces along y are
+    split into ``segment``-long pieces (about 5k triangles with the defaults).
+    """
+    b = TriBuilder()
+    half = n_lines * pitch / 2.0
+    xs = [(-half + i * pitch + (pitch - width) / 2, -half + i * pitch + (pitch + width) / 2) for i in range(n_lines)]
+    y0, y1 = -length / 2, length / 2
+    ny = max(1, int(round(length / segment)))
+    ys = np.linspace(y0, y1, ny + 1)
+    V = formats.VACUUM
+    # Profile along x: list of (x_start, x_end, z)
+    prof = []
+    xcur = -half
+    for (a, c) in xs:
+        if a > xcur:
+            prof.append((xcur, a, 0.0))
+        prof.append((a, c, height))
+        xcur = c
+    if xcur < half:
+        prof.append((xcur, half, 0.0))
+    for j in range(ny):
+        ya, yb = ys[j], ys[j + 1]
+        for (a, c, z) in prof:
+            b.quad((a, ya, z), (c, ya, z), (c, yb, z), (a, yb, z), 0, V)     # top (+z)
+        for (a, c) in xs:
+            b.quad((a, ya, 0.0), (a, ya, height), (a, yb, height), (a, yb, 0.0), 0, V)   # -x wall
+            b.quad((c, ya, 0.0), (c, yb, 0.0), (c, yb, height), (c, ya, height), 0, V)   # +x wall
+    # substrate block sides (z from -depth to 0) and bottom
+    b.quad((-half, y0, -depth), (-half, y1, -depth), (half, y1, -depth), (half, y0, -depth), 0, V)   # bottom
+    b.quad((half, y0, -depth), (half, y1, -depth), (half, y1, 0.0), (half, y0, 0.0), 0, V)          # +x
+    b.quad((-half, y0, -depth), (-half, y0, 0.0), (-half, y1, 0.0), (-half, y1, -depth), 0, V)      # -x
+    b.quad((-half, y1, -depth), (-half, y1, 0.0), (half, y1, 0.0), (half, y1, -depth), 0, V)        # +y
+    b.quad((-half, y0, -depth), (half, y0, -depth), (half, y0, 0.0), (-half, y0, 0.0), 0, V)        # -y
+    # line end caps at y = +-length/2
+    for (a, c) in xs:
+        b.quad((a, y1, 0.0), (a, y1, height), (c, y1, height), (c, y1, 0.0), 0, V)   # +y
+        b.quad((a, y0, 0.0), (c, y0, 0.0), (c, y0, height), (a, y0, height), 0, V)   # -y
+    m = 50.0
+    b.quad((-half - m, y0 - m, detector_z), (half + m, y0 - m, detector_z),
+           (half + m, y1 + m, detector_z), (-half - m, y1 + m, detector_z),
+           formats.DETECTOR, formats.DETECTOR)
+    return b.array()
+
+
+def rough_geometry(n=512, size=1000.0, rms=3.0, corr=10.0, depth=1000.0, seed=0, detector_z=50.0):
+    """Slab whose top surface is a seeded Gaussian random height field
+    (``n`` x ``n`` samples, RMS ``rms`` nm, correlation length ``corr`` nm)."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    h = rng.standard_normal((n, n))
+    dx = size / (n - 1)
+    k = np.fft.fftfreq(n, d=dx)
+    kk = k[:, None] ** 2 + k[None, :] ** 2
+    filt = np.exp(-(math.pi ** 2) * corr ** 2 * kk / 2.0)
+    h = np.real(np.fft.ifft2(np.fft.fft2(h) * filt))
+    h *= rms / h.std()
+    xs = np.linspace(-size / 2, size / 2, n)
+    V = formats.VACUUM
+    rows = []
+    X, Y = np.meshgrid(xs, xs, indexing="ij")
+    P = np.stack([X, Y, h], -1).astype(np.float32)
+    a = P[:-1, :-1].reshape(-1, 3)
+    b_ = P[1:, :-1].reshape(-1, 3)
+    c = P[1:, 1:].reshape(-1, 3)
+    d = P[:-1, 1:].reshape(-1, 3)
+    top = np.zeros(2 * a.shape[0], formats.TRI_DTYPE)
+    top["mat_in"] = 0
+    top["mat_out"] = V
+    top["v"][0::2] = np.stack([a, b_, c], 1)
+    top["v"][1::2] = np.stack([a, c, d], 1)
+    b = TriBuilder()
+    lo, hi = -size / 2, size / 2
+    b.quad((lo, lo, -depth), (lo, hi, -depth), (hi, hi, -depth), (hi, lo, -depth), 0, V)
+    # side walls follow the height profile along each edge
+    for i in range(n - 1):
+        x0, x1 = xs[i], xs[i + 1]
+        b.quad((x0, lo, -depth), (x1, lo, -depth), (x1, lo, h[i + 1, 0]), (x0, lo, h[i, 0]), 0, V)
+        b.quad((x0, hi, -depth), (x0, hi, h[i, -1]), (x1, hi, h[i + 1, -1]), (x1, hi, -depth), 0, V)
+        b.quad((lo, x0, -depth), (lo, x0, h[0, i]), (lo, x1, h[0, i + 1]), (lo, x1, -depth), 0, V)
+        b.quad((hi, x0, -depth), (hi, x1, -depth), (hi, x1, h[-1, i + 1]), (hi, x0, h[-1, i]), 0, V)
+    m = 20.0
+    b.quad((lo - m, lo - m, detector_z), (hi + m, lo - m, detector_z), (hi + m, hi + m, detector_z),
+           (lo - m, hi + m, detector_z), formats.DETECTOR, formats.DETECTOR)
+    return np.concatenate([top, b.array()])
+
+
+# ----------------------------------------------------------------------------
+# Primaries
+# ----------------------------------------------------------------------------
+def point_beam(n, energy, pos=(0.0, 0.0, 1.0), direction=(0.0, 0.0, -1.0), pixel=(0, 0)):
+    r = np.zeros(n, formats.RECORD_DTYPE)
+    r["pos"] = pos
+    r["dir"] = direction
+    r["E"] = energy
+    r["px"] = pixel[0]
+    r["py"] = pixel[1]
+    return r
+
+
+def scan_beam(nx, ny, per_pixel, energy, spacing=1.0, origin=(-128.0, -128.0), z_start=75.0,
+              sigma=1.0, divergence_deg=0.5, seed=0, energies=None, rows=None):
+    """Raster scan: ``per_pixel`` primaries per pixel, Gaussian spot focused at
+    z=0 (``sigma`` nm) with Gaussian angular divergence, starting at
+    ``z_start``.  If ``energies`` is given, each primary's energy is drawn
+    uniformly from that list.  ``rows`` restricts the scan to those y rows."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    rows = range(ny) if rows is None else rows
+    py, px = np.meshgrid(np.asarray(list(rows)), np.arange(nx), indexing="ij")
+    px = np.repeat(px.ravel(), per_pixel)
+    py = np.repeat(py.ravel(), per_pixel)
+    n = px.size
+    cx = origin[0] + px * spacing + rng.normal(0.0, sigma, n)
+    cy = origin[1] + py * spacing + rng.normal(0.0, sigma, n)
+    div = math.radians(divergence_deg)
+    tx = np.tan(rng.normal(0.0, div, n))
+    ty = np.tan(rng.normal(0.0, div, n))
+    dirs = np.stack([tx, ty, -np.ones(n)], 1)
+    pos = np.stack([cx - tx * z_start, cy - ty * z_start, np.full(n, z_start)], 1)
+    if energies is None:
+        E = np.full(n, energy)
+    else:
+        E = np.asarray(energies, np.float64)[rng.integers(0, len(energies), n)]
+    return formats.make_records(pos, dirs, E, px, py)

@@ -1,0 +1,43 @@
+"""Generate tests/golden/golden.json from the reference's own CPU code.
+
+Run in an environment where oracle/_ref/libnbref.so has been built from the
+reference source tree (oracle/Makefile).  The vectors are outputs of the
+reference's octree<false>::propagate on the synthetic cube geometry of
+nebula_b200.generators.cube_geometry(), so tests can check the oracle and
+the kernels against them where the reference is not available."""
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+import oracle  # noqa: E402
+from nebula_b200 import generators as g  # noqa: E402
+
+
+def main():
+    rng = np.random.default_rng(2024)
+    tris = g.cube_geometry()
+    rg = oracle.RefGeometry(tris)
+    n = 256
+    pos = (rg.aabb_min + (rg.aabb_max - rg.aabb_min) * rng.random((n, 3))).astype(np.float32)
+    pos[: n // 2, 2] = rng.normal(0, 20, n // 2).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    d = d.astype(np.float32)
+    dist = rng.exponential(200.0, n).astype(np.float32)
+    ign = np.full(n, -1, np.int32)
+    imat = rng.choice(np.array([-123, 0], np.int32), n)
+    od, ot = rg.propagate(pos, d, dist, ign, imat)
+    out = {"cube_rays": {"pos": pos.tolist(), "dir": d.tolist(), "dist": dist.tolist(), "ignore_tri": ign.tolist(),
+                         "ignore_mat": imat.tolist(), "tri": ot.tolist(),
+                         "dist_bits": od.view(np.uint32).tolist()}}
+    with open(os.path.join(HERE, "golden.json"), "w") as f:
+        json.dump(out, f)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,66 @@
+"""The C-ABI library: it loads without a GPU, exports every entry point that
+include/nbx.h declares, and reports errors by code instead of crashing."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import nebula_b200 as nb
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "nbx.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(nbx_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_exports_every_declared_symbol():
+    syms = declared_symbols()
+    assert len(syms) >= 30
+    out = subprocess.run(["nm", "-D", "--defined-only", nb.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(l.split()[-1] for l in out.splitlines() if l.strip())
+    missing = [s for s in syms if s not in exported]
+    assert not missing, missing
+    L = nb.lib()
+    for s in syms:
+        assert getattr(L, s) is not None
+
+
+def test_version_and_errors():
+    L = nb.lib()
+    a, b, c = C.c_int(), C.c_int(), C.c_int()
+    assert L.nbx_version(C.byref(a), C.byref(b), C.byref(c)) == 0
+    assert (a.value, b.value, c.value) == (1, 0, 2)
+    assert L.nbx_error_string(-8) == b"device queue overflow"
+    assert L.nbx_load_tri(None, None, None) == -1
+
+
+def test_create_without_device_reports_nodev():
+    if nb.device_count() > 0:
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(nb.NbxError) as e:
+        nb.Context()
+    assert e.value.code == -7
+
+
+def test_host_calls_without_device(inputs):
+    tris = nb.triangles_from_tri_array(inputs["cube"])
+    o = nb.HostOctree(tris)
+    assert o.octree_data[:8].tolist() != [0] * 8
+    m = nb.HostMaterial(inputs["si"])
+    assert m.max_energy > 9999
+
+
+def test_cli_usage_and_errors(tmp_path):
+    cli = os.path.join(ROOT, "nebula_b200", "nebula_b200")
+    if not os.path.exists(cli):
+        pytest.skip("CLI not built")
+    r = subprocess.run([cli], capture_output=True, text=True)
+    assert r.returncode == 1 and "Usage" in r.stderr
+    r = subprocess.run([cli, "--bogus=1", "a", "b", "c"], capture_output=True, text=True)
+    assert r.returncode != 0

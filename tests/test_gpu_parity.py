@@ -1,0 +1,289 @@
+"""GPU parity: the sm_100a kernels against the oracle, through the C ABI.
+
+* Philox4x32-10 blocks: bit-exact against the C restatement and the published
+  known-answer vectors.
+* Octree ray queries: bit-exact (same triangle, same float distance) against
+  the reference's own octree<false>::propagate on fixed ray batches over
+  several geometries.
+* Table lookups: bit-exact against the reference's table_1D/2D::get and
+  get_rounddown, with the reference loader's tables.
+* Single transport steps: against the C restatement fed the same Philox
+  uniforms; geometry-only steps bit-exact, physics steps within a tolerance
+  that absorbs last-bit differences of CUDA's and glibc's transcendentals.
+* Whole runs: SE/BSE yields and exit-energy spectra of the GPU path against the
+  reference CPU path (cpu_mt_main-style driver) within 3 sigma / chi-square.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+import nebula_b200 as nb
+from nebula_b200 import formats, generators as g
+
+pytestmark = pytest.mark.gpu
+
+KAT = [  # Random123 known-answer vectors for philox4x32-10: counter, key, result
+    ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+    ((0xFFFFFFFF,) * 4, (0xFFFFFFFF,) * 2, (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+    ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+     (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+]
+
+
+@pytest.fixture(scope="module")
+def ctx_grating(inputs, oracle_built):
+    return nb.setup(inputs["grating"], [inputs["si"]], device=0)
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def test_philox_kat_and_oracle(ctx_grating):
+    ctr = np.array([k[0] for k in KAT], np.uint32)
+    key = np.array([k[1] for k in KAT], np.uint32)
+    out = ctx_grating.philox(ctr, key)
+    assert np.array_equal(out, np.array([k[2] for k in KAT], np.uint32))
+    rng = np.random.default_rng(0)
+    ctr = rng.integers(0, 2 ** 32, (4096, 4), dtype=np.uint64).astype(np.uint32)
+    key = rng.integers(0, 2 ** 32, (4096, 2), dtype=np.uint64).astype(np.uint32)
+    out = ctx_grating.philox(ctr, key)
+    ref = np.array([oracle.philox(c, k) for c, k in zip(ctr, key)], np.uint32)
+    assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("geom", ["cube", "grating", "rough"])
+def test_ray_query_bit_exact_vs_reference(inputs, oracle_built, ray_sampler, geom):
+    tris = inputs[geom]
+    ctx = nb.setup(tris, [inputs["si"]], device=0)
+    rg = oracle.RefGeometry(tris)
+    for seed in range(3):
+        n = 50000
+        pos, d, dist = ray_sampler(rg.aabb_min, rg.aabb_max, n, seed)
+        rng = np.random.default_rng(100 + seed)
+        ign = np.full(n, -1, np.int32)
+        ntri = len(ctx.octree.triangles)
+        ign[::4] = rng.integers(0, ntri, len(ign[::4]))
+        imat = rng.choice(np.array([-123, 0, -126], np.int32), n)
+        gd, gt = ctx.ray_query(pos, d, dist, ign, imat)
+        rd, rt = rg.propagate(pos, d, dist, ign, imat)
+        assert np.array_equal(gt, rt), "triangle ids differ at %s" % np.nonzero(gt != rt)[0][:10]
+        assert np.array_equal(_bits(gd), _bits(rd)), "distances differ"
+        assert (gt >= 0).sum() > n // 20
+    ctx.close()
+
+
+def test_ray_query_edge_cases(inputs, oracle_built):
+    """Empty batch; rays from outside the domain; zero-length; rays along cell planes."""
+    tris = inputs["cube"]
+    ctx = nb.setup(tris, [inputs["si"]], device=0)
+    rg = oracle.RefGeometry(tris)
+    e = np.zeros((0, 3), np.float32)
+    od, ot = ctx.ray_query(e, e, np.zeros(0, np.float32), np.zeros(0, np.int32), np.zeros(0, np.int32))
+    assert len(od) == 0 and len(ot) == 0
+    pos = np.array([[0, 0, 5], [0, 0, 5], [0, 0, -500], [0, 0, 0], [1100, 0, 5], [0, 0, 1.0], [3000, 0, 0]],
+                   np.float32)
+    d = np.array([[0, 0, -1], [0, 0, 1], [1, 0, 0], [0, 1, 0], [-1, 0, 0], [0, 0, -1], [-1, 0, 0]], np.float32)
+    dist = np.array([100, 100, 1e9, 5, 1e9, 0.0, 10.0], np.float32)
+    ign = np.full(len(dist), -1, np.int32)
+    imat = np.array([-123, -123, 0, 0, -123, -123, -123], np.int32)
+    gd, gt = ctx.ray_query(pos, d, dist, ign, imat)
+    rd, rt = rg.propagate(pos, d, dist, ign, imat)
+    assert np.array_equal(gt, rt)
+    assert np.array_equal(_bits(gd), _bits(rd))
+    ctx.close()
+
+
+@pytest.mark.parametrize("mat", ["si", "sio2", "w"])
+def test_table_query_bit_exact_vs_reference(inputs, oracle_built, mat):
+    ctx = nb.setup(inputs["cube"], [inputs[mat]], device=0)
+    rm = oracle.RefMaterial(inputs[mat])
+    rng = np.random.default_rng(3)
+    n = 100000
+    # log energies across and beyond the table (extrapolation), uniforms from Philox
+    x = rng.uniform(-1.0, 10.5, n).astype(np.float32)
+    ctr = np.stack([np.arange(n), np.zeros(n), np.full(n, 7), np.zeros(n)], 1).astype(np.uint32)
+    bits = ctx.philox(ctr, np.tile(np.array([[1234, 0]], np.uint32), (n, 1)))[:, 0]
+    y = ((bits >> 9).astype(np.float32) * np.float32(1.1920928955078125e-07) + np.float32(5.9604644775390625e-08))
+    y = y.astype(np.float32)
+    for name in ("el_imfp", "in_imfp", "el_icdf", "in_icdf", "ion"):
+        gv = ctx.table_query(0, name, x, y)
+        rv = rm.eval(name, x, y)
+        assert np.array_equal(_bits(gv), _bits(rv)), name
+    ctx.close()
+
+
+def _electrons_on(ctx, rng, n, region_lo, region_hi, mats):
+    e = np.zeros(n, nb.ELECTRON_DTYPE)
+    e["pos"] = region_lo + (region_hi - region_lo) * rng.random((n, 3))
+    d = rng.normal(size=(n, 3))
+    e["dir"] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    e["E"] = np.exp(rng.uniform(np.log(13.0), np.log(1500.0), n))
+    e["mat"] = rng.choice(mats, n)
+    e["last_tri"] = -1
+    e["tag"] = np.arange(n)
+    e["uid"] = rng.integers(0, 2 ** 62, n, dtype=np.uint64)
+    e["step"] = rng.integers(0, 1000, n)
+    return e
+
+
+def test_step_vs_restatement(inputs, oracle_built):
+    """One transport step per electron on the GPU and in the C restatement
+    (same Philox uniforms, same tables).  Vacuum steps (geometry only) are
+    bit-exact; material steps agree to float32 tolerance except where a
+    last-bit transcendental difference flips a discrete choice (rare)."""
+    tris = inputs["grating"]
+    ctx = nb.setup(tris, [inputs["si"]], device=0, seed=99)
+    pg = oracle.PortGeometry(tris)
+    rm = oracle.RefMaterial(inputs["si"])
+    pms, arr = oracle.port_materials([rm])
+    prm = oracle.Params(99, 0.0, rm.max_energy)
+    rng = np.random.default_rng(11)
+    n = 20000
+    lo = np.array([-200, -200, -50], np.float32)
+    hi = np.array([200, 200, 80], np.float32)
+    e0 = _electrons_on(ctx, rng, n, lo, hi, np.array([-123, 0], np.int32))
+    ge, gst, gev, gse, ghs = ctx.step_query(e0)
+    P = oracle.port()
+    close = 0
+    material_steps = 0
+    for i in range(n):
+        el = oracle.Electron()
+        C.memmove(C.byref(el), e0[i:i + 1].ctypes.data, 52)
+        el.uid = int(e0["uid"][i])
+        el.step = int(e0["step"][i])
+        ev = C.c_int()
+        hs = C.c_int()
+        se = oracle.Electron()
+        st = P.nbo_step(C.byref(pg.s), arr, C.byref(prm), C.byref(el), C.byref(ev), C.byref(se), C.byref(hs))
+        if e0["mat"][i] < 0:
+            assert st == gst[i] and ev.value == gev[i], i
+            assert np.array_equal(_bits(np.array(el.pos, np.float32)), _bits(ge["pos"][i])), i
+            continue
+        material_steps += 1
+        ok = (st == gst[i] and ev.value == gev[i] and hs.value == ghs[i]
+              and np.allclose(np.array(el.pos), ge["pos"][i], rtol=1e-4, atol=1e-4)
+              and np.allclose(np.array(el.dir), ge["dir"][i], rtol=1e-3, atol=1e-4)
+              and abs(el.E - ge["E"][i]) <= 1e-4 * max(1.0, abs(el.E)))
+        close += ok
+    assert material_steps > n // 3
+    assert close >= 0.999 * material_steps, (close, material_steps)
+    ctx.close()
+
+
+def _run_gpu(ctx, recs):
+    ctx.reset_tallies()
+    ctx.push_records(recs)
+    ctx.run()
+    se, bse = ctx.tag_counts(0, len(recs))
+    return ctx.stats(), se.astype(np.float64), bse.astype(np.float64)
+
+
+def _z(a, b):
+    return (a.mean() - b.mean()) / np.sqrt(a.var() / len(a) + b.var() / len(b))
+
+
+def _chi2_two_sample(h1, h2):
+    n1, n2 = h1.sum(), h2.sum()
+    m = (h1 + h2) > 0
+    k1, k2 = np.sqrt(n2 / n1), np.sqrt(n1 / n2)
+    chi2 = (((k1 * h1 - k2 * h2) ** 2) / (h1 + h2))[m].sum()
+    dof = m.sum() - 1
+    return chi2, dof
+
+
+def test_whole_run_vs_reference_cpu(inputs, oracle_built, tmp_path):
+    """Cube, 10^4 primaries at 1 keV (the reference's CPU-sized config):
+    per-primary SE/BSE yields within 3 sigma, exit-energy spectrum chi-square
+    within 3 sqrt(2 dof)."""
+    tri = inputs["cube_tri"]
+    recs = g.point_beam(10000, 1000.0, pos=(0.0, 0.0, 1.0))
+    pri = str(tmp_path / "c1.pri")
+    formats.write_pri(pri, recs)
+    ref_recs, st, _ = oracle.ref_run(tri, pri, [inputs["si"]], seed=1, count_events=True)
+    ctx = nb.setup(inputs["cube"], [inputs["si"]], device=0, seed=5, record_detected=True)
+    s, se, bse = _run_gpu(ctx, recs)
+    det = ctx.flush_detected()
+    # per-primary reference counts from the pixel-less records: use totals and
+    # binomial-like variance estimates from the GPU's per-primary spread
+    n = len(recs)
+    ref_se_total = (ref_recs["E"] < 50).sum()
+    ref_bse_total = (ref_recs["E"] >= 50).sum()
+    for total_ref, counts in ((ref_se_total, se), (ref_bse_total, bse)):
+        mean_g = counts.mean()
+        var = counts.var()
+        z = (mean_g - total_ref / n) / np.sqrt(2 * var / n)
+        assert abs(z) < 3, (mean_g, total_ref / n, z)
+    bins = np.concatenate([np.arange(0, 50, 2.0), np.arange(50, 1001, 50.0)])
+    h_g, _ = np.histogram(det["E"], bins)
+    h_r, _ = np.histogram(ref_recs["E"], bins)
+    chi2, dof = _chi2_two_sample(h_g.astype(float), h_r.astype(float))
+    assert abs(chi2 - dof) <= 3 * np.sqrt(2 * dof), (chi2, dof)
+    # events per primary within a few percent
+    ev_g = (s["events_elastic"] + s["events_inelastic"] + s["events_boundary"]) / n
+    ev_r = (st["n_intersect"] + st["n_elastic"] + st["n_inelastic"]) / n
+    assert abs(ev_g - ev_r) / ev_r < 0.05, (ev_g, ev_r)
+    ctx.close()
+
+
+def test_whole_run_grating_rows_vs_reference(inputs, oracle_built, tmp_path):
+    """Grating scan subsample (2 rows x 64 px x 20 primaries at 500 eV):
+    y-averaged cross-line SE/BSE profiles agree by chi-square."""
+    tri = inputs["grating_tri"]
+    recs = g.scan_beam(64, 2, 20, 500.0, origin=(-32.0, -1.0), seed=4)
+    pri = str(tmp_path / "c2.pri")
+    formats.write_pri(pri, recs)
+    ref_recs, st, _ = oracle.ref_run(tri, pri, [inputs["si"]], seed=2)
+    ctx = nb.setup(inputs["grating"], [inputs["si"]], device=0, seed=6)
+    s, se, bse = _run_gpu(ctx, recs)
+    px = recs["px"]
+    for sel, counts in ((ref_recs["E"] < 50, se), (ref_recs["E"] >= 50, bse)):
+        ref_prof = np.bincount(ref_recs["px"][sel], minlength=64).astype(float)
+        gpu_prof = np.bincount(px, weights=counts, minlength=64)
+        chi2, dof = _chi2_two_sample(gpu_prof, ref_prof)
+        assert abs(chi2 - dof) <= 3 * np.sqrt(2 * dof), (chi2, dof)
+    ctx.close()
+
+
+def test_whole_run_vs_restatement_same_streams(inputs, oracle_built):
+    """The GPU path and the C restatement share per-electron Philox streams:
+    total yields agree within 3 sigma and many primaries' counts coincide."""
+    tris = inputs["grating_small"]
+    recs = g.scan_beam(16, 16, 4, 500.0, origin=(-8.0, -8.0), seed=8)
+    ctx = nb.setup(tris, [inputs["si"]], device=0, seed=77)
+    s, se, bse = _run_gpu(ctx, recs)
+    pg = oracle.PortGeometry(tris)
+    rm = oracle.RefMaterial(inputs["si"])
+    pms, arr = oracle.port_materials([rm])
+    prim = np.zeros((len(recs), 7), np.float32)
+    prim[:, 0:3] = recs["pos"]
+    prim[:, 3:6] = recs["dir"]
+    prim[:, 6] = recs["E"]
+    c, ose, obse, _, _ = oracle.port_run(pg, arr, prim, np.arange(len(recs), dtype=np.uint32), 77,
+                                         max_energy=rm.max_energy)
+    assert abs(_z(se, ose.astype(float))) < 3
+    assert abs(_z(bse, obse.astype(float))) < 3
+    same = np.mean((se == ose) & (bse == obse))
+    assert same > 0.3, same
+    ctx.close()
+
+
+def test_run_conservation_and_edge_cases(inputs, oracle_built):
+    """Empty run; primaries outside the domain and below threshold terminate
+    without events; every pushed primary is accounted for."""
+    ctx = nb.setup(inputs["cube"], [inputs["si"]], device=0)
+    ctx.run()   # nothing queued
+    r = g.point_beam(4, 1000.0)
+    r["pos"][0] = (1e6, 0, 0)        # outside the domain
+    r["E"][1] = 0.0                  # zero energy (enters material below barrier)
+    r["dir"][2] = (0, 0, 1)          # straight to the detector
+    ctx.push_records(r)
+    ctx.run()
+    s = ctx.stats()
+    assert s["primaries_done"] == 4
+    se, bse = ctx.tag_counts(0, 4)
+    assert se[0] == 0 and bse[0] == 0
+    assert bse[2] == 1               # 1 keV straight up: detected as BSE-range energy
+    ctx.close()

@@ -1,0 +1,118 @@
+"""Pinning the oracle: the C restatement (oracle/nbx_oracle.c) against the
+reference's own CPU code compiled from its sources (oracle/_ref) and against
+published known-answer vectors.  The reference has no tests or golden
+vectors of its own, so these comparisons are what pin parity."""
+import ctypes as C
+import json
+import os
+
+import numpy as np
+import pytest
+
+from nebula_b200 import formats, generators as g
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+KAT = [
+    ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+    ((0xFFFFFFFF,) * 4, (0xFFFFFFFF,) * 2, (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+    ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+     (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+]
+
+
+def test_philox_known_answers(oracle_built):
+    for ctr, key, out in KAT:
+        assert tuple(int(v) for v in oracle_built.philox(ctr, key)) == out
+
+
+def test_uniform_open_interval(oracle_built):
+    P = oracle_built.port()
+    assert P.nbo_u01(0) == np.float32(2.0 ** -24)
+    assert P.nbo_u01(0xFFFFFFFF) == np.float32(1 - 2.0 ** -24)
+    assert 0 < P.nbo_u01(0x80000000) < 1
+
+
+@pytest.mark.parametrize("geom", ["cube", "grating", "rough"])
+def test_propagate_bit_exact(oracle_built, inputs, ray_sampler, geom):
+    tris = inputs[geom]
+    rg = oracle_built.RefGeometry(tris)
+    pg = oracle_built.PortGeometry(tris)
+    n = 60000
+    pos, d, dist = ray_sampler(rg.aabb_min, rg.aabb_max, n, 42)
+    rng = np.random.default_rng(1)
+    ign = np.full(n, -1, np.int32)
+    ign[::3] = rng.integers(0, len(pg.tri), len(ign[::3]))
+    imat = rng.choice(np.array([-123, 0, -126], np.int32), n)
+    rd, rt = rg.propagate(pos, d, dist, ign, imat)
+    od, ot = pg.propagate(pos, d, dist, ign, imat)
+    assert np.array_equal(rt, ot)
+    assert np.array_equal(rd.view(np.uint32), od.view(np.uint32))
+    assert (rt >= 0).sum() > n // 20
+    assert pg.max_extent == np.float32(rg.max_extent)
+
+
+def test_tables_bit_exact(oracle_built, inputs):
+    rm = oracle_built.RefMaterial(inputs["si"])
+    pm = oracle_built.PortMaterial(rm)
+    P = oracle_built.port()
+    rng = np.random.default_rng(2)
+    x = rng.uniform(-1.0, 10.5, 5000).astype(np.float32)
+    y = rng.random(5000).astype(np.float32)
+    for name, fn, two in (("el_imfp", P.nbo_table1d_get, False), ("in_imfp", P.nbo_table1d_get, False),
+                          ("el_icdf", P.nbo_table2d_get, True), ("in_icdf", P.nbo_table2d_get, True),
+                          ("ion", P.nbo_table2d_get_rounddown, True)):
+        t = C.byref(getattr(pm.s, name))
+        got = np.array([fn(t, float(a), float(b)) if two else fn(t, float(a)) for a, b in zip(x, y)], np.float32)
+        ref = rm.eval(name, x, y)
+        assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), name
+
+
+def test_golden_fixture(oracle_built, inputs):
+    """Committed golden vectors (tests/golden/, made by make_golden.py from
+    the reference's own propagate and table code) still hold."""
+    path = os.path.join(HERE, "golden", "golden.json")
+    with open(path) as f:
+        gold = json.load(f)
+    pg = oracle_built.PortGeometry(g.cube_geometry())
+    r = gold["cube_rays"]
+    od, ot = pg.propagate(np.array(r["pos"], np.float32), np.array(r["dir"], np.float32),
+                          np.array(r["dist"], np.float32), np.array(r["ignore_tri"], np.int32),
+                          np.array(r["ignore_mat"], np.int32))
+    assert ot.tolist() == r["tri"]
+    assert od.view(np.uint32).tolist() == r["dist_bits"]
+
+
+def _chi2(h1, h2):
+    n1, n2 = h1.sum(), h2.sum()
+    m = (h1 + h2) > 0
+    k1, k2 = np.sqrt(n2 / n1), np.sqrt(n1 / n2)
+    return (((k1 * h1 - k2 * h2) ** 2) / (h1 + h2))[m].sum(), m.sum() - 1
+
+
+def test_whole_run_statistics(oracle_built, inputs, tmp_path):
+    """C restatement vs reference cpu_mt_main-style run on the cube at 1 keV:
+    SE/BSE yields within 3 sigma, spectra by chi-square."""
+    recs = g.point_beam(6000, 1000.0, pos=(0.0, 0.0, 1.0))
+    pri = str(tmp_path / "c1.pri")
+    formats.write_pri(pri, recs)
+    ref_recs, st, _ = oracle_built.ref_run(inputs["cube_tri"], pri, [inputs["si"]], seed=3, count_events=True)
+    pg = oracle_built.PortGeometry(inputs["cube"])
+    rm = oracle_built.RefMaterial(inputs["si"])
+    pms, arr = oracle_built.port_materials([rm])
+    prim = np.zeros((len(recs), 7), np.float32)
+    prim[:, 0:3] = recs["pos"]
+    prim[:, 3:6] = recs["dir"]
+    prim[:, 6] = recs["E"]
+    c, se, bse, orecs, _ = oracle_built.port_run(pg, arr, prim, np.arange(len(recs), dtype=np.uint32), 5,
+                                                 max_energy=rm.max_energy, records_cap=100000)
+    n = len(recs)
+    for mine, ref_total in ((se, (ref_recs["E"] < 50).sum()), (bse, (ref_recs["E"] >= 50).sum())):
+        z = (mine.mean() - ref_total / n) / np.sqrt(2 * mine.var() / n)
+        assert abs(z) < 3, z
+    bins = np.concatenate([np.arange(0, 50, 2.0), np.arange(50, 1001, 50.0)])
+    chi2, dof = _chi2(np.histogram(orecs["E"], bins)[0].astype(float), np.histogram(ref_recs["E"], bins)[0].astype(float))
+    assert abs(chi2 - dof) <= 3 * np.sqrt(2 * dof), (chi2, dof)
+    ev_o = (c["n_elastic"] + c["n_inelastic"] + c["n_boundary"]) / n
+    ev_r = (st["n_intersect"] + st["n_elastic"] + st["n_inelastic"]) / n
+    assert abs(ev_o - ev_r) / ev_r < 0.05
