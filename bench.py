@@ -237,6 +237,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="nbx", choices=["nbx", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rows", type=int, default=NY, help="pixel rows of the scan (profiling runs use fewer)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -246,7 +247,7 @@ def main():
     import nebula_b200 as nb
 
     tmp = tempfile.mkdtemp(prefix="nbx_bench_")
-    mat, tris, tri_path, recs = make_workload(tmp, rank)
+    mat, tris, tri_path, recs = make_workload(tmp, rank, rows=None if args.rows >= NY else range(args.rows))
     ctx = nb.setup(tris, [mat], device=local, seed=0x78C7E39B + rank)
     n = len(recs)
     prim = np.zeros((n, 7), np.float32)

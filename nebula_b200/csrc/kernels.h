@@ -54,7 +54,7 @@ struct TransportArgs {
     float inv_bin_width;
 };
 
-constexpr int kLocalStack = 8;   // per-thread spill slots when `out` is full
+constexpr int kLocalStack = 16;  // per-thread stack of parked ancestors (depth-first cascades)
 
 cudaError_t launch_transport(const dev::Physics& P, const TransportArgs& a, int grid, int block, cudaStream_t s);
 int transport_max_blocks_per_sm(int block);

@@ -1,0 +1,320 @@
+// nebula_b200: command-line drop-in for Nebula's nebula_gpu.
+//
+//   nebula_b200 [options] <geometry.tri> <primaries.pri> mat0.mat ... matN.mat > detected.bin
+//
+// Same options, inputs and output as source/gpu_main.cu:221-440: detected
+// electrons are written to stdout as 36-byte records {pos, dir, E, px, py};
+// progress and timing go to stderr; usage errors exit with status 1.  The
+// host side calls the library only through the C ABI of include/nbx.h.
+// --prescan-size and --batch-factor are accepted for compatibility: the
+// persistent queue needs no prescan (gpu_main.cu:109-175 sized frames with it).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <iostream>
+#include <map>
+#include <numeric>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "nbx.h"
+
+namespace {
+
+// --key=value / --key value parser with the reference's rules
+// (source/common/cli_params.h:54-90): unknown keys are errors.
+struct Cli {
+    std::map<std::string, std::pair<std::string, std::string>> opts;   // key -> (description, value)
+    std::vector<std::string> positional;
+    std::string program;
+    void add(const std::string& k, const std::string& d, const std::string& v) { opts[k] = {d, v}; }
+    void parse(int argc, char** argv) {
+        program = argv[0];
+        for (int i = 1; i < argc; ++i) {
+            std::string item = argv[i];
+            if (item.size() >= 2 && item[0] == '-' && item[1] == '-') {
+                std::string key, value;
+                const auto split = item.find('=', 2);
+                if (split == std::string::npos) {
+                    key = item.substr(2);
+                    value = (++i < argc) ? argv[i] : "";
+                    if (value == "=") value = (++i < argc) ? argv[i] : "";
+                } else {
+                    key = item.substr(2, split - 2);
+                    value = item.substr(split + 1);
+                }
+                auto it = opts.find(key);
+                if (it == opts.end()) throw std::runtime_error("Unexpected key '" + key + "'");
+                it->second.second = value;
+            } else {
+                positional.push_back(item);
+            }
+        }
+    }
+    void usage(std::ostream& out) const {
+        out << "Usage: " << program << " [options] <geometry.tri> <primaries.pri> [material0.mat] .. [materialN.mat]\n"
+            << "Options:\n";
+        for (auto& o : opts) out << "\t--" << o.first << ": " << o.second.first << " [" << o.second.second << "]\n";
+    }
+    template <typename T>
+    T get(const std::string& k) const {
+        std::istringstream ss(opts.at(k).second);
+        T v{};
+        ss >> v;
+        return v;
+    }
+};
+
+template <>
+bool Cli::get<bool>(const std::string& k) const {
+    const std::string& v = opts.at(k).second;
+    return v == "1" || v == "true" || v == "True" || v == "yes";
+}
+
+struct Timer {
+    std::vector<std::pair<std::string, double>> rows;
+    std::chrono::steady_clock::time_point t0;
+    void start() { t0 = std::chrono::steady_clock::now(); }
+    void stop(const std::string& name) {
+        rows.emplace_back(name, std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+    }
+    void print() const {
+        size_t w = 0;
+        for (auto& r : rows) w = std::max(w, r.first.size());
+        std::fprintf(stderr, "Timing (seconds):\n");
+        for (auto& r : rows) std::fprintf(stderr, "%*s: %.3f\n", int(w), r.first.c_str(), r.second);
+    }
+};
+
+uint64_t morton(uint16_t x, uint16_t y, uint16_t z) {
+    uint64_t m = 0;
+    for (unsigned i = 0; i < 16; ++i) {
+        m |= (uint64_t(x) & (uint64_t(1) << i)) << (2 * i + 0);
+        m |= (uint64_t(y) & (uint64_t(1) << i)) << (2 * i + 1);
+        m |= (uint64_t(z) & (uint64_t(1) << i)) << (2 * i + 2);
+    }
+    return m;
+}
+
+int die(nbx_ctx* ctx, int rc, const char* what) {
+    std::fprintf(stderr, "Error: %s: %s (%s)\n", what, nbx_error_string(rc), ctx ? nbx_last_error(ctx) : "");
+    return 1;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    std::fprintf(stderr, "This is nebula_b200 (Nebula-compatible, version %d.%d.%d)\n\n", NBX_VERSION_MAJOR,
+                 NBX_VERSION_MINOR, NBX_VERSION_PATCH);
+    Cli p;
+    p.add("energy-threshold", "Lowest energy to simulate", "0");
+    p.add("capacity", "Electron capacity on the GPU", "1000000");
+    p.add("prescan-size", "Number of electrons to use for prescan", "1000");
+    p.add("batch-factor", "Multiplication factor for electron batch size", "0.9");
+    p.add("seed", "Random seed", std::to_string(0x78c7e39b));
+    p.add("sort-primaries", "Sort primary electrons before simulation", "0");
+    p.add("device", "CUDA device ordinal", "0");
+    try {
+        p.parse(argc, argv);
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "%s\n", e.what());
+        p.usage(std::cerr);
+        return 1;
+    }
+    const float energy_threshold = p.get<float>("energy-threshold");
+    const uint64_t capacity = p.get<uint64_t>("capacity");
+    const uint32_t prescan = p.get<uint32_t>("prescan-size");
+    const float batch_factor = p.get<float>("batch-factor");
+    const uint32_t seed = p.get<uint32_t>("seed");
+    const bool sort_primaries = p.get<bool>("sort-primaries");
+    const int device = p.get<int>("device");
+    if (p.positional.size() < 3 || capacity == 0 || prescan == 0 || batch_factor <= 0) {
+        p.usage(std::cerr);
+        return 1;
+    }
+    Timer timer;
+
+    // Geometry (gpu_main.cu:287-325)
+    std::fprintf(stderr, "Loading geometry...\n");
+    timer.start();
+    nbx_triangle* tris = nullptr;
+    uint64_t n_tris = 0;
+    int rc = nbx_load_tri(p.positional[0].c_str(), &tris, &n_tris);
+    timer.stop("Loading triangles");
+    if (rc != NBX_OK || n_tris == 0) {
+        std::fprintf(stderr, "Error: could not load triangles!\n");
+        p.usage(std::cerr);
+        return 1;
+    }
+    {
+        int max_material = -1;
+        for (uint64_t i = 0; i < n_tris; ++i) max_material = std::max({max_material, tris[i].mat_in, tris[i].mat_out});
+        const int provided = int(p.positional.size()) - 2;
+        if (max_material > provided - 1) {
+            std::fprintf(stderr, "Error: not enough materials provided for this geometry!\n  Expected %d materials, %d provided.\n",
+                         max_material + 1, provided);
+            return 1;
+        }
+        if (max_material < provided - 1)
+            std::fprintf(stderr, "Warning: too many materials provided for this geometry!\n  Expected %d materials, %d provided.\n",
+                         max_material + 1, provided);
+    }
+    timer.start();
+    nbx_octree* oct = nullptr;
+    rc = nbx_octree_build(tris, n_tris, &oct);
+    nbx_free(tris);
+    if (rc != NBX_OK) return die(nullptr, rc, "octree build");
+    timer.stop("Building acceleration structure");
+
+    // Materials (gpu_main.cu:332-349)
+    std::fprintf(stderr, "Loading materials...\n");
+    timer.start();
+    std::vector<nbx_material*> mats;
+    float max_energy = INFINITY;
+    for (size_t i = 2; i < p.positional.size(); ++i) {
+        nbx_material* m = nullptr;
+        rc = nbx_material_load(p.positional[i].c_str(), &m);
+        if (rc != NBX_OK) {
+            std::fprintf(stderr, "Error: could not load material %s\n", p.positional[i].c_str());
+            return 1;
+        }
+        std::fprintf(stderr, "  Material %zu:\n    Name: %s\n", i - 2, m->name);
+        max_energy = std::min(max_energy, m->max_energy);
+        mats.push_back(m);
+    }
+    timer.stop("Loading materials");
+
+    // Primaries (gpu_main.cu:352-380, io/load_pri_file.cpp:134-246)
+    std::fprintf(stderr, "Loading primary electrons...\n");
+    timer.start();
+    nbx_record* pri = nullptr;
+    uint64_t n_pri = 0;
+    rc = nbx_load_pri(p.positional[1].c_str(), &pri, &n_pri);
+    if (rc != NBX_OK || n_pri == 0) {
+        std::fprintf(stderr, "Error: could not load primary electrons!\n");
+        p.usage(std::cerr);
+        return 1;
+    }
+    {
+        const float eps = 10 * 1.1920928955078125e-07f;
+        uint64_t outside = 0, low = 0, high = 0, dir0 = 0;
+        for (uint64_t i = 0; i < n_pri; ++i) {
+            const nbx_record& r = pri[i];
+            bool inside = true;
+            for (int k = 0; k < 3; ++k)
+                inside = inside && r.pos[k] > oct->center[k] - oct->halfsize[k] && r.pos[k] < oct->center[k] + oct->halfsize[k];
+            outside += !inside;
+            low += !(r.E > eps);
+            high += r.E > max_energy;
+            dir0 += !(std::fabs(r.dir[0]) > eps || std::fabs(r.dir[1]) > eps || std::fabs(r.dir[2]) > eps);
+        }
+        if (outside) std::fprintf(stderr, "WARNING: %llu primary electrons starting outside geometry.\n", (unsigned long long)outside);
+        if (low) std::fprintf(stderr, "WARNING: %llu primary electrons starting with low kinetic energy.\n", (unsigned long long)low);
+        if (high)
+            std::fprintf(stderr, "WARNING: %llu primary electrons starting with kinetic energy higher than what is "
+                                 "available in the material files. Limit is %g keV.\n", (unsigned long long)high, max_energy / 1000);
+        if (dir0) std::fprintf(stderr, "WARNING: %llu primary electrons start with unphysical direction vector.\n", (unsigned long long)dir0);
+    }
+    if (sort_primaries) {
+        // Morton order of the start positions (io/load_pri_file.cpp:186-229)
+        float vmin[3], vmax[3];
+        for (int k = 0; k < 3; ++k) vmin[k] = vmax[k] = pri[0].pos[k];
+        for (uint64_t i = 0; i < n_pri; ++i)
+            for (int k = 0; k < 3; ++k) {
+                vmin[k] = std::min(vmin[k], pri[i].pos[k]);
+                vmax[k] = std::max(vmax[k], pri[i].pos[k]);
+            }
+        std::vector<uint64_t> key(n_pri);
+        for (uint64_t i = 0; i < n_pri; ++i) {
+            uint16_t q[3];
+            for (int k = 0; k < 3; ++k) {
+                const float sz = vmax[k] - vmin[k];
+                q[k] = uint16_t((pri[i].pos[k] - vmin[k]) / sz * 65535);
+            }
+            key[i] = morton(q[0], q[1], q[2]);
+        }
+        std::vector<uint64_t> perm(n_pri);
+        std::iota(perm.begin(), perm.end(), 0);
+        std::stable_sort(perm.begin(), perm.end(), [&](uint64_t a, uint64_t b) { return key[a] < key[b]; });
+        std::vector<nbx_record> sorted(n_pri);
+        for (uint64_t i = 0; i < n_pri; ++i) sorted[i] = pri[perm[i]];
+        std::memcpy(pri, sorted.data(), sizeof(nbx_record) * n_pri);
+    }
+    timer.stop("Loading primary electrons");
+
+    // Device context
+    nbx_config cfg;
+    nbx_config_default(&cfg);
+    cfg.device = device;
+    cfg.seed = seed;
+    cfg.energy_threshold = energy_threshold;
+    cfg.record_detected = 1;
+    cfg.record_capacity = 1ull << 24;
+    nbx_ctx* ctx = nullptr;
+    rc = nbx_create(&ctx, &cfg);
+    if (rc != NBX_OK) return die(nullptr, rc, "nbx_create");
+    if ((rc = nbx_set_geometry(ctx, oct)) != NBX_OK) return die(ctx, rc, "set_geometry");
+    for (auto* m : mats)
+        if ((rc = nbx_add_material(ctx, m)) != NBX_OK) return die(ctx, rc, "add_material");
+    std::fprintf(stderr, "\nLoaded %llu triangles.\nLoaded %llu primaries.\nLoaded %zu materials.\n\n",
+                 (unsigned long long)oct->n_triangles, (unsigned long long)n_pri, mats.size());
+
+    // Simulation: batches of `capacity` primaries, detected records streamed out.
+    timer.start();
+    const uint64_t batch = std::max<uint64_t>(capacity, 1);
+    std::vector<nbx_particle> part;
+    std::vector<uint32_t> tags;
+    std::vector<nbx_detected> det(1u << 20);
+    std::vector<nbx_record> out;
+    uint64_t done = 0;
+    while (done < n_pri) {
+        const uint64_t n = std::min(batch, n_pri - done);
+        part.resize(n);
+        tags.resize(n);
+        for (uint64_t i = 0; i < n; ++i) {
+            std::memcpy(part[i].pos, pri[done + i].pos, 12);
+            std::memcpy(part[i].dir, pri[done + i].dir, 12);
+            part[i].E = pri[done + i].E;
+            tags[i] = uint32_t(done + i);
+        }
+        uint64_t acc = 0;
+        if ((rc = nbx_push(ctx, part.data(), tags.data(), n, &acc)) != NBX_OK) return die(ctx, rc, "push");
+        if ((rc = nbx_run(ctx)) != NBX_OK) return die(ctx, rc, "run");
+        for (;;) {
+            uint64_t got = 0;
+            if ((rc = nbx_flush_detected(ctx, det.data(), det.size(), &got)) != NBX_OK) return die(ctx, rc, "flush");
+            if (got == 0) break;
+            out.resize(got);
+            for (uint64_t i = 0; i < got; ++i) {
+                std::memcpy(out[i].pos, det[i].pos, 12);
+                std::memcpy(out[i].dir, det[i].dir, 12);
+                out[i].E = det[i].E;
+                out[i].px = pri[det[i].tag].px;
+                out[i].py = pri[det[i].tag].py;
+            }
+            std::fwrite(out.data(), sizeof(nbx_record), got, stdout);
+        }
+        done += n;
+        std::fprintf(stderr, " \rProgress %.2f%%", 100.0 * double(done) / double(n_pri));
+    }
+    std::fflush(stdout);
+    timer.stop("Simulation");
+    nbx_stats st;
+    nbx_get_stats(ctx, &st);
+    std::fprintf(stderr, "\n\nSimulation successful!\n  events: %llu elastic, %llu inelastic, %llu boundary; %llu detected",
+                 (unsigned long long)st.events_elastic, (unsigned long long)st.events_inelastic,
+                 (unsigned long long)st.events_boundary, (unsigned long long)st.detected);
+    if (st.records_dropped) std::fprintf(stderr, " (%llu records dropped)", (unsigned long long)st.records_dropped);
+    std::fprintf(stderr, "\n\n");
+    timer.print();
+    nbx_destroy(ctx);
+    for (auto* m : mats) nbx_material_free(m);
+    nbx_octree_free(oct);
+    nbx_free(pri);
+    return 0;
+}

@@ -540,11 +540,12 @@ int nbx_run(nbx_ctx* ctx) {
         ctx->generations = 0;
         ctx->last_run_ms = ctx->last_kernel_ms = 0;
         if (ctx->n_queued == 0) return NBX_OK;
-        // Secondary-queue capacity: explicit, else 8 per queued primary
-        // (at least 1M), bounded by a quarter of the free device memory.
+        // Overflow-queue capacity (secondaries of cascades deeper than the
+        // per-thread stack): explicit, else one per queued primary (at least
+        // 1M), bounded by a quarter of the free device memory.
         size_t free_b = 0, total_b = 0;
         ck(cudaMemGetInfo(&free_b, &total_b), "meminfo");
-        uint64_t want = ctx->cfg.capacity ? ctx->cfg.capacity : std::max<uint64_t>(1ull << 20, 8 * ctx->n_queued);
+        uint64_t want = ctx->cfg.capacity ? ctx->cfg.capacity : std::max<uint64_t>(1ull << 20, ctx->n_queued);
         const uint64_t budget = (free_b / 4) / (2 * 48);
         want = std::min<uint64_t>(want, std::max<uint64_t>(budget, 1ull << 16));
         want = std::min<uint64_t>(want, 0xFFFFFFF0ull);

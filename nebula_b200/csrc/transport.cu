@@ -6,10 +6,13 @@
 // iteration).  Here each thread keeps one electron in registers and runs
 // init -> event passes back to back until the electron terminates or is
 // detected, then refills from a device queue with a warp-aggregated atomic.
-// Secondaries are pushed to the next generation's queue (warp-aggregated);
-// if that queue is full a thread keeps up to kLocalStack of its own
-// secondaries and simulates them itself.  Detections are tallied per
-// primary tag on the device; detected records are optional.
+// Cascades run depth-first, child first: when an event creates a secondary,
+// the parent is parked on a small per-thread stack and the secondary is
+// simulated at once, so a primary's whole cascade normally stays in one
+// thread and never touches global memory.  Only a cascade deeper than the
+// stack hands secondaries to the next generation's queue (warp-aggregated
+// push).  Detections are tallied per primary tag on the device; detected
+// records are optional.
 #include <cooperative_groups.h>
 
 #include "kernels.h"
@@ -52,8 +55,15 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 }
 
 __global__ void __launch_bounds__(256) transport_kernel(const dev::Physics P, const TransportArgs a) {
+    __shared__ float leaf_cache[13 * 256];
+    const dev::LeafCache cache{leaf_cache + threadIdx.x, int(blockDim.x)};
+    cache.f(0) = 0.0f;   // location 0: empty
+    cache.f(1) = 0.0f;
     const uint32_t n_in = min(*a.n_in, a.in_capacity);
     dev::Electron e;
+    // Child-first depth-first cascade: when an event creates a secondary the
+    // parent is parked here and the secondary is simulated at once, so the
+    // stack only ever holds the current electron's ancestors.
     dev::Electron stack[kLocalStack];
     int sp = 0;
     bool alive = false;
@@ -82,25 +92,29 @@ __global__ void __launch_bounds__(256) transport_kernel(const dev::Physics P, co
         int ev;
         bool has_se;
         dev::Electron se;
-        const int st = dev::step(P, e, &ev, &se, &has_se);
+        const int st = dev::step(P, e, &ev, &se, &has_se, cache);
         ++c_steps;
         c_el += (ev == dev::kEvElastic);
         c_inel += (ev == dev::kEvInelastic);
         c_bd += (ev == dev::kEvBoundary);
         if (has_se) {
+            // an inelastic step never ends its electron: st == kAlive here
             ++c_se;
+            if (sp < kLocalStack) {
+                stack[sp++] = e;
+                e = se;
+                continue;
+            }
+            // Deep cascade: hand the secondary to the next generation.
             cg::coalesced_group g = cg::coalesced_threads();
             uint32_t base = 0;
             if (g.thread_rank() == 0) base = atomicAdd(a.out_tail, g.size());
             base = g.shfl(base, 0);
             const uint32_t slot = base + g.thread_rank();
-            if (slot < a.out_capacity) {
+            if (slot < a.out_capacity)
                 store_electron(a.out, slot, se);
-            } else if (sp < kLocalStack) {
-                stack[sp++] = se;
-            } else {
+            else
                 ++c_ovf;
-            }
         }
         if (st == dev::kAlive) continue;
         alive = false;
@@ -152,14 +166,24 @@ __global__ void __launch_bounds__(256) transport_kernel(const dev::Physics P, co
     }
 }
 
-__global__ void ray_query_kernel(const dev::Geometry g, const float* pos, const float* dir, const float* dist,
-                                 const int32_t* ignore_tri, const int32_t* ignore_mat, uint64_t n, float* out_dist,
-                                 int32_t* out_tri) {
-    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+// Each thread answers kRaysPerThread consecutive rays, carrying its leaf
+// cache from one to the next (a spatially coherent batch exercises the
+// cached descent; any batch must give the reference's answers).
+constexpr int kRaysPerThread = 8;
+__global__ void __launch_bounds__(128) ray_query_kernel(const dev::Geometry g, const float* pos, const float* dir,
+                                                        const float* dist, const int32_t* ignore_tri,
+                                                        const int32_t* ignore_mat, uint64_t n, float* out_dist,
+                                                        int32_t* out_tri) {
+    __shared__ float leaf_cache[13 * 128];
+    const dev::LeafCache cache{leaf_cache + threadIdx.x, int(blockDim.x)};
+    cache.f(0) = 0.0f;
+    cache.f(1) = 0.0f;
+    const uint64_t first = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) * kRaysPerThread;
+    for (uint64_t i = first; i < n && i < first + kRaysPerThread; ++i) {
         int hit;
         const dev::V3 p{pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
         const dev::V3 d{dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]};
-        out_dist[i] = dev::propagate(g, p, d, dist[i], ignore_tri[i], ignore_mat[i], &hit);
+        out_dist[i] = dev::propagate(g, p, d, dist[i], ignore_tri[i], ignore_mat[i], &hit, cache);
         out_tri[i] = hit;
     }
 }
@@ -309,7 +333,9 @@ cudaError_t launch_ray_query(const dev::Geometry& g, const float* pos, const flo
                              const int32_t* ignore_tri, const int32_t* ignore_mat, uint64_t n, float* out_dist,
                              int32_t* out_tri, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
-    ray_query_kernel<<<grid_for(n, 128), 128, 0, s>>>(g, pos, dir, dist, ignore_tri, ignore_mat, n, out_dist, out_tri);
+    const uint64_t threads = (n + kRaysPerThread - 1) / kRaysPerThread;
+    const int blocks = int((threads + 127) / 128);
+    ray_query_kernel<<<blocks, 128, 0, s>>>(g, pos, dir, dist, ignore_tri, ignore_mat, n, out_dist, out_tri);
     return cudaGetLastError();
 }
 

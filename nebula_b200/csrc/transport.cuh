@@ -163,37 +163,96 @@ __device__ __forceinline__ bool in_domain(const Geometry& g, V3 p) {
            (p.z > g.cz - g.hz) && (p.z < g.cz + g.hz);
 }
 
+// Per-thread memo of the last octree leaf a descent reached, kept in shared
+// memory as 13 words strided by the block size: location code (2 words), raw
+// leaf value, the leaf's AABB centre and scale (ax, ay, az, aw) exactly as the
+// descent computed them, and per-axis bounds (lo, hi].  A position p with
+// lo < p <= hi on every axis gives the same octant at every level of a descent
+// from the root (octant bit = p > centre), so it lands in the same leaf with
+// the same float AABB: reusing the memo is bit-identical to descending.
+struct LeafCache {
+    float* base;   // nullptr: no cache
+    int stride;
+    __device__ __forceinline__ float& f(int i) const { return base[i * stride]; }
+};
+
 // octree::propagate (geometry/octree.inl:33-192).  Returns the travelled
 // distance; *hit receives the triangle index or -1.
 __device__ __forceinline__ float propagate(const Geometry& g, V3 start, V3 dir, float distance, int ignore_tri,
-                                           int ignore_mat, int* hit) {
+                                           int ignore_mat, int* hit, LeafCache cache = LeafCache{nullptr, 0}) {
     const int32_t* od = g.octree;
     V3 cur = start;
     float to_go = distance;
     uint64_t location = 1;
+    bool first = true;
     do {
-        float ax = g.cx, ay = g.cy, az = g.cz, aw = 1;
-        int index = 0;
-        for (int i = 60 - __clzll(location); i >= 0; i -= 3) {
-            const unsigned octant = unsigned(location >> i) & 7u;
-            index = __ldg(od + index + octant);
-            ax += aw * g.hx * (float(octant & 1) - 0.5f);
-            ay += aw * g.hy * (float((octant & 2) >> 1) - 0.5f);
-            az += aw * g.hz * (float((octant & 4) >> 2) - 0.5f);
-            aw *= 0.5f;
+        float ax, ay, az, aw;
+        int index;
+        bool cached = false;
+        if (first && cache.base) {
+            const uint64_t cl = uint64_t(__float_as_uint(cache.f(0))) | (uint64_t(__float_as_uint(cache.f(1))) << 32);
+            if (cl > 1 && cur.x > cache.f(7) && cur.x <= cache.f(10) && cur.y > cache.f(8) && cur.y <= cache.f(11) &&
+                cur.z > cache.f(9) && cur.z <= cache.f(12)) {
+                location = cl;
+                index = __float_as_int(cache.f(2));
+                ax = cache.f(3);
+                ay = cache.f(4);
+                az = cache.f(5);
+                aw = cache.f(6);
+                cached = true;
+            }
         }
-        while (index >= 0) {
-            unsigned octant = 0;
-            octant ^= (cur.x > ax) ? 1u : 0u;
-            octant ^= (cur.y > ay) ? 2u : 0u;
-            octant ^= (cur.z > az) ? 4u : 0u;
-            location = (location << 3) | octant;
-            index = __ldg(od + index + octant);
-            ax += aw * g.hx * (float(octant & 1) - 0.5f);
-            ay += aw * g.hy * (float((octant & 2) >> 1) - 0.5f);
-            az += aw * g.hz * (float((octant & 4) >> 2) - 0.5f);
-            aw *= 0.5f;
+        if (!cached) {
+            const float inf = __int_as_float(0x7f800000);
+            float lox = -inf, loy = -inf, loz = -inf, hix = inf, hiy = inf, hiz = inf;
+            ax = g.cx;
+            ay = g.cy;
+            az = g.cz;
+            aw = 1;
+            index = 0;
+            for (int i = 60 - __clzll(location); i >= 0; i -= 3) {
+                const unsigned octant = unsigned(location >> i) & 7u;
+                index = __ldg(od + index + octant);
+                if (octant & 1) lox = ax; else hix = ax;
+                if (octant & 2) loy = ay; else hiy = ay;
+                if (octant & 4) loz = az; else hiz = az;
+                ax += aw * g.hx * (float(octant & 1) - 0.5f);
+                ay += aw * g.hy * (float((octant & 2) >> 1) - 0.5f);
+                az += aw * g.hz * (float((octant & 4) >> 2) - 0.5f);
+                aw *= 0.5f;
+            }
+            while (index >= 0) {
+                unsigned octant = 0;
+                octant ^= (cur.x > ax) ? 1u : 0u;
+                octant ^= (cur.y > ay) ? 2u : 0u;
+                octant ^= (cur.z > az) ? 4u : 0u;
+                location = (location << 3) | octant;
+                index = __ldg(od + index + octant);
+                if (octant & 1) lox = ax; else hix = ax;
+                if (octant & 2) loy = ay; else hiy = ay;
+                if (octant & 4) loz = az; else hiz = az;
+                ax += aw * g.hx * (float(octant & 1) - 0.5f);
+                ay += aw * g.hy * (float((octant & 2) >> 1) - 0.5f);
+                az += aw * g.hz * (float((octant & 4) >> 2) - 0.5f);
+                aw *= 0.5f;
+            }
+            if (cache.base) {
+                cache.f(0) = __uint_as_float(uint32_t(location));
+                cache.f(1) = __uint_as_float(uint32_t(location >> 32));
+                cache.f(2) = __int_as_float(index);
+                cache.f(3) = ax;
+                cache.f(4) = ay;
+                cache.f(5) = az;
+                cache.f(6) = aw;
+                cache.f(7) = lox;
+                cache.f(8) = loy;
+                cache.f(9) = loz;
+                cache.f(10) = hix;
+                cache.f(11) = hiy;
+                cache.f(12) = hiz;
+            }
         }
+        first = false;
         index = -index;
 
         float intersect;
@@ -414,7 +473,8 @@ __device__ __forceinline__ int boundary(const Physics& P, Electron& e, float u) 
 // cpu_particle_manager.inl:214-235).  Uniforms: block 0 of the step's Philox
 // stream feeds the two free paths and the first two event draws; block 1 the
 // remaining four inelastic draws.
-__device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, Electron* se, bool* has_se) {
+__device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, Electron* se, bool* has_se,
+                                    LeafCache cache = LeafCache{nullptr, 0}) {
     *event = kEvNone;
     *has_se = false;
     if (!in_domain(P.geo, V3{e.px, e.py, e.pz})) return kTerminated;
@@ -445,7 +505,7 @@ __device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, E
     }
     const V3 nd = normalised(V3{e.dx, e.dy, e.dz});
     int hit;
-    const float tdist = propagate(P.geo, V3{e.px, e.py, e.pz}, nd, dist, e.last_tri, e.mat, &hit);
+    const float tdist = propagate(P.geo, V3{e.px, e.py, e.pz}, nd, dist, e.last_tri, e.mat, &hit, cache);
     int status = kAlive;
     if (hit < 0) {
         e.px += nd.x * dist;
