@@ -268,6 +268,9 @@ def main():
     pin_p[:] = prim
     pin_t[:] = tags
     ctx.set_tag_range(n)
+    # Autotune the transport launch shape on a 16-row sample of the scan.
+    sample = np.arange(min(n, 16 * NX * PER_PIXEL))   # records are row-major: the first 16 rows
+    tuned = ctx.autotune(prim[sample], tags[sample])
 
     def one_step():
         ctx.push(pin_p, pin_t)
@@ -342,7 +345,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "parallelism": "replicas x%d" % world,
                        "l2": "inputs larger than L2 (primary queue %.0f MB per step)" % (n * 48 / 1e6),
-                       "block_size": 256},
+                       "autotuned": {"blocks_per_sm_variant": tuned[0], "block_size": tuned[1]}},
             "primaries_per_s": prim_all / t_dev,
             "events_per_primary": events / (n * args.steps),
             "se_yield": mean_se, "bse_yield": float(bse.sum()) / (n * args.steps),

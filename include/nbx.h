@@ -151,8 +151,8 @@ typedef struct {
     uint64_t capacity;         /* electrons per device queue; 0 = sized from free HBM */
     int32_t record_detected;   /* keep per-electron detected records */
     uint64_t record_capacity;  /* detected records held on the device; 0 = auto */
-    int32_t block_size;        /* threads per block of the transport kernel; 0 = tuned */
-    int32_t blocks_per_sm;     /* resident blocks per SM; 0 = occupancy maximum */
+    int32_t block_size;        /* threads per block of the transport kernel; 0 = 256 */
+    int32_t blocks_per_sm;     /* transport variant: 2, 3 or 4 resident blocks per SM; 0 = 3 */
 } nbx_config;
 
 typedef struct {
@@ -211,6 +211,14 @@ int nbx_pixel_yields(nbx_ctx* ctx, const uint32_t* pixel_of_tag, uint64_t n_tags
 /* Detected-energy histogram: n_bins bins of bin_width eV from 0. */
 int nbx_get_spectrum(nbx_ctx* ctx, uint64_t* counts, uint32_t n_bins, float* bin_width);
 int nbx_reset_tallies(nbx_ctx* ctx);
+
+/* Autotuner (no counterpart in the reference, whose launch shape is fixed at
+ * 32-thread blocks over the whole capacity, drivers/gpu/gpu_driver.inl:64):
+ * runs the given sample once per transport variant (2, 3, 4 resident blocks
+ * per SM) and block size (256, 128), keeps the fastest, and resets the
+ * tallies.  Random streams of later pushes are unaffected. */
+int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n,
+                 int32_t* blocks_per_sm, int32_t* block_size);
 
 /* ---- kernel-level queries (host buffers in/out) ------------------------- */
 /* Batched octree propagate; ignore_tri / out_tri index the linearized

@@ -126,6 +126,7 @@ def lib():
         "nbx_table_query": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp, _vp, C.c_uint64, _vp]),
         "nbx_philox": (C.c_int, [_vp, _vp, _vp, C.c_uint64, _vp]),
         "nbx_step_query": (C.c_int, [_vp, _vp, C.c_uint64, _vp, _vp, _vp, _vp]),
+        "nbx_autotune": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -281,6 +282,15 @@ class Context:
 
     def run(self):
         self._ck(self.L.nbx_run(self.h))
+
+    def autotune(self, particles: np.ndarray, tags: np.ndarray):
+        """Pick the fastest transport variant / block size on a sample; returns (blocks_per_sm, block)."""
+        p = np.ascontiguousarray(particles, np.float32).reshape(-1, 7)
+        t = np.ascontiguousarray(tags, np.uint32)
+        v = C.c_int32()
+        b = C.c_int32()
+        self._ck(self.L.nbx_autotune(self.h, _ptr(p), _ptr(t), len(t), C.byref(v), C.byref(b)))
+        return v.value, b.value
 
     def stats(self) -> dict:
         s = Stats()

@@ -56,8 +56,10 @@ struct TransportArgs {
 
 constexpr int kLocalStack = 16;  // per-thread stack of parked ancestors (depth-first cascades)
 
-cudaError_t launch_transport(const dev::Physics& P, const TransportArgs& a, int grid, int block, cudaStream_t s);
-int transport_max_blocks_per_sm(int block);
+// variant: resident blocks per SM the kernel was compiled for (2, 3 or 4).
+cudaError_t launch_transport(const dev::Physics& P, const TransportArgs& a, int grid, int block, int variant,
+                             cudaStream_t s);
+int transport_max_blocks_per_sm(int block, int variant);
 
 cudaError_t launch_ray_query(const dev::Geometry& g, const float* pos, const float* dir, const float* dist,
                              const int32_t* ignore_tri, const int32_t* ignore_mat, uint64_t n, float* out_dist,

@@ -118,7 +118,7 @@ struct nbx_ctx {
     // stats
     uint64_t pushed = 0, generations = 0;
     double last_run_ms = 0, last_kernel_ms = 0;
-    int block = 256, bpsm = 0;
+    int block = 256, bpsm = 0, variant = 3;
 
     ~nbx_ctx() {
         for (auto* t : tables) delete t;
@@ -395,8 +395,10 @@ int nbx_create(nbx_ctx** out, const nbx_config* cfg) {
         ck(cudaMemset(ctx->rec_count.p, 0, 4), "memset");
         ctx->block = c.block_size > 0 ? c.block_size : 256;
         if (ctx->block % 32 != 0 || ctx->block > 256) throw ApiError(NBX_ERR_ARG, "block_size must be a multiple of 32, <= 256");
-        const int maxb = nbx::transport_max_blocks_per_sm(ctx->block);
-        ctx->bpsm = c.blocks_per_sm > 0 ? std::min(c.blocks_per_sm, maxb) : maxb;
+        // Kernel variant = resident 256-thread blocks per SM it was register-
+        // limited for (2, 3 or 4); default 3 (80 registers).
+        ctx->variant = (c.blocks_per_sm >= 2 && c.blocks_per_sm <= 4) ? c.blocks_per_sm : 3;
+        ctx->bpsm = nbx::transport_max_blocks_per_sm(ctx->block, ctx->variant);
         if (c.record_detected) {
             ctx->rec_cap = c.record_capacity ? c.record_capacity : (1ull << 24);
             ctx->rec_a.alloc(ctx->rec_cap);
@@ -589,7 +591,7 @@ int nbx_run(nbx_ctx* ctx) {
                 a.out_tail = ctl + kMaxGenerations + g;
                 a.out_capacity = cap;
                 a.in_capacity = uint32_t(std::min<uint64_t>(in->cap, 0xFFFFFFF0ull));
-                ck(nbx::launch_transport(ctx->phys, a, grid, ctx->block, ctx->stream), "transport launch");
+                ck(nbx::launch_transport(ctx->phys, a, grid, ctx->block, ctx->variant, ctx->stream), "transport launch");
             }
             uint32_t last = 0;
             ck(cudaMemcpyAsync(&last, ctl + kMaxGenerations + (g - 1), 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
@@ -826,6 +828,40 @@ int nbx_step_query(nbx_ctx* ctx, nbx_electron* electrons, uint64_t n, int32_t* s
         ck(cudaStreamSynchronize(s), "sync");
         return NBX_OK;
     });
+}
+
+int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n,
+                 int32_t* blocks_per_sm, int32_t* block_size) {
+    if (!ctx || !particles || !tags || n == 0) return NBX_ERR_ARG;
+    if (!ctx->have_geometry) return fail(ctx, NBX_ERR_STATE, "nbx_autotune before nbx_set_geometry");
+    if (ctx->n_queued) return fail(ctx, NBX_ERR_STATE, "nbx_autotune with primaries queued");
+    const int variants[3] = {2, 3, 4};
+    const int blocks[2] = {256, 128};
+    double best = 1e300;
+    int best_v = ctx->variant, best_b = ctx->block;
+    const uint64_t uid_save = ctx->uid_next;
+    for (int v : variants) {
+        for (int b : blocks) {
+            ctx->variant = v;
+            ctx->block = b;
+            ctx->bpsm = nbx::transport_max_blocks_per_sm(b, v);
+            int rc = nbx_push(ctx, particles, tags, n, nullptr);
+            if (rc == NBX_OK) rc = nbx_run(ctx);
+            if (rc != NBX_OK) return rc;
+            if (ctx->last_run_ms < best) {
+                best = ctx->last_run_ms;
+                best_v = v;
+                best_b = b;
+            }
+        }
+    }
+    ctx->variant = best_v;
+    ctx->block = best_b;
+    ctx->bpsm = nbx::transport_max_blocks_per_sm(best_b, best_v);
+    ctx->uid_next = uid_save;
+    if (blocks_per_sm) *blocks_per_sm = best_v;
+    if (block_size) *block_size = best_b;
+    return nbx_reset_tallies(ctx);
 }
 
 }  // extern "C"

@@ -54,7 +54,10 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
     return v;
 }
 
-__global__ void __launch_bounds__(256) transport_kernel(const dev::Physics P, const TransportArgs a) {
+// MinBlocks: resident 256-thread blocks per SM the register allocation must
+// allow (2: 128 registers, 3: 80, 4: 64); the host picks the variant.
+template <int MinBlocks>
+__global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Physics P, const TransportArgs a) {
     __shared__ float leaf_cache[13 * 256];
     const dev::LeafCache cache{leaf_cache + threadIdx.x, int(blockDim.x)};
     cache.f(0) = 0.0f;   // location 0: empty
@@ -318,14 +321,25 @@ int grid_for(uint64_t n, int block) {
 
 }  // namespace
 
-cudaError_t launch_transport(const dev::Physics& P, const TransportArgs& a, int grid, int block, cudaStream_t s) {
-    transport_kernel<<<grid, block, 0, s>>>(P, a);
+cudaError_t launch_transport(const dev::Physics& P, const TransportArgs& a, int grid, int block, int variant,
+                             cudaStream_t s) {
+    switch (variant) {
+    case 2: transport_kernel<2><<<grid, block, 0, s>>>(P, a); break;
+    case 4: transport_kernel<4><<<grid, block, 0, s>>>(P, a); break;
+    default: transport_kernel<3><<<grid, block, 0, s>>>(P, a); break;
+    }
     return cudaGetLastError();
 }
 
-int transport_max_blocks_per_sm(int block) {
+int transport_max_blocks_per_sm(int block, int variant) {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel, block, 0) != cudaSuccess) return 1;
+    cudaError_t e;
+    switch (variant) {
+    case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<2>, block, 0); break;
+    case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<4>, block, 0); break;
+    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<3>, block, 0); break;
+    }
+    if (e != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
 

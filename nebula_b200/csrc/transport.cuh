@@ -323,13 +323,17 @@ __device__ __forceinline__ float propagate(const Geometry& g, V3 start, V3 dir, 
 // ---------------------------------------------------------------------------
 // Physics
 // ---------------------------------------------------------------------------
+// The two scattering mechanisms share their first half: a 2D ICDF lookup at
+// (log E, U) and the random normal to the current direction.  step() runs
+// that half once for every lane that scatters (the warp stays converged) and
+// then branches into the mechanism-specific remainder below.
+
 // kieft_elastic<acoustic phonon loss, atomic recoil>::execute (physics/kieft/elastic.h:68-115)
-__device__ __forceinline__ void elastic(const Material& m, Electron& e, float u_cos, float u_phi) {
-    const float x = logf(e.E);
-    const float cos_theta = clampr(table2d_get(m.el_icdf, x, u_cos), -1, 1);
+// after the ICDF lookup (icdf_value) and with d = normalised(dir),
+// n = normalised(make_normal_vec(d, phi)).
+__device__ __forceinline__ void elastic_finish(const Material& m, Electron& e, float icdf_value, V3 d, V3 n) {
+    const float cos_theta = clampr(icdf_value, -1, 1);
     const float sin_theta = sqrtf(1 - cos_theta * cos_theta);
-    const V3 d = normalised(V3{e.dx, e.dy, e.dz});
-    const V3 n = normalised(make_normal_vec(d, (2 * kPi) * u_phi));
     e.dx = d.x * cos_theta + n.x * sin_theta;
     e.dy = d.y * cos_theta + n.y * sin_theta;
     e.dz = d.z * cos_theta + n.z * sin_theta;
@@ -339,12 +343,16 @@ __device__ __forceinline__ void elastic(const Material& m, Electron& e, float u_
         e.E -= m.recoil_const * (1 - cos_theta) * e.E;
 }
 
-// kieft_inelastic<all options>::execute (physics/kieft/inelastic.h:69-206).
-// Returns true and fills *se when a secondary is created.
-__device__ __forceinline__ bool inelastic(const Material& m, Electron& e, const float u[6], Electron* se) {
+// kieft_inelastic<all options>::execute (physics/kieft/inelastic.h:69-206)
+// after the log-omega' ICDF lookup (log_omega0), with d and n as above.
+// u_bind, u_omega: binding-energy and energy-loss draws; u_v1, u_v2: the
+// instantaneous-momentum unit vector.  Returns true and fills *se when a
+// secondary is created.
+__device__ __forceinline__ bool inelastic_finish(const Material& m, Electron& e, float log_omega0, V3 d, V3 n,
+                                                 float u_bind, float u_omega, float u_v1, float u_v2, Electron* se) {
     const float K = e.E;
-    const float omega0 = expf(table2d_get(m.in_icdf, logf(K), u[0]));
-    float binding = table2d_rounddown(m.ion, logf(omega0), u[1]);
+    const float omega0 = expf(log_omega0);
+    float binding = table2d_rounddown(m.ion, logf(omega0), u_bind);
     float omega;
     {
         const float omega_max = 0.5f * (K + omega0 - m.fermi);
@@ -354,7 +362,7 @@ __device__ __forceinline__ bool inelastic(const Material& m, Electron& e, const 
             omega_min = 0.5f * (K + omega0 - sqrtf(K * (K - 2 * omega0)));
             w0 = omega0;
         }
-        const float U = u[2];
+        const float U = u_omega;
         if ((w0 > 0) && (omega_min > w0) && (omega_min < omega_max)) {
             const float f_min = 1 / w0 * logf((omega_min - w0) / omega_min);
             const float f_max = 1 / w0 * logf((omega_max - w0) / omega_max);
@@ -369,14 +377,12 @@ __device__ __forceinline__ bool inelastic(const Material& m, Electron& e, const 
         } else if (omega0 > m.band_gap) {
             binding = m.band_gap;
         } else {
-            e.E -= omega0;
+            e.E -= omega0;   // optical phonon: direction untouched, no secondary
             return false;
         }
     }
     binding = max_ref(0, binding);
 
-    const V3 d = normalised(V3{e.dx, e.dy, e.dz});
-    const V3 n = normalised(make_normal_vec(d, (2 * kPi) * u[3]));
     const float Kp = e.E - m.fermi + 2 * binding;
     const float dK = binding + omega;
     const float cos_theta = sqrtf(dK / Kp);
@@ -384,7 +390,7 @@ __device__ __forceinline__ bool inelastic(const Material& m, Electron& e, const 
     V3 s{d.x * cos_theta + n.x * sin_theta, d.y * cos_theta + n.y * sin_theta, d.z * cos_theta + n.z * sin_theta};
     s = normalised(s);
     {
-        const V3 uv = make_unit_vec(2 * u[4] - 1, (2 * kPi) * u[5]);
+        const V3 uv = make_unit_vec(2 * u_v1 - 1, (2 * kPi) * u_v2);
         const float a = sqrtf(binding / dK);
         s.x += a * uv.x;
         s.y += a * uv.y;
@@ -470,9 +476,12 @@ __device__ __forceinline__ int boundary(const Physics& P, Electron& e, float u) 
 }
 
 // One pass of init -> intersect -> scatter (drivers/cpu/cpu_driver.inl:73-161,
-// cpu_particle_manager.inl:214-235).  Uniforms: block 0 of the step's Philox
-// stream feeds the two free paths and the first two event draws; block 1 the
-// remaining four inelastic draws.
+// cpu_particle_manager.inl:214-235).  Uniforms of step k come from Philox
+// blocks (k, 0) and (k, 1) of the electron's stream: block 0 x/y feed the
+// inelastic/elastic free paths, z the ICDF probability (or the boundary
+// transmission draw), w the scattering azimuth; block 1 the remaining four
+// inelastic draws.  The mechanisms' log(E) is the init pass's log(E): the
+// energy has not changed in between, so the value is the same.
 __device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, Electron* se, bool* has_se,
                                     LeafCache cache = LeafCache{nullptr, 0}) {
     *event = kEvNone;
@@ -481,10 +490,11 @@ __device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, E
     const uint4 r0 = draw(P.seed, e, 0);
     int type = 0;
     float dist = P.geo.max_extent;
+    float logE = 0;
     if (e.mat >= 0) {
         const Material& m = P.mat[e.mat];
         if (e.E < m.barrier + P.min_energy || e.E > m.barrier + P.max_energy) return kTerminated;
-        const float logE = logf(e.E);
+        logE = logf(e.E);
         dist = __int_as_float(0x7f800000);
         {
             const float imfp = expf(table1d_get(m.in_imfp, logE));
@@ -511,16 +521,23 @@ __device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, E
         e.px += nd.x * dist;
         e.py += nd.y * dist;
         e.pz += nd.z * dist;
-        if (type == 2) {
+        if (type != 0) {
+            // Shared first half of both mechanisms (see elastic_finish).
+            // Uniforms: block 0 z -> ICDF probability, w -> azimuth; block 1
+            // -> binding, energy loss and the two unit-vector draws.
             e.last_tri = -1;
-            elastic(P.mat[e.mat], e, u01(r0.z), u01(r0.w));
-            *event = kEvElastic;
-        } else if (type == 1) {
-            e.last_tri = -1;
+            const Material& m = P.mat[e.mat];
+            const bool inel = (type == 1);
             const uint4 r1 = draw(P.seed, e, 1);
-            const float u[6] = {u01(r0.z), u01(r0.w), u01(r1.x), u01(r1.y), u01(r1.z), u01(r1.w)};
-            *has_se = inelastic(P.mat[e.mat], e, u, se);
-            *event = kEvInelastic;
+            const float tv = table2d_get(inel ? m.in_icdf : m.el_icdf, logE, u01(r0.z));
+            const V3 n = normalised(make_normal_vec(nd, (2 * kPi) * u01(r0.w)));
+            if (!inel) {
+                elastic_finish(m, e, tv, nd, n);
+                *event = kEvElastic;
+            } else {
+                *has_se = inelastic_finish(m, e, tv, nd, n, u01(r1.x), u01(r1.y), u01(r1.z), u01(r1.w), se);
+                *event = kEvInelastic;
+            }
         }
     } else {
         e.px += nd.x * tdist;

@@ -483,8 +483,10 @@ int nbo_step(const nbo_geometry* g, const nbo_material* mats, const nbo_params* 
             uint32_t r1c[4] = {e->step, 1u, (uint32_t)e->uid, (uint32_t)(e->uid >> 32)};
             const uint32_t key[2] = {p->seed, 0u};
             nbo_philox4x32_10(r1c, key, r1);
-            const float u[6] = {nbo_u01(r0[2]), nbo_u01(r0[3]), nbo_u01(r1[0]),
-                                nbo_u01(r1[1]), nbo_u01(r1[2]), nbo_u01(r1[3])};
+            /* slots: omega' ICDF <- block 0 z, binding <- block 1 x, energy loss
+             * <- block 1 y, azimuth <- block 0 w, unit vector <- block 1 z, w */
+            const float u[6] = {nbo_u01(r0[2]), nbo_u01(r1[0]), nbo_u01(r1[1]),
+                                nbo_u01(r0[3]), nbo_u01(r1[2]), nbo_u01(r1[3])};
             *has_se = nbo_inelastic(&mats[e->mat], e, u, se);
             *event = NBO_EV_INELASTIC;
         }
