@@ -252,6 +252,26 @@ typedef struct {
 int nbx_step_query(nbx_ctx* ctx, nbx_electron* electrons, uint64_t n, int32_t* status, int32_t* event,
                    nbx_electron* secondaries, int32_t* has_se);
 
+/* ---- allocation-free transport ------------------------------------------- */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory (a host application whose own caching allocator owns the GPU's
+ * memory, or a pipeline that must not let an allocation's implicit device
+ * synchronisation stall its streams): simulates n <= NBX_NOALLOC_MAX_PRIMARIES
+ * primaries and their cascades from DEVICE buffers without allocating
+ * anything.  d_particles holds n x 7 floats (pos, dir, E), d_tags n tags;
+ * uid_base numbers the primaries' random streams exactly as the n primaries
+ * of an nbx_push starting at that running index, so both entry points give
+ * identical tallies.  Detections are ADDED to d_se_count / d_bse_count
+ * (n_tags each, caller-zeroed).  counts (host, may be null) receives
+ * {elastic, inelastic, boundary, detected} of this call.  Scratch lives in a
+ * fixed array of about 9.5 MB that every GPU loading the library keeps until
+ * exit; the first call on a device resolves its address and should come
+ * before any stream capture; calls that overlap on the GPU race on it.
+ * Sizes beyond the maximum return NBX_ERR_ARG. */
+#define NBX_NOALLOC_MAX_PRIMARIES 65536
+int nbx_run_noalloc(nbx_ctx* ctx, const float* d_particles, const uint32_t* d_tags, uint32_t n, uint64_t uid_base,
+                    uint32_t* d_se_count, uint32_t* d_bse_count, uint64_t n_tags, uint64_t counts[4]);
+
 #ifdef __cplusplus
 }
 #endif

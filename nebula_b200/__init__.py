@@ -127,6 +127,8 @@ def lib():
         "nbx_philox": (C.c_int, [_vp, _vp, _vp, C.c_uint64, _vp]),
         "nbx_step_query": (C.c_int, [_vp, _vp, C.c_uint64, _vp, _vp, _vp, _vp]),
         "nbx_autotune": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+        "nbx_run_noalloc": (C.c_int, [_vp, _vp, _vp, C.c_uint32, C.c_uint64, _vp, _vp, C.c_uint64,
+                                      C.POINTER(C.c_uint64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -363,6 +365,17 @@ class Context:
         hs = np.zeros(n, np.int32)
         self._ck(self.L.nbx_step_query(self.h, _ptr(e), n, _ptr(st), _ptr(ev), _ptr(se), _ptr(hs)))
         return e, st, ev, se, hs
+
+
+def run_noalloc(ctx: Context, d_particles: int, d_tags: int, n: int, uid_base: int, d_se: int, d_bse: int,
+                n_tags: int):
+    """nbx_run_noalloc on device pointers (ints); returns {elastic, inelastic,
+    boundary, detected} of the call."""
+    counts = (C.c_uint64 * 4)()
+    rc = ctx.L.nbx_run_noalloc(ctx.h, _vp(d_particles), _vp(d_tags), n, uid_base, _vp(d_se), _vp(d_bse), n_tags,
+                               counts)
+    ctx._ck(rc)
+    return dict(zip(("elastic", "inelastic", "boundary", "detected"), [int(c) for c in counts]))
 
 
 def setup(tri_path_or_array, mat_paths, **ctx_kwargs):

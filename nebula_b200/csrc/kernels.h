@@ -72,6 +72,13 @@ cudaError_t launch_step_query(const dev::Physics& P, void* electrons, uint64_t n
                               void* secondaries, int32_t* has_se, cudaStream_t s);
 cudaError_t launch_pixel_yields(const uint32_t* se, const uint32_t* bse, const uint32_t* pixel_of_tag,
                                 uint64_t n_tags, uint64_t n_pixels, double* out, cudaStream_t s);
+// Allocation-free transport on the file-scope scratch of transport.cu
+// (see nbx_run_noalloc).  Returns 0 or an NBX_ERR_* code with *err set.
+constexpr uint32_t kNoAllocMaxPrimaries = 65536;
+int run_transport_noalloc(const dev::Physics& P, int grid, int block, int variant, cudaStream_t s,
+                          const float* d_particles,
+                          const uint32_t* d_tags, uint32_t n, uint64_t uid_base, uint32_t* d_se, uint32_t* d_bse,
+                          uint64_t n_tags, uint64_t counts[4], const char** err);
 cudaError_t launch_fill_queue(Queue q, const float* particles, const uint32_t* tags, uint64_t uid_base,
                               uint64_t n, uint64_t offset, cudaStream_t s);
 

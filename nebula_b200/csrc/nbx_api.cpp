@@ -864,4 +864,23 @@ int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* ta
     return nbx_reset_tallies(ctx);
 }
 
+// Allocation-free transport (see include/nbx.h): device buffers in, device
+// tallies out, scratch from the library's file-scope array.  Nothing here or
+// in run_transport_noalloc allocates memory.
+int nbx_run_noalloc(nbx_ctx* ctx, const float* d_particles, const uint32_t* d_tags, uint32_t n, uint64_t uid_base,
+                    uint32_t* d_se_count, uint32_t* d_bse_count, uint64_t n_tags, uint64_t counts[4]) {
+    if (!ctx || (n && (!d_particles || !d_tags)) || (n_tags && (!d_se_count || !d_bse_count))) return NBX_ERR_ARG;
+    if (!ctx->have_geometry) return fail(ctx, NBX_ERR_STATE, "nbx_run_noalloc before nbx_set_geometry");
+    if (n > NBX_NOALLOC_MAX_PRIMARIES)
+        return fail(ctx, NBX_ERR_ARG, "nbx_run_noalloc takes at most NBX_NOALLOC_MAX_PRIMARIES (65536) primaries per call");
+    ctx->err.clear();
+    if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return fail(ctx, NBX_ERR_CUDA, "cudaSetDevice failed");
+    const char* err = "";
+    const int rc = nbx::run_transport_noalloc(ctx->phys, ctx->sms * ctx->bpsm, ctx->block, ctx->variant, ctx->stream,
+                                              d_particles,
+                                              d_tags, n, uid_base, d_se_count, d_bse_count, n_tags, counts, &err);
+    if (rc != 0) return fail(ctx, rc, err);
+    return NBX_OK;
+}
+
 }  // extern "C"

@@ -15,6 +15,8 @@
 // records are optional.
 #include <cooperative_groups.h>
 
+#include <mutex>
+
 #include "kernels.h"
 #include "transport.cuh"
 
@@ -386,6 +388,141 @@ cudaError_t launch_fill_queue(Queue q, const float* particles, const uint32_t* t
     if (n == 0) return cudaSuccess;
     fill_queue_kernel<<<grid_for(n, 256), 256, 0, s>>>(q, particles, tags, uid_base, n, offset);
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free transport for callers that cannot allocate device memory.
+//
+// Some callers cannot call cudaMalloc: a host application whose own caching
+// allocator already owns the device memory, or a pipeline that must not let
+// an allocation's implicit device synchronisation stall its streams.  For
+// them, nbx_run_noalloc runs the same transport kernel with its scratch
+// (primary queue, two overflow queues for deep cascades, per-generation
+// cursors, counters) carved from the file-scope array below: at most
+// kNoAllocMaxPrimaries primaries per call, about 9.5 MB that every GPU which
+// loads this library holds until the process exits.  Host code cannot use the
+// array's name as a device address, so the first call on each device looks the
+// address up with cudaGetSymbolAddress (with that device current) and caches
+// it; that first call should therefore come before any stream capture.  The
+// array is shared by all calls and keeps the last call's contents; each call
+// clears the cursors and counters it needs.  Calls that overlap on the GPU race
+// on the array and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr size_t kNoAllocOverflow = 1u << 16;
+constexpr int kNoAllocGenerations = 256;
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr size_t kQueueBytes(size_t n) { return align256(n * 16) * 2 + align256(n * 16); }
+constexpr size_t kOffPrim = 0;
+constexpr size_t kOffOv0 = kOffPrim + kQueueBytes(kNoAllocMaxPrimaries);
+constexpr size_t kOffOv1 = kOffOv0 + kQueueBytes(kNoAllocOverflow);
+constexpr size_t kOffCtl = kOffOv1 + kQueueBytes(kNoAllocOverflow);
+constexpr size_t kOffCnt = kOffCtl + align256(sizeof(uint32_t) * (2 * kNoAllocGenerations + 2));
+constexpr size_t kNoAllocScratchBytes = kOffCnt + align256(sizeof(unsigned long long) * kNumCounters);
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mutex;
+void* g_noalloc_base[256] = {};
+
+Queue carve_queue(unsigned char* base, size_t off, size_t n) {
+    Queue q;
+    q.a = reinterpret_cast<float4*>(base + off);
+    q.b = reinterpret_cast<float4*>(base + off + align256(n * 16));
+    q.c = reinterpret_cast<uint4*>(base + off + 2 * align256(n * 16));
+    return q;
+}
+}  // namespace
+
+int run_transport_noalloc(const dev::Physics& P, int grid, int block, int variant, cudaStream_t s,
+                          const float* d_particles,
+                          const uint32_t* d_tags, uint32_t n, uint64_t uid_base, uint32_t* d_se, uint32_t* d_bse,
+                          uint64_t n_tags, uint64_t counts[4], const char** err) {
+    *err = "";
+    if (n > kNoAllocMaxPrimaries) {
+        *err = "nbx_run_noalloc takes at most NBX_NOALLOC_MAX_PRIMARIES primaries per call";
+        return -1;
+    }
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 256) {
+        *err = "cudaGetDevice failed";
+        return -3;
+    }
+    unsigned char* base;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+        if (!g_noalloc_base[device]) {
+            void* ptr = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+            if (e != cudaSuccess || !ptr) {
+                *err = "cudaGetSymbolAddress of the transport scratch failed";
+                return -3;
+            }
+            g_noalloc_base[device] = ptr;
+        }
+        base = static_cast<unsigned char*>(g_noalloc_base[device]);
+    }
+    uint32_t* ctl = reinterpret_cast<uint32_t*>(base + kOffCtl);
+    unsigned long long* cnt = reinterpret_cast<unsigned long long*>(base + kOffCnt);
+    const Queue prim = carve_queue(base, kOffPrim, kNoAllocMaxPrimaries);
+    const Queue ov[2] = {carve_queue(base, kOffOv0, kNoAllocOverflow), carve_queue(base, kOffOv1, kNoAllocOverflow)};
+    auto fail = [&](const char* what) {
+        *err = what;
+        return -3;
+    };
+    if (cudaMemsetAsync(ctl, 0, sizeof(uint32_t) * (2 * kNoAllocGenerations + 2), s) != cudaSuccess ||
+        cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * kNumCounters, s) != cudaSuccess)
+        return fail("clearing the transport scratch failed");
+    if (n == 0) {
+        if (counts) counts[0] = counts[1] = counts[2] = counts[3] = 0;
+        return cudaStreamSynchronize(s) == cudaSuccess ? 0 : fail("stream synchronisation failed");
+    }
+    const uint32_t n_prim = n;
+    if (cudaMemcpyAsync(ctl + 2 * kNoAllocGenerations, &n_prim, 4, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return fail("writing the primary count failed");
+    fill_queue_kernel<<<grid_for(n, 256), 256, 0, s>>>(prim, d_particles, d_tags, uid_base, n, 0);
+    if (cudaGetLastError() != cudaSuccess) return fail("queue fill launch failed");
+
+    TransportArgs a{};
+    a.se_count = d_se;
+    a.bse_count = d_bse;
+    a.n_tags = n_tags;
+    a.counters = cnt;
+    a.out_capacity = uint32_t(kNoAllocOverflow);
+    int g = 0;
+    for (;;) {
+        for (int k = 0; k < 8 && g < kNoAllocGenerations; ++k, ++g) {
+            a.in = g == 0 ? prim : ov[(g - 1) % 2];
+            a.in_capacity = uint32_t(g == 0 ? kNoAllocMaxPrimaries : kNoAllocOverflow);
+            a.out = ov[g % 2];
+            a.n_in = g == 0 ? ctl + 2 * kNoAllocGenerations : ctl + kNoAllocGenerations + (g - 1);
+            a.head = ctl + g;
+            a.out_tail = ctl + kNoAllocGenerations + g;
+            if (launch_transport(P, a, grid, block, variant, s) != cudaSuccess) return fail("transport launch failed");
+        }
+        uint32_t last = 0;
+        if (cudaMemcpyAsync(&last, ctl + kNoAllocGenerations + (g - 1), 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return fail("transport failed");
+        if (last == 0) break;
+        if (g >= kNoAllocGenerations) {
+            *err = "secondary generations exceed the allocation-free limit";
+            return -8;
+        }
+    }
+    unsigned long long c[kNumCounters];
+    if (cudaMemcpy(c, cnt, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) return fail("reading counters failed");
+    if (counts) {
+        counts[0] = c[kCntElastic];
+        counts[1] = c[kCntInelastic];
+        counts[2] = c[kCntBoundary];
+        counts[3] = c[kCntDetected];
+    }
+    if (c[kCntOverflow]) {
+        *err = "overflow queue of the allocation-free transport is full: electrons lost";
+        return -8;
+    }
+    return 0;
 }
 
 }  // namespace nbx
