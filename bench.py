@@ -316,13 +316,20 @@ def main():
 
     # End-to-end through the C ABI from pinned host buffers.
     e2e_s = []
+    parts = {"push_ms": 0.0, "run_ms": 0.0, "yields_ms": 0.0}
     for _ in range(args.steps):
         barrier(dist)
         t0 = time.perf_counter()
         ctx.push(pin_p, pin_t)
+        t1 = time.perf_counter()
         ctx.run()
+        t2 = time.perf_counter()
         out = ctx.pixel_yields(pixel_of_tag, NX * NY)
-        e2e_s.append(time.perf_counter() - t0)
+        t3 = time.perf_counter()
+        e2e_s.append(t3 - t0)
+        parts["push_ms"] += 1000 * (t1 - t0) / args.steps
+        parts["run_ms"] += 1000 * (t2 - t1) / args.steps
+        parts["yields_ms"] += 1000 * (t3 - t2) / args.steps
     t_e2e = allreduce_max(dist, sum(e2e_s))
     e2e_val = ev_all / t_e2e
     h2d = n * 7 * 4 + n * 4
@@ -353,7 +360,7 @@ def main():
             "generations_per_step": gens,
             "gpu_launches": int(launches),
             "e2e": {"value": e2e_val, "unit": "events/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "pinned_host": pinned},
+                    "pinned_host": pinned, "breakdown_ms_per_step": {k: round(v, 2) for k, v in parts.items()}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "bytes_per_event": round(b_event, 2), "bytes_breakdown": b_parts,

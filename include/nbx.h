@@ -170,6 +170,10 @@ typedef struct {
     uint64_t records_dropped;
     uint64_t generations;     /* kernel launches of the last nbx_run */
     uint64_t queue_overflow;
+    uint64_t inferences;      /* warp-level network evaluations (learned mode) */
+    uint64_t roulette_killed; /* electrons ended by Russian roulette (learned mode) */
+    uint64_t splits;          /* electrons split in two (learned mode) */
+    uint64_t samples;         /* training samples recorded (sample mode) */
     double last_run_ms;       /* device time of the last nbx_run (CUDA events) */
     double last_kernel_ms;    /* device time of its transport launches only */
 } nbx_stats;
@@ -197,6 +201,10 @@ int nbx_add_material(nbx_ctx* ctx, const nbx_material* mat);
 int nbx_set_tag_range(nbx_ctx* ctx, uint64_t n_tags);
 /* Queue primaries (host buffers).  *accepted <= n is how many fit. */
 int nbx_push(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n, uint64_t* accepted);
+/* Random-stream index of the next pushed primary (default: running count of
+ * pushed primaries).  Replicas on several GPUs set it to the global index of
+ * their first primary so the combined result does not depend on sharding. */
+int nbx_set_uid_base(nbx_ctx* ctx, uint64_t base);
 /* Simulate every queued electron and all its secondaries to the end. */
 int nbx_run(nbx_ctx* ctx);
 int nbx_get_running_count(nbx_ctx* ctx, uint64_t* n);
@@ -219,6 +227,49 @@ int nbx_reset_tallies(nbx_ctx* ctx);
  * tallies.  Random streams of later pushes are unaffected. */
 int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n,
                  int32_t* blocks_per_sm, int32_t* block_size);
+
+/* ---- escape-probability network (no counterpart in the reference) ------- */
+/* MLP 6 -> 64 -> 64 -> 1 (SiLU, sigmoid), BF16 tensor-core kernels with FP32
+ * accumulation, used only as the importance function of the weighted
+ * roulette / splitting.  Parameters: NBX_MLP_PARAMS floats, row-major
+ * [out][in] with inputs padded to 16 and the output to 8:
+ * W1[64][16] b1[64] W2[64][64] b2[64] W3[8][64] b3[8] (padding forced to 0).
+ * Features (6 per sample): log(E/eV) scaled, distance to the nearest surface
+ * scaled, direction cosine toward that surface's outward normal, material
+ * one-hot (3). */
+#define NBX_MLP_PARAMS 5768
+
+/* Transport modes.  PLAIN: analogue transport (the reference's method).
+ * SAMPLE: plain transport that also records, for about one in sixteen steps
+ * of each electron in a material (at most one record per electron), the
+ * network features with the label "this electron's sub-cascade produced a
+ * detected electron below 50 eV" (nbx_set_sample_capacity, nbx_get_samples).
+ * LEARNED: every rr_period steps in a material the network predicts that
+ * probability p; p < rr_threshold plays Russian roulette (survive with
+ * p / rr_threshold, weight divided by it), p > split_threshold splits the
+ * electron once into two halves of its weight.  Weighted detections go to
+ * nbx_get_tag_weights; the per-tag counts stay unweighted. */
+#define NBX_MODE_PLAIN 0
+#define NBX_MODE_SAMPLE 1
+#define NBX_MODE_LEARNED 2
+int nbx_set_mode(nbx_ctx* ctx, int32_t mode, float rr_threshold, float split_threshold, int32_t rr_period);
+/* Nearest-triangle map over the box [lo, hi) with the given cell size (nm);
+ * surfaces farther than d_max (nm) count as "far".  Needed for the distance
+ * and cosine features. */
+int nbx_build_surface_map(nbx_ctx* ctx, const float lo[3], const float hi[3], float cell, float d_max);
+int nbx_set_sample_capacity(nbx_ctx* ctx, uint64_t capacity);
+/* Copy out (and clear) the recorded samples: features n x 6, labels n. */
+int nbx_get_samples(nbx_ctx* ctx, float* features, float* labels, uint64_t cap, uint64_t* n);
+int nbx_get_tag_weights(nbx_ctx* ctx, uint64_t first_tag, uint64_t n, float* se_w, float* bse_w);
+int nbx_mlp_set_params(nbx_ctx* ctx, const float* params);
+int nbx_mlp_get_params(nbx_ctx* ctx, float* params);
+/* Gradient of the mean binary cross-entropy over n samples at the current
+ * parameters (no update). */
+int nbx_mlp_grad(nbx_ctx* ctx, const float* features, const float* labels, uint64_t n, float* grad, float* loss);
+/* Adam (beta 0.9/0.999, eps 1e-8) over shuffled mini-batches. */
+int nbx_mlp_train(nbx_ctx* ctx, const float* features, const float* labels, uint64_t n, int32_t epochs,
+                  int32_t batch, float lr, uint32_t seed, float* loss_per_epoch);
+int nbx_mlp_predict(nbx_ctx* ctx, const float* features, uint64_t n, float* out);
 
 /* ---- kernel-level queries (host buffers in/out) ------------------------- */
 /* Batched octree propagate; ignore_tri / out_tri index the linearized
@@ -251,6 +302,8 @@ typedef struct {
 } nbx_electron;
 int nbx_step_query(nbx_ctx* ctx, nbx_electron* electrons, uint64_t n, int32_t* status, int32_t* event,
                    nbx_electron* secondaries, int32_t* has_se);
+/* The network's 6 input features for each electron (n x 6 floats). */
+int nbx_features_query(nbx_ctx* ctx, const nbx_electron* electrons, uint64_t n, float* out);
 
 /* ---- allocation-free transport ------------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device

@@ -67,7 +67,8 @@ class Stats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "primaries_pushed", "primaries_done", "steps", "events_elastic", "events_inelastic", "events_boundary",
         "secondaries", "detected", "detected_se", "detected_bse", "terminated", "records_dropped", "generations",
-        "queue_overflow")] + [("last_run_ms", C.c_double), ("last_kernel_ms", C.c_double)]
+        "queue_overflow")] + [("last_run_ms", C.c_double), ("last_kernel_ms", C.c_double)] + [
+        (n, C.c_uint64) for n in ("inferences", "roulette_killed", "splits", "samples")]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -126,6 +127,18 @@ def lib():
         "nbx_table_query": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp, _vp, C.c_uint64, _vp]),
         "nbx_philox": (C.c_int, [_vp, _vp, _vp, C.c_uint64, _vp]),
         "nbx_step_query": (C.c_int, [_vp, _vp, C.c_uint64, _vp, _vp, _vp, _vp]),
+        "nbx_set_uid_base": (C.c_int, [_vp, C.c_uint64]),
+        "nbx_set_mode": (C.c_int, [_vp, C.c_int32, C.c_float, C.c_float, C.c_int32]),
+        "nbx_build_surface_map": (C.c_int, [_vp, _vp, _vp, C.c_float, C.c_float]),
+        "nbx_set_sample_capacity": (C.c_int, [_vp, C.c_uint64]),
+        "nbx_get_samples": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.POINTER(C.c_uint64)]),
+        "nbx_get_tag_weights": (C.c_int, [_vp, C.c_uint64, C.c_uint64, _vp, _vp]),
+        "nbx_features_query": (C.c_int, [_vp, _vp, C.c_uint64, _vp]),
+        "nbx_mlp_set_params": (C.c_int, [_vp, _vp]),
+        "nbx_mlp_get_params": (C.c_int, [_vp, _vp]),
+        "nbx_mlp_grad": (C.c_int, [_vp, _vp, _vp, C.c_uint64, _vp, C.POINTER(C.c_float)]),
+        "nbx_mlp_train": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.c_int32, C.c_int32, C.c_float, C.c_uint32, _vp]),
+        "nbx_mlp_predict": (C.c_int, [_vp, _vp, C.c_uint64, _vp]),
         "nbx_autotune": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
         "nbx_run_noalloc": (C.c_int, [_vp, _vp, _vp, C.c_uint32, C.c_uint64, _vp, _vp, C.c_uint64,
                                       C.POINTER(C.c_uint64)]),
@@ -285,6 +298,9 @@ class Context:
     def run(self):
         self._ck(self.L.nbx_run(self.h))
 
+    def set_uid_base(self, base):
+        self._ck(self.L.nbx_set_uid_base(self.h, base))
+
     def autotune(self, particles: np.ndarray, tags: np.ndarray):
         """Pick the fastest transport variant / block size on a sample; returns (blocks_per_sm, block)."""
         p = np.ascontiguousarray(particles, np.float32).reshape(-1, 7)
@@ -354,6 +370,70 @@ class Context:
         key = np.ascontiguousarray(key, np.uint32).reshape(-1, 2)
         out = np.zeros_like(ctr)
         self._ck(self.L.nbx_philox(self.h, _ptr(ctr), _ptr(key), len(ctr), _ptr(out)))
+        return out
+
+    # ---- learned roulette -------------------------------------------------
+    MODES = {"plain": 0, "sample": 1, "learned": 2}
+
+    def set_mode(self, mode, rr_threshold=0.05, split_threshold=0.5, rr_period=8):
+        self._ck(self.L.nbx_set_mode(self.h, self.MODES.get(mode, mode), rr_threshold, split_threshold, rr_period))
+
+    def build_surface_map(self, lo, hi, cell=1.0, d_max=20.0):
+        lo = np.ascontiguousarray(lo, np.float32)
+        hi = np.ascontiguousarray(hi, np.float32)
+        self._ck(self.L.nbx_build_surface_map(self.h, _ptr(lo), _ptr(hi), cell, d_max))
+
+    def set_sample_capacity(self, n):
+        self._ck(self.L.nbx_set_sample_capacity(self.h, n))
+
+    def get_samples(self, cap):
+        f = np.zeros((cap, 6), np.float32)
+        y = np.zeros(cap, np.float32)
+        n = C.c_uint64()
+        self._ck(self.L.nbx_get_samples(self.h, _ptr(f), _ptr(y), cap, C.byref(n)))
+        return f[: n.value], y[: n.value]
+
+    def tag_weights(self, first, n):
+        se = np.zeros(n, np.float32)
+        bse = np.zeros(n, np.float32)
+        self._ck(self.L.nbx_get_tag_weights(self.h, first, n, _ptr(se), _ptr(bse)))
+        return se, bse
+
+    def features(self, electrons):
+        e = np.ascontiguousarray(electrons, ELECTRON_DTYPE)
+        out = np.zeros((len(e), 6), np.float32)
+        self._ck(self.L.nbx_features_query(self.h, _ptr(e), len(e), _ptr(out)))
+        return out
+
+    def mlp_set_params(self, params):
+        p = np.ascontiguousarray(params, np.float32)
+        assert p.size == 5768
+        self._ck(self.L.nbx_mlp_set_params(self.h, _ptr(p)))
+
+    def mlp_get_params(self):
+        p = np.zeros(5768, np.float32)
+        self._ck(self.L.nbx_mlp_get_params(self.h, _ptr(p)))
+        return p
+
+    def mlp_grad(self, features, labels):
+        f = np.ascontiguousarray(features, np.float32)
+        y = np.ascontiguousarray(labels, np.float32)
+        g = np.zeros(5768, np.float32)
+        loss = C.c_float()
+        self._ck(self.L.nbx_mlp_grad(self.h, _ptr(f), _ptr(y), len(y), _ptr(g), C.byref(loss)))
+        return loss.value, g
+
+    def mlp_train(self, features, labels, epochs=5, batch=8192, lr=1e-3, seed=0):
+        f = np.ascontiguousarray(features, np.float32)
+        y = np.ascontiguousarray(labels, np.float32)
+        losses = np.zeros(epochs, np.float32)
+        self._ck(self.L.nbx_mlp_train(self.h, _ptr(f), _ptr(y), len(y), epochs, batch, lr, seed, _ptr(losses)))
+        return losses
+
+    def mlp_predict(self, features):
+        f = np.ascontiguousarray(features, np.float32)
+        out = np.zeros(len(f), np.float32)
+        self._ck(self.L.nbx_mlp_predict(self.h, _ptr(f), len(f), _ptr(out)))
         return out
 
     def step_query(self, electrons: np.ndarray):

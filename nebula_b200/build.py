@@ -16,7 +16,7 @@ LIB = os.path.join(HERE, "libnbx.so")
 CLI = os.path.join(HERE, "nebula_b200")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_SRCS = ["nbx_api.cpp", "h5lite.cpp", "material.cpp", "octree.cpp"]
-CUDA_SRCS = ["transport.cu"]
+CUDA_SRCS = ["transport.cu", "mlp.cu"]
 
 
 def _nvcc():

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "dev_types.h"
+#include "features.cuh"
 
 namespace nbx {
 
@@ -30,6 +31,10 @@ enum Counter : int {
     kCntRecordsDropped,
     kCntOverflow,
     kCntPopped,
+    kCntInferences,
+    kCntRouletteKilled,
+    kCntSplit,
+    kCntSamples,
     kNumCounters
 };
 
@@ -52,14 +57,38 @@ struct TransportArgs {
     unsigned long long* hist;   // detected-energy histogram
     int n_bins;
     float inv_bin_width;
+    // sample mode: one (features, label) record per sampled electron
+    float* sample_feat;         // [capacity][6]
+    float* sample_label;        // [capacity]: sub-cascade produced a detected SE
+    uint32_t* sample_count;
+    uint32_t sample_capacity;
+    // learned mode: weighted roulette / splitting driven by the network
+    const float* mlp_params;
+    float* se_w;                // per-tag weighted detections below / at or above 50 eV
+    float* bse_w;
+    float rr_threshold;
+    float split_threshold;
+    int rr_period;              // infer every rr_period steps of an electron
+    dev::SurfaceMap smap;
 };
+
+enum : int { kModePlain = 0, kModeSample = 1, kModeLearned = 2 };
 
 constexpr int kLocalStack = 16;  // per-thread stack of parked ancestors (depth-first cascades)
 
-// variant: resident blocks per SM the kernel was compiled for (2, 3 or 4).
+// variant: resident blocks per SM the kernel was compiled for (2, 3 or 4);
+// mode: kModePlain, kModeSample or kModeLearned.
 cudaError_t launch_transport(const dev::Physics& P, const TransportArgs& a, int grid, int block, int variant,
-                             cudaStream_t s);
-int transport_max_blocks_per_sm(int block, int variant);
+                             cudaStream_t s, int mode = kModePlain);
+int transport_max_blocks_per_sm(int block, int variant, int mode = kModePlain);
+// Nearest-triangle map over [lo, lo + n * cell): candidates are triangle
+// indices; cells farther than d_max from all candidates get -1.
+cudaError_t launch_build_surface_map(const float4* tri, const int32_t* candidates, int n_candidates, int32_t* map,
+                                     float lox, float loy, float loz, float cell, int nx, int ny, int nz, float d_max,
+                                     cudaStream_t s);
+// Features of n electrons (56-byte nbx_electron records) for testing.
+cudaError_t launch_features(const dev::Geometry& g, const dev::SurfaceMap& S, const void* electrons, uint64_t n,
+                            float* out, cudaStream_t s);
 
 cudaError_t launch_ray_query(const dev::Geometry& g, const float* pos, const float* dir, const float* dist,
                              const int32_t* ignore_tri, const int32_t* ignore_mat, uint64_t n, float* out_dist,

@@ -20,6 +20,8 @@
 
 #include "kernels.h"
 #include "material.h"
+#include "mlp.cuh"
+#include "mlp_kernels.h"
 #include "nbx.h"
 #include "octree.h"
 
@@ -114,6 +116,24 @@ struct nbx_ctx {
     DevBuf<unsigned long long> hist;
     DevBuf<float4> rec_a, rec_b;
     DevBuf<uint32_t> rec_count;
+    // escape-probability network: FP32 master parameters, Adam moments, gradient
+    DevBuf<float> mlp_params, mlp_m, mlp_v, mlp_grad, mlp_loss;
+    DevBuf<float> mlp_feat, mlp_lab, mlp_out;
+    DevBuf<uint32_t> mlp_index;
+    bool mlp_ready = false;
+    int mlp_step = 0;
+    // transport mode (plain / sample / learned) and its buffers
+    int mode = nbx::kModePlain;
+    float rr_threshold = 0.05f, split_threshold = 0.5f;
+    int rr_period = 8;
+    DevBuf<int32_t> smap_cells;
+    nbx::dev::SurfaceMap smap{};
+    DevBuf<float> sample_feat, sample_label;
+    DevBuf<uint32_t> sample_count;
+    uint64_t sample_cap = 0;
+    DevBuf<float> se_w, bse_w;
+    DevBuf<uint32_t> yield_map;   // nbx_pixel_yields work buffers (grow-only)
+    DevBuf<double> yield_out;
     uint64_t rec_cap = 0;
     // stats
     uint64_t pushed = 0, generations = 0;
@@ -189,6 +209,22 @@ void ensure_tags(nbx_ctx* ctx, uint64_t n_tags) {
     std::swap(ctx->se_count.n, s.n);
     std::swap(ctx->bse_count.p, b.p);
     std::swap(ctx->bse_count.n, b.n);
+    {
+        DevBuf<float> sw, bw;
+        sw.alloc(n_tags);
+        bw.alloc(n_tags);
+        ck(cudaMemsetAsync(sw.p, 0, n_tags * 4, ctx->stream), "memset");
+        ck(cudaMemsetAsync(bw.p, 0, n_tags * 4, ctx->stream), "memset");
+        if (ctx->n_tags) {
+            ck(cudaMemcpyAsync(sw.p, ctx->se_w.p, ctx->n_tags * 4, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+            ck(cudaMemcpyAsync(bw.p, ctx->bse_w.p, ctx->n_tags * 4, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+        }
+        ck(cudaStreamSynchronize(ctx->stream), "sync");
+        std::swap(ctx->se_w.p, sw.p);
+        std::swap(ctx->se_w.n, sw.n);
+        std::swap(ctx->bse_w.p, bw.p);
+        std::swap(ctx->bse_w.n, bw.n);
+    }
     ctx->n_tags = n_tags;
 }
 
@@ -575,7 +611,25 @@ int nbx_run(nbx_ctx* ctx) {
         a.hist = ctx->hist.p;
         a.n_bins = kHistBins;
         a.inv_bin_width = 1.0f / kHistWidth;
-        const int grid = ctx->sms * ctx->bpsm;
+        a.smap = ctx->smap;
+        if (ctx->mode == nbx::kModeSample) {
+            if (!ctx->sample_cap) throw ApiError(NBX_ERR_STATE, "sample mode without nbx_set_sample_capacity");
+            a.sample_feat = ctx->sample_feat.p;
+            a.sample_label = ctx->sample_label.p;
+            a.sample_count = ctx->sample_count.p;
+            a.sample_capacity = uint32_t(std::min<uint64_t>(ctx->sample_cap, 0xFFFFFFF0ull));
+        }
+        if (ctx->mode == nbx::kModeLearned) {
+            if (!ctx->mlp_ready) throw ApiError(NBX_ERR_STATE, "learned mode without network parameters");
+            a.mlp_params = ctx->mlp_params.p;
+            a.se_w = ctx->se_w.p;
+            a.bse_w = ctx->bse_w.p;
+            a.rr_threshold = ctx->rr_threshold;
+            a.split_threshold = ctx->split_threshold;
+            a.rr_period = ctx->rr_period;
+        }
+        const int bpsm = nbx::transport_max_blocks_per_sm(ctx->block, ctx->variant, ctx->mode);
+        const int grid = ctx->sms * bpsm;
 
         ck(cudaEventRecord(ctx->ev0, ctx->stream), "event");
         int g = 0;
@@ -591,7 +645,8 @@ int nbx_run(nbx_ctx* ctx) {
                 a.out_tail = ctl + kMaxGenerations + g;
                 a.out_capacity = cap;
                 a.in_capacity = uint32_t(std::min<uint64_t>(in->cap, 0xFFFFFFF0ull));
-                ck(nbx::launch_transport(ctx->phys, a, grid, ctx->block, ctx->variant, ctx->stream), "transport launch");
+                ck(nbx::launch_transport(ctx->phys, a, grid, ctx->block, ctx->variant, ctx->stream, ctx->mode),
+                   "transport launch");
             }
             uint32_t last = 0;
             ck(cudaMemcpyAsync(&last, ctl + kMaxGenerations + (g - 1), 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
@@ -639,6 +694,10 @@ int nbx_get_stats(nbx_ctx* ctx, nbx_stats* out) {
         out->terminated = c[nbx::kCntTerminated];
         out->records_dropped = c[nbx::kCntRecordsDropped];
         out->queue_overflow = c[nbx::kCntOverflow];
+        out->inferences = c[nbx::kCntInferences];
+        out->roulette_killed = c[nbx::kCntRouletteKilled];
+        out->splits = c[nbx::kCntSplit];
+        out->samples = c[nbx::kCntSamples];
         out->generations = ctx->generations;
         out->last_run_ms = ctx->last_run_ms;
         out->last_kernel_ms = ctx->last_kernel_ms;
@@ -700,15 +759,15 @@ int nbx_pixel_yields(nbx_ctx* ctx, const uint32_t* pixel_of_tag, uint64_t n_tags
     if (!ctx || !pixel_of_tag || !out) return NBX_ERR_ARG;
     if (n_tags > ctx->n_tags) return fail(ctx, NBX_ERR_ARG, "n_tags beyond the tallied range");
     return guarded(ctx, [&] {
-        DevBuf<uint32_t> map;
-        DevBuf<double> res;
-        map.alloc(std::max<uint64_t>(n_tags, 1));
-        res.alloc(std::max<uint64_t>(5 * n_pixels, 1));
-        ck(cudaMemcpyAsync(map.p, pixel_of_tag, 4 * n_tags, cudaMemcpyHostToDevice, ctx->stream), "H2D");
-        ck(cudaMemsetAsync(res.p, 0, 8 * 5 * n_pixels, ctx->stream), "memset");
-        ck(nbx::launch_pixel_yields(ctx->se_count.p, ctx->bse_count.p, map.p, n_tags, n_pixels, res.p, ctx->stream),
+        ctx->yield_map.ensure(std::max<uint64_t>(n_tags, 1));
+        ctx->yield_out.ensure(std::max<uint64_t>(5 * n_pixels, 1));
+        uint32_t* map = ctx->yield_map.p;
+        double* res = ctx->yield_out.p;
+        ck(cudaMemcpyAsync(map, pixel_of_tag, 4 * n_tags, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+        ck(cudaMemsetAsync(res, 0, 8 * 5 * n_pixels, ctx->stream), "memset");
+        ck(nbx::launch_pixel_yields(ctx->se_count.p, ctx->bse_count.p, map, n_tags, n_pixels, res, ctx->stream),
            "pixel yields");
-        ck(cudaMemcpyAsync(out, res.p, 8 * 5 * n_pixels, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        ck(cudaMemcpyAsync(out, res, 8 * 5 * n_pixels, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
         ck(cudaStreamSynchronize(ctx->stream), "sync");
         return NBX_OK;
     });
@@ -734,6 +793,8 @@ int nbx_reset_tallies(nbx_ctx* ctx) {
         if (ctx->n_tags) {
             ck(cudaMemsetAsync(ctx->se_count.p, 0, 4 * ctx->n_tags, ctx->stream), "memset");
             ck(cudaMemsetAsync(ctx->bse_count.p, 0, 4 * ctx->n_tags, ctx->stream), "memset");
+            ck(cudaMemsetAsync(ctx->se_w.p, 0, 4 * ctx->n_tags, ctx->stream), "memset");
+            ck(cudaMemsetAsync(ctx->bse_w.p, 0, 4 * ctx->n_tags, ctx->stream), "memset");
         }
         ck(cudaStreamSynchronize(ctx->stream), "sync");
         ctx->pushed = ctx->n_queued;
@@ -862,6 +923,258 @@ int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* ta
     if (blocks_per_sm) *blocks_per_sm = best_v;
     if (block_size) *block_size = best_b;
     return nbx_reset_tallies(ctx);
+}
+
+int nbx_set_uid_base(nbx_ctx* ctx, uint64_t base) {
+    if (!ctx) return NBX_ERR_ARG;
+    if (base >= (1ull << 63)) return fail(ctx, NBX_ERR_ARG, "uid base must be below 2^63");
+    ctx->uid_next = base;
+    return NBX_OK;
+}
+
+int nbx_set_mode(nbx_ctx* ctx, int32_t mode, float rr_threshold, float split_threshold, int32_t rr_period) {
+    if (!ctx || mode < 0 || mode > 2 || !(rr_threshold >= 0) || !(split_threshold > 0) || rr_period <= 0)
+        return NBX_ERR_ARG;
+    ctx->mode = mode;
+    ctx->rr_threshold = rr_threshold;
+    ctx->split_threshold = split_threshold;
+    ctx->rr_period = rr_period;
+    return NBX_OK;
+}
+
+int nbx_build_surface_map(nbx_ctx* ctx, const float lo[3], const float hi[3], float cell, float d_max) {
+    if (!ctx || !lo || !hi || !(cell > 0) || !(d_max > 0)) return NBX_ERR_ARG;
+    if (!ctx->have_geometry) return fail(ctx, NBX_ERR_STATE, "surface map before nbx_set_geometry");
+    return guarded(ctx, [&] {
+        int n[3];
+        for (int k = 0; k < 3; ++k) {
+            if (!(hi[k] > lo[k])) throw ApiError(NBX_ERR_ARG, "empty surface-map box");
+            n[k] = int(std::ceil((hi[k] - lo[k]) / cell));
+        }
+        const uint64_t cells = uint64_t(n[0]) * n[1] * n[2];
+        if (cells > (1ull << 31)) throw ApiError(NBX_ERR_ARG, "surface map larger than 2^31 cells");
+        // candidates: triangles whose box reaches the map box grown by d_max
+        std::vector<float4> t(3 * size_t(ctx->phys.geo.n_tri));
+        ck(cudaMemcpy(t.data(), ctx->tris.p, sizeof(float4) * t.size(), cudaMemcpyDeviceToHost), "D2H");
+        std::vector<int32_t> cand;
+        for (int i = 0; i < ctx->phys.geo.n_tri; ++i) {
+            const float4 r0 = t[3 * i], e1 = t[3 * i + 1], e2 = t[3 * i + 2];
+            const float xs[3] = {r0.x, r0.x + e1.x, r0.x + e2.x}, ys[3] = {r0.y, r0.y + e1.y, r0.y + e2.y},
+                        zs[3] = {r0.z, r0.z + e1.z, r0.z + e2.z};
+            const float mn[3] = {std::min({xs[0], xs[1], xs[2]}), std::min({ys[0], ys[1], ys[2]}), std::min({zs[0], zs[1], zs[2]})};
+            const float mx[3] = {std::max({xs[0], xs[1], xs[2]}), std::max({ys[0], ys[1], ys[2]}), std::max({zs[0], zs[1], zs[2]})};
+            bool near = true;
+            for (int k = 0; k < 3; ++k) near = near && mx[k] >= lo[k] - d_max && mn[k] <= hi[k] + d_max;
+            int mi;
+            std::memcpy(&mi, &r0.w, 4);
+            if (near && mi >= 0) cand.push_back(i);   // detector / special sheets are not material surfaces
+        }
+        ctx->smap_cells.alloc(std::max<uint64_t>(cells, 1));
+        DevBuf<int32_t> dcand;
+        dcand.alloc(std::max<size_t>(cand.size(), 1));
+        if (!cand.empty())
+            ck(cudaMemcpy(dcand.p, cand.data(), 4 * cand.size(), cudaMemcpyHostToDevice), "H2D");
+        ck(nbx::launch_build_surface_map(ctx->tris.p, dcand.p, int(cand.size()), ctx->smap_cells.p, lo[0], lo[1], lo[2],
+                                         cell, n[0], n[1], n[2], d_max, ctx->stream), "surface map");
+        ck(cudaStreamSynchronize(ctx->stream), "surface map");
+        ctx->smap.cell_tri = ctx->smap_cells.p;
+        ctx->smap.lox = lo[0];
+        ctx->smap.loy = lo[1];
+        ctx->smap.loz = lo[2];
+        ctx->smap.inv_cell = 1.0f / cell;
+        ctx->smap.nx = n[0];
+        ctx->smap.ny = n[1];
+        ctx->smap.nz = n[2];
+        ctx->smap.d_max = d_max;
+        return NBX_OK;
+    });
+}
+
+int nbx_set_sample_capacity(nbx_ctx* ctx, uint64_t capacity) {
+    if (!ctx || capacity == 0) return NBX_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->sample_feat.alloc(6 * capacity);
+        ctx->sample_label.alloc(capacity);
+        ctx->sample_count.alloc(1);
+        ck(cudaMemset(ctx->sample_count.p, 0, 4), "memset");
+        ck(cudaMemset(ctx->sample_label.p, 0, 4 * capacity), "memset");
+        ctx->sample_cap = capacity;
+        return NBX_OK;
+    });
+}
+
+int nbx_get_samples(nbx_ctx* ctx, float* features, float* labels, uint64_t cap, uint64_t* n) {
+    if (!ctx || !n || (cap && (!features || !labels))) return NBX_ERR_ARG;
+    return guarded(ctx, [&] {
+        *n = 0;
+        if (!ctx->sample_cap) return NBX_OK;
+        uint32_t cnt = 0;
+        ck(cudaMemcpy(&cnt, ctx->sample_count.p, 4, cudaMemcpyDeviceToHost), "D2H");
+        const uint64_t have = std::min<uint64_t>(cnt, ctx->sample_cap);
+        const uint64_t take = std::min<uint64_t>(have, cap);
+        if (take) {
+            ck(cudaMemcpy(features, ctx->sample_feat.p, 24 * take, cudaMemcpyDeviceToHost), "D2H");
+            ck(cudaMemcpy(labels, ctx->sample_label.p, 4 * take, cudaMemcpyDeviceToHost), "D2H");
+        }
+        ck(cudaMemset(ctx->sample_count.p, 0, 4), "memset");
+        ck(cudaMemset(ctx->sample_label.p, 0, 4 * ctx->sample_cap), "memset");
+        *n = take;
+        return NBX_OK;
+    });
+}
+
+int nbx_get_tag_weights(nbx_ctx* ctx, uint64_t first, uint64_t n, float* se_w, float* bse_w) {
+    if (!ctx) return NBX_ERR_ARG;
+    if (first + n > ctx->n_tags) return fail(ctx, NBX_ERR_ARG, "tag range beyond nbx_set_tag_range");
+    return guarded(ctx, [&] {
+        if (n == 0) return NBX_OK;
+        if (se_w) ck(cudaMemcpy(se_w, ctx->se_w.p + first, 4 * n, cudaMemcpyDeviceToHost), "D2H");
+        if (bse_w) ck(cudaMemcpy(bse_w, ctx->bse_w.p + first, 4 * n, cudaMemcpyDeviceToHost), "D2H");
+        return NBX_OK;
+    });
+}
+
+int nbx_features_query(nbx_ctx* ctx, const nbx_electron* electrons, uint64_t n, float* out) {
+    if (!ctx || (n && (!electrons || !out))) return NBX_ERR_ARG;
+    if (!ctx->have_geometry) return fail(ctx, NBX_ERR_STATE, "no geometry");
+    return guarded(ctx, [&] {
+        if (n == 0) return NBX_OK;
+        DevBuf<uint8_t> e;
+        DevBuf<float> f;
+        e.alloc(56 * n);
+        f.alloc(6 * n);
+        ck(cudaMemcpyAsync(e.p, electrons, 56 * n, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+        ck(nbx::launch_features(ctx->phys.geo, ctx->smap, e.p, n, f.p, ctx->stream), "features");
+        ck(cudaMemcpyAsync(out, f.p, 24 * n, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        ck(cudaStreamSynchronize(ctx->stream), "sync");
+        return NBX_OK;
+    });
+}
+
+// ---- escape-probability network ----------------------------------------
+namespace {
+void mlp_alloc(nbx_ctx* ctx) {
+    if (ctx->mlp_params.p) return;
+    ctx->mlp_params.alloc(nbx::mlp::kParams);
+    ctx->mlp_m.alloc(nbx::mlp::kParams);
+    ctx->mlp_v.alloc(nbx::mlp::kParams);
+    ctx->mlp_grad.alloc(nbx::mlp::kParams);
+    ctx->mlp_loss.alloc(1);
+    ck(cudaMemset(ctx->mlp_params.p, 0, 4 * nbx::mlp::kParams), "memset");
+    ck(cudaMemset(ctx->mlp_m.p, 0, 4 * nbx::mlp::kParams), "memset");
+    ck(cudaMemset(ctx->mlp_v.p, 0, 4 * nbx::mlp::kParams), "memset");
+}
+void mlp_upload(nbx_ctx* ctx, const float* features, const float* labels, uint64_t n) {
+    ctx->mlp_feat.ensure(std::max<uint64_t>(n, 1) * nbx::mlp::kFeatures);
+    ck(cudaMemcpyAsync(ctx->mlp_feat.p, features, 4 * n * nbx::mlp::kFeatures, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    if (labels) {
+        ctx->mlp_lab.ensure(std::max<uint64_t>(n, 1));
+        ck(cudaMemcpyAsync(ctx->mlp_lab.p, labels, 4 * n, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    }
+}
+}  // namespace
+
+int nbx_mlp_set_params(nbx_ctx* ctx, const float* params) {
+    if (!ctx || !params) return NBX_ERR_ARG;
+    return guarded(ctx, [&] {
+        mlp_alloc(ctx);
+        std::vector<float> p(params, params + nbx::mlp::kParams);
+        // padding entries must stay zero (inputs 6..15, outputs 1..7)
+        for (int o = 0; o < nbx::mlp::kHidden; ++o)
+            for (int i = nbx::mlp::kFeatures; i < nbx::mlp::kIn; ++i) p[nbx::mlp::kOffW1 + o * nbx::mlp::kIn + i] = 0;
+        for (int o = 1; o < nbx::mlp::kOut; ++o) {
+            for (int i = 0; i < nbx::mlp::kHidden; ++i) p[nbx::mlp::kOffW3 + o * nbx::mlp::kHidden + i] = 0;
+            p[nbx::mlp::kOffB3 + o] = 0;
+        }
+        ck(cudaMemcpy(ctx->mlp_params.p, p.data(), 4 * nbx::mlp::kParams, cudaMemcpyHostToDevice), "H2D");
+        ck(cudaMemset(ctx->mlp_m.p, 0, 4 * nbx::mlp::kParams), "memset");
+        ck(cudaMemset(ctx->mlp_v.p, 0, 4 * nbx::mlp::kParams), "memset");
+        ctx->mlp_step = 0;
+        ctx->mlp_ready = true;
+        return NBX_OK;
+    });
+}
+
+int nbx_mlp_get_params(nbx_ctx* ctx, float* out) {
+    if (!ctx || !out) return NBX_ERR_ARG;
+    if (!ctx->mlp_ready) return fail(ctx, NBX_ERR_STATE, "network parameters not set");
+    return guarded(ctx, [&] {
+        ck(cudaMemcpy(out, ctx->mlp_params.p, 4 * nbx::mlp::kParams, cudaMemcpyDeviceToHost), "D2H");
+        return NBX_OK;
+    });
+}
+
+int nbx_mlp_grad(nbx_ctx* ctx, const float* features, const float* labels, uint64_t n, float* grad, float* loss) {
+    if (!ctx || !features || !labels || n == 0 || !grad) return NBX_ERR_ARG;
+    if (!ctx->mlp_ready) return fail(ctx, NBX_ERR_STATE, "network parameters not set");
+    return guarded(ctx, [&] {
+        mlp_upload(ctx, features, labels, n);
+        ck(cudaMemsetAsync(ctx->mlp_grad.p, 0, 4 * nbx::mlp::kParams, ctx->stream), "memset");
+        ck(cudaMemsetAsync(ctx->mlp_loss.p, 0, 4, ctx->stream), "memset");
+        ck(nbx::mlp::launch_train(ctx->mlp_params.p, ctx->mlp_feat.p, ctx->mlp_lab.p, nullptr, 0, n, 1.0f / float(n),
+                                  ctx->mlp_grad.p, ctx->mlp_loss.p, ctx->stream), "train kernel");
+        ck(cudaMemcpyAsync(grad, ctx->mlp_grad.p, 4 * nbx::mlp::kParams, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        float l = 0;
+        ck(cudaMemcpyAsync(&l, ctx->mlp_loss.p, 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        ck(cudaStreamSynchronize(ctx->stream), "sync");
+        if (loss) *loss = l;
+        return NBX_OK;
+    });
+}
+
+int nbx_mlp_train(nbx_ctx* ctx, const float* features, const float* labels, uint64_t n, int32_t epochs,
+                  int32_t batch, float lr, uint32_t seed, float* loss_per_epoch) {
+    if (!ctx || !features || !labels || n == 0 || epochs <= 0 || batch <= 0 || !(lr > 0)) return NBX_ERR_ARG;
+    if (!ctx->mlp_ready) return fail(ctx, NBX_ERR_STATE, "network parameters not set");
+    return guarded(ctx, [&] {
+        mlp_upload(ctx, features, labels, n);
+        ctx->mlp_index.ensure(n);
+        std::vector<uint32_t> perm(n);
+        uint64_t state = 0x9E3779B97F4A7C15ull ^ seed;
+        auto next = [&]() {   // splitmix64
+            uint64_t z = (state += 0x9E3779B97F4A7C15ull);
+            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+            z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+            return z ^ (z >> 31);
+        };
+        for (int ep = 0; ep < epochs; ++ep) {
+            for (uint64_t i = 0; i < n; ++i) perm[i] = uint32_t(i);
+            for (uint64_t i = n - 1; i > 0; --i) std::swap(perm[i], perm[next() % (i + 1)]);
+            ck(cudaMemcpyAsync(ctx->mlp_index.p, perm.data(), 4 * n, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+            ck(cudaMemsetAsync(ctx->mlp_loss.p, 0, 4, ctx->stream), "memset");
+            uint64_t n_batches = 0;
+            for (uint64_t first = 0; first + uint64_t(batch) <= n || (first == 0 && n < uint64_t(batch));
+                 first += uint64_t(batch)) {
+                const uint64_t count = std::min<uint64_t>(uint64_t(batch), n - first);
+                ck(cudaMemsetAsync(ctx->mlp_grad.p, 0, 4 * nbx::mlp::kParams, ctx->stream), "memset");
+                ck(nbx::mlp::launch_train(ctx->mlp_params.p, ctx->mlp_feat.p, ctx->mlp_lab.p, ctx->mlp_index.p, first,
+                                          count, 1.0f / float(count), ctx->mlp_grad.p, ctx->mlp_loss.p, ctx->stream),
+                   "train kernel");
+                ck(nbx::mlp::launch_adam(ctx->mlp_params.p, ctx->mlp_grad.p, ctx->mlp_m.p, ctx->mlp_v.p, lr, 0.9f,
+                                         0.999f, 1e-8f, ++ctx->mlp_step, ctx->stream), "adam kernel");
+                ++n_batches;
+            }
+            float l = 0;
+            ck(cudaMemcpyAsync(&l, ctx->mlp_loss.p, 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+            ck(cudaStreamSynchronize(ctx->stream), "sync");
+            if (loss_per_epoch) loss_per_epoch[ep] = l / float(std::max<uint64_t>(n_batches, 1));
+        }
+        return NBX_OK;
+    });
+}
+
+int nbx_mlp_predict(nbx_ctx* ctx, const float* features, uint64_t n, float* out) {
+    if (!ctx || !features || !out) return NBX_ERR_ARG;
+    if (!ctx->mlp_ready) return fail(ctx, NBX_ERR_STATE, "network parameters not set");
+    return guarded(ctx, [&] {
+        if (n == 0) return NBX_OK;
+        mlp_upload(ctx, features, nullptr, n);
+        ctx->mlp_out.ensure(n);
+        ck(nbx::mlp::launch_predict(ctx->mlp_params.p, ctx->mlp_feat.p, n, ctx->mlp_out.p, ctx->stream), "predict");
+        ck(cudaMemcpyAsync(out, ctx->mlp_out.p, 4 * n, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        ck(cudaStreamSynchronize(ctx->stream), "sync");
+        return NBX_OK;
+    });
 }
 
 // Allocation-free transport (see include/nbx.h): device buffers in, device

@@ -16,8 +16,11 @@
 #include <cooperative_groups.h>
 
 #include <mutex>
+#include <type_traits>
 
+#include "features.cuh"
 #include "kernels.h"
+#include "mlp.cuh"
 #include "transport.cuh"
 
 namespace cg = cooperative_groups;
@@ -56,28 +59,68 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
     return v;
 }
 
+struct LearnedSmem {
+    mlp::Weights w;
+    __nv_bfloat16 xs[8 * 32 * mlp::kIn];
+};
+
+// Per-electron state of the sample and learned modes, parked alongside the
+// electron on the cascade stack.
+struct Extra {
+    float w;          // statistical weight (learned mode)
+    int rec;          // sample record slot, -1 none (sample mode)
+    uint32_t flags;   // bit 0: sub-cascade produced a detected SE; bit 1: already split
+};
+
+__device__ __forceinline__ uint32_t mix32(uint64_t x) {
+    x ^= x >> 33;
+    x *= 0xFF51AFD7ED558CCDull;
+    x ^= x >> 33;
+    return uint32_t(x);
+}
+
 // MinBlocks: resident 256-thread blocks per SM the register allocation must
 // allow (2: 128 registers, 3: 80, 4: 64); the host picks the variant.
-template <int MinBlocks>
+// Mode: kModePlain (analogue transport), kModeSample (plain transport that
+// also records one (features, label) training sample per sampled electron)
+// or kModeLearned (weighted roulette / splitting with the network as the
+// importance function; the warp stays converged for the tensor-core
+// inference, so lanes without work idle until the whole warp is done).
+template <int MinBlocks, int Mode>
 __global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Physics P, const TransportArgs a) {
     __shared__ float leaf_cache[13 * 256];
     const dev::LeafCache cache{leaf_cache + threadIdx.x, int(blockDim.x)};
     cache.f(0) = 0.0f;   // location 0: empty
     cache.f(1) = 0.0f;
+    constexpr bool kExtra = (Mode != kModePlain);
+    // network weights and one 32 x 16 feature tile per warp (learned mode only)
+    __shared__ __align__(16) typename std::conditional<Mode == kModeLearned, LearnedSmem, char>::type lsm;
+    if constexpr (Mode == kModeLearned) {
+        mlp::load_weights(lsm.w, a.mlp_params);
+        __syncthreads();
+    }
     const uint32_t n_in = min(*a.n_in, a.in_capacity);
     dev::Electron e;
     // Child-first depth-first cascade: when an event creates a secondary the
     // parent is parked here and the secondary is simulated at once, so the
     // stack only ever holds the current electron's ancestors.
     dev::Electron stack[kLocalStack];
+    Extra ex{1.0f, -1, 0u};
+    Extra exs[kExtra ? kLocalStack : 1];
     int sp = 0;
-    bool alive = false;
+    bool alive = false, drained = false;
+    uint32_t carry_hit = 0;
     unsigned long long c_steps = 0, c_el = 0, c_inel = 0, c_bd = 0, c_se = 0, c_det = 0, c_dse = 0, c_dbse = 0,
-                       c_term = 0, c_drop = 0, c_ovf = 0, c_pop = 0;
+                       c_term = 0, c_drop = 0, c_ovf = 0, c_pop = 0, c_inf = 0, c_kill = 0, c_split = 0, c_smp = 0;
     for (;;) {
-        if (!alive) {
+        if (!alive && !drained) {
             if (sp > 0) {
                 e = stack[--sp];
+                if constexpr (kExtra) {
+                    ex = exs[sp];
+                    ex.flags |= carry_hit;
+                    carry_hit = 0;
+                }
                 alive = true;
             } else {
                 uint32_t idx;
@@ -88,10 +131,80 @@ __global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Ph
                     base = g.shfl(base, 0);
                     idx = base + g.thread_rank();
                 }
-                if (idx >= n_in) break;
-                load_electron(a.in, idx, e);
-                ++c_pop;
-                alive = true;
+                if (idx >= n_in) {
+                    drained = true;
+                } else {
+                    load_electron(a.in, idx, e);
+                    if constexpr (kExtra) {
+                        const uint32_t wbits = a.in.c[idx].w;
+                        ex.w = (Mode == kModeLearned && wbits != 0xFFFFFFFFu) ? __uint_as_float(wbits) : 1.0f;
+                        ex.rec = -1;
+                        ex.flags = 0;
+                        carry_hit = 0;
+                    }
+                    ++c_pop;
+                    alive = true;
+                }
+            }
+        }
+        if constexpr (Mode == kModeLearned) {
+            if (__all_sync(0xffffffffu, !alive)) break;
+            const bool want = alive && e.mat >= 0 && (e.step % uint32_t(a.rr_period)) == 0;
+            if (__any_sync(0xffffffffu, want)) {
+                ++c_inf;
+                __nv_bfloat16* xs = lsm.xs + (threadIdx.x >> 5) * 32 * mlp::kIn;
+                float f[6] = {0, 0, 0, 0, 0, 0};
+                if (want) {
+                    const dev::V3 d = dev::normalised(dev::V3{e.dx, e.dy, e.dz});
+                    dev::electron_features(P.geo, a.smap, e.px, e.py, e.pz, d.x, d.y, d.z, logf(e.E), e.mat, f);
+                }
+                const int lane = threadIdx.x & 31;
+#pragma unroll
+                for (int k = 0; k < mlp::kIn; ++k) xs[lane * mlp::kIn + k] = __float2bfloat16_rn(k < 6 ? f[k] : 0.0f);
+                __syncwarp();
+                const float logit = mlp::warp_forward(lsm.w, xs);
+                __syncwarp();
+                if (want) {
+                    const float pr = mlp::sigmoid(logit);
+                    if (pr < a.rr_threshold) {
+                        // Russian roulette: survive with q = p / threshold, weight / q.
+                        const float q = fmaxf(pr / a.rr_threshold, 1e-3f);
+                        const float u = dev::u01(dev::draw(P.seed, e, 2).x);
+                        if (u < q) {
+                            ex.w /= q;
+                        } else {
+                            alive = false;
+                            ++c_kill;
+                        }
+                    } else if (pr > a.split_threshold && !(ex.flags & 2u) && sp < kLocalStack) {
+                        // Split in two halves of the weight; the copy follows
+                        // its own random stream.
+                        ex.w *= 0.5f;
+                        ex.flags |= 2u;
+                        stack[sp] = e;
+                        stack[sp].uid = dev::secondary_uid(e.uid ^ 0x5DEECE66Dull, e.step);
+                        exs[sp] = ex;
+                        ++sp;
+                        ++c_split;
+                    }
+                }
+            }
+            if (!alive) continue;
+        } else {
+            if (!alive) break;
+        }
+        if constexpr (Mode == kModeSample) {
+            if (ex.rec < 0 && e.mat >= 0 && (mix32(e.uid ^ (uint64_t(e.step) << 40)) & 15u) == 0) {
+                const uint32_t slot = atomicAdd(a.sample_count, 1u);
+                if (slot < a.sample_capacity) {
+                    float f[6];
+                    const dev::V3 d = dev::normalised(dev::V3{e.dx, e.dy, e.dz});
+                    dev::electron_features(P.geo, a.smap, e.px, e.py, e.pz, d.x, d.y, d.z, logf(e.E), e.mat, f);
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) a.sample_feat[size_t(slot) * 6 + k] = f[k];
+                    ex.rec = int(slot);
+                    ++c_smp;
+                }
             }
         }
         int ev;
@@ -106,8 +219,14 @@ __global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Ph
             // an inelastic step never ends its electron: st == kAlive here
             ++c_se;
             if (sp < kLocalStack) {
-                stack[sp++] = e;
+                stack[sp] = e;
+                if constexpr (kExtra) exs[sp] = ex;
+                ++sp;
                 e = se;
+                if constexpr (kExtra) {
+                    ex.rec = -1;
+                    ex.flags = 0;   // the secondary inherits the weight only
+                }
                 continue;
             }
             // Deep cascade: hand the secondary to the next generation.
@@ -116,36 +235,48 @@ __global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Ph
             if (g.thread_rank() == 0) base = atomicAdd(a.out_tail, g.size());
             base = g.shfl(base, 0);
             const uint32_t slot = base + g.thread_rank();
-            if (slot < a.out_capacity)
+            if (slot < a.out_capacity) {
                 store_electron(a.out, slot, se);
-            else
+                if constexpr (Mode == kModeLearned) a.out.c[slot].w = __float_as_uint(ex.w);
+            } else {
                 ++c_ovf;
+            }
         }
         if (st == dev::kAlive) continue;
         alive = false;
+        uint32_t hit = 0;
         if (st == dev::kTerminated) {
             ++c_term;
-            continue;
-        }
-        // detected
-        ++c_det;
-        const bool is_se = e.E < 50;
-        c_dse += is_se;
-        c_dbse += !is_se;
-        if (e.tag < a.n_tags) atomicAdd(is_se ? a.se_count + e.tag : a.bse_count + e.tag, 1u);
-        if (a.hist) {
-            int bin = dev::floor_to_int(e.E * a.inv_bin_width);
-            bin = bin < 0 ? 0 : (bin >= a.n_bins ? a.n_bins - 1 : bin);
-            atomicAdd(a.hist + bin, 1ull);
-        }
-        if (a.rec_a) {
-            const uint32_t slot = atomicAdd(a.rec_count, 1u);
-            if (slot < a.rec_capacity) {
-                a.rec_a[slot] = make_float4(e.px, e.py, e.pz, e.E);
-                a.rec_b[slot] = make_float4(e.dx, e.dy, e.dz, __uint_as_float(e.tag));
-            } else {
-                ++c_drop;
+        } else {
+            // detected
+            ++c_det;
+            const bool is_se = e.E < 50;
+            hit = is_se ? 1u : 0u;
+            c_dse += is_se;
+            c_dbse += !is_se;
+            if (e.tag < a.n_tags) {
+                atomicAdd(is_se ? a.se_count + e.tag : a.bse_count + e.tag, 1u);
+                if constexpr (Mode == kModeLearned) atomicAdd(is_se ? a.se_w + e.tag : a.bse_w + e.tag, ex.w);
             }
+            if (a.hist) {
+                int bin = dev::floor_to_int(e.E * a.inv_bin_width);
+                bin = bin < 0 ? 0 : (bin >= a.n_bins ? a.n_bins - 1 : bin);
+                atomicAdd(a.hist + bin, 1ull);
+            }
+            if (a.rec_a) {
+                const uint32_t slot = atomicAdd(a.rec_count, 1u);
+                if (slot < a.rec_capacity) {
+                    a.rec_a[slot] = make_float4(e.px, e.py, e.pz, e.E);
+                    a.rec_b[slot] = make_float4(e.dx, e.dy, e.dz, __uint_as_float(e.tag));
+                } else {
+                    ++c_drop;
+                }
+            }
+        }
+        if constexpr (Mode == kModeSample) {
+            const uint32_t sub = (ex.flags | hit) & 1u;
+            if (ex.rec >= 0) a.sample_label[ex.rec] = float(sub);
+            carry_hit = sub;
         }
     }
     // Counters: one atomic per warp per counter.
@@ -162,6 +293,10 @@ __global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Ph
     v[kCntRecordsDropped] = c_drop;
     v[kCntOverflow] = c_ovf;
     v[kCntPopped] = c_pop;
+    v[kCntInferences] = c_inf;
+    v[kCntRouletteKilled] = c_kill;
+    v[kCntSplit] = c_split;
+    v[kCntSamples] = c_smp;
     __syncwarp();
     const int lane = threadIdx.x & 31;
 #pragma unroll
@@ -323,26 +458,91 @@ int grid_for(uint64_t n, int block) {
 
 }  // namespace
 
-cudaError_t launch_transport(const dev::Physics& P, const TransportArgs& a, int grid, int block, int variant,
-                             cudaStream_t s) {
+template <int Mode>
+static cudaError_t launch_mode(const dev::Physics& P, const TransportArgs& a, int grid, int block, int variant,
+                               cudaStream_t s) {
     switch (variant) {
-    case 2: transport_kernel<2><<<grid, block, 0, s>>>(P, a); break;
-    case 4: transport_kernel<4><<<grid, block, 0, s>>>(P, a); break;
-    default: transport_kernel<3><<<grid, block, 0, s>>>(P, a); break;
+    case 2: transport_kernel<2, Mode><<<grid, block, 0, s>>>(P, a); break;
+    case 4: transport_kernel<4, Mode><<<grid, block, 0, s>>>(P, a); break;
+    default: transport_kernel<3, Mode><<<grid, block, 0, s>>>(P, a); break;
     }
     return cudaGetLastError();
 }
 
-int transport_max_blocks_per_sm(int block, int variant) {
+cudaError_t launch_transport(const dev::Physics& P, const TransportArgs& a, int grid, int block, int variant,
+                             cudaStream_t s, int mode) {
+    if (mode == kModeSample) return launch_mode<kModeSample>(P, a, grid, block, variant, s);
+    if (mode == kModeLearned) return launch_mode<kModeLearned>(P, a, grid, block, variant, s);
+    return launch_mode<kModePlain>(P, a, grid, block, variant, s);
+}
+
+template <int Mode>
+static int max_blocks_mode(int block, int variant) {
     int n = 0;
     cudaError_t e;
     switch (variant) {
-    case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<2>, block, 0); break;
-    case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<4>, block, 0); break;
-    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<3>, block, 0); break;
+    case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<2, Mode>, block, 0); break;
+    case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<4, Mode>, block, 0); break;
+    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<3, Mode>, block, 0); break;
     }
     if (e != cudaSuccess) return 1;
     return n > 0 ? n : 1;
+}
+
+int transport_max_blocks_per_sm(int block, int variant, int mode) {
+    if (mode == kModeSample) return max_blocks_mode<kModeSample>(block, variant);
+    if (mode == kModeLearned) return max_blocks_mode<kModeLearned>(block, variant);
+    return max_blocks_mode<kModePlain>(block, variant);
+}
+
+namespace {
+__global__ void build_surface_map_kernel(const float4* tri, const int32_t* cand, int n_cand, int32_t* map, float lox,
+                                         float loy, float loz, float cell, int nx, int ny, int nz, float d_max) {
+    const uint64_t n = uint64_t(nx) * ny * nz;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const int ix = int(i % nx), iy = int((i / nx) % ny), iz = int(i / (uint64_t(nx) * ny));
+        const float px = lox + (ix + 0.5f) * cell, py = loy + (iy + 0.5f) * cell, pz = loz + (iz + 0.5f) * cell;
+        float best = d_max * d_max;
+        int bi = -1;
+        for (int k = 0; k < n_cand; ++k) {
+            const int ti = __ldg(cand + k);
+            const float d2 = dev::dist2_to_triangle(tri, ti, px, py, pz);
+            if (d2 < best) {
+                best = d2;
+                bi = ti;
+            }
+        }
+        map[i] = bi;
+    }
+}
+
+__global__ void features_kernel(const dev::Geometry g, const dev::SurfaceMap S, const ElectronRecord* el, uint64_t n,
+                                float* out) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const ElectronRecord& r = el[i];
+        const dev::V3 d = dev::normalised(dev::V3{r.dir[0], r.dir[1], r.dir[2]});
+        float f[6];
+        dev::electron_features(g, S, r.pos[0], r.pos[1], r.pos[2], d.x, d.y, d.z, logf(r.E), r.mat, f);
+        for (int k = 0; k < 6; ++k) out[6 * i + k] = f[k];
+    }
+}
+}  // namespace
+
+cudaError_t launch_build_surface_map(const float4* tri, const int32_t* candidates, int n_candidates, int32_t* map,
+                                     float lox, float loy, float loz, float cell, int nx, int ny, int nz, float d_max,
+                                     cudaStream_t s) {
+    const uint64_t n = uint64_t(nx) * ny * nz;
+    if (n == 0) return cudaSuccess;
+    build_surface_map_kernel<<<grid_for(n, 128), 128, 0, s>>>(tri, candidates, n_candidates, map, lox, loy, loz, cell,
+                                                              nx, ny, nz, d_max);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_features(const dev::Geometry& g, const dev::SurfaceMap& S, const void* electrons, uint64_t n,
+                            float* out, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    features_kernel<<<grid_for(n, 128), 128, 0, s>>>(g, S, static_cast<const ElectronRecord*>(electrons), n, out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_ray_query(const dev::Geometry& g, const float* pos, const float* dir, const float* dist,
