@@ -238,6 +238,8 @@ def main():
     ap.add_argument("--impl", default="nbx", choices=["nbx", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=NY, help="pixel rows of the scan (profiling runs use fewer)")
+    ap.add_argument("--variant", type=int, default=0, help="transport variant 2/3/4 (0: autotune)")
+    ap.add_argument("--block", type=int, default=0, help="threads per block with --variant (0: 128)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -269,8 +271,15 @@ def main():
     pin_t[:] = tags
     ctx.set_tag_range(n)
     # Autotune the transport launch shape on a 16-row sample of the scan.
-    sample = np.arange(min(n, 16 * NX * PER_PIXEL))   # records are row-major: the first 16 rows
-    tuned = ctx.autotune(prim[sample], tags[sample])
+    if args.variant:
+        ctx.close()
+        ctx = nb.setup(tris, [mat], device=local, seed=0x78C7E39B + rank, blocks_per_sm=args.variant,
+                       block_size=args.block or 128)
+        ctx.set_tag_range(n)
+        tuned = (args.variant, args.block or 128)
+    else:
+        sample = np.arange(min(n, 16 * NX * PER_PIXEL))   # records are row-major: the first 16 rows
+        tuned = ctx.autotune(prim[sample], tags[sample])
 
     def one_step():
         ctx.push(pin_p, pin_t)

@@ -244,11 +244,15 @@ int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* ta
  * of each electron in a material (at most one record per electron), the
  * network features with the label "this electron's sub-cascade produced a
  * detected electron below 50 eV" (nbx_set_sample_capacity, nbx_get_samples).
- * LEARNED: every rr_period steps in a material the network predicts that
- * probability p; p < rr_threshold plays Russian roulette (survive with
- * p / rr_threshold, weight divided by it), p > split_threshold splits the
- * electron once into two halves of its weight.  Weighted detections go to
- * nbx_get_tag_weights; the per-tag counts stay unweighted. */
+ * LEARNED: every rr_period iterations of a warp the network predicts that
+ * probability p for each of its electrons in a material, and a weight window
+ * acts on it: the target weight is min(rr_threshold / p, 32) when
+ * p < rr_threshold and 1 otherwise; an electron lighter than half its target
+ * plays Russian roulette (survives with weight / target, then carries the
+ * target weight); one heavier than twice its target with p > split_threshold
+ * is split into two halves.  The expected weighted tally is unchanged (the
+ * method stays unbiased).  Weighted detections go to nbx_get_tag_weights;
+ * the per-tag counts stay unweighted. */
 #define NBX_MODE_PLAIN 0
 #define NBX_MODE_SAMPLE 1
 #define NBX_MODE_LEARNED 2

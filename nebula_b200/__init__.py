@@ -67,8 +67,8 @@ class Stats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "primaries_pushed", "primaries_done", "steps", "events_elastic", "events_inelastic", "events_boundary",
         "secondaries", "detected", "detected_se", "detected_bse", "terminated", "records_dropped", "generations",
-        "queue_overflow")] + [("last_run_ms", C.c_double), ("last_kernel_ms", C.c_double)] + [
-        (n, C.c_uint64) for n in ("inferences", "roulette_killed", "splits", "samples")]
+        "queue_overflow", "inferences", "roulette_killed", "splits", "samples")] + [
+        ("last_run_ms", C.c_double), ("last_kernel_ms", C.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

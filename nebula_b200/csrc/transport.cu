@@ -59,6 +59,9 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
     return v;
 }
 
+// Largest weight the roulette may give a survivor.
+constexpr float kMaxWeight = 32.0f;
+
 struct LearnedSmem {
     mlp::Weights w;
     __nv_bfloat16 xs[8 * 32 * mlp::kIn];
@@ -108,6 +111,7 @@ __global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Ph
     Extra ex{1.0f, -1, 0u};
     Extra exs[kExtra ? kLocalStack : 1];
     int sp = 0;
+    int warp_iter = 0;
     bool alive = false, drained = false;
     uint32_t carry_hit = 0;
     unsigned long long c_steps = 0, c_el = 0, c_inel = 0, c_bd = 0, c_se = 0, c_det = 0, c_dse = 0, c_dbse = 0,
@@ -149,43 +153,52 @@ __global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Ph
         }
         if constexpr (Mode == kModeLearned) {
             if (__all_sync(0xffffffffu, !alive)) break;
-            const bool want = alive && e.mat >= 0 && (e.step % uint32_t(a.rr_period)) == 0;
-            if (__any_sync(0xffffffffu, want)) {
-                ++c_inf;
-                __nv_bfloat16* xs = lsm.xs + (threadIdx.x >> 5) * 32 * mlp::kIn;
-                float f[6] = {0, 0, 0, 0, 0, 0};
-                if (want) {
-                    const dev::V3 d = dev::normalised(dev::V3{e.dx, e.dy, e.dz});
-                    dev::electron_features(P.geo, a.smap, e.px, e.py, e.pz, d.x, d.y, d.z, logf(e.E), e.mat, f);
-                }
-                const int lane = threadIdx.x & 31;
+            // Every rr_period iterations of the (converged) warp, all its
+            // electrons in a material are scored together on the tensor cores.
+            if (++warp_iter == a.rr_period) {
+                warp_iter = 0;
+                const bool want = alive && e.mat >= 0;
+                if (__any_sync(0xffffffffu, want)) {
+                    ++c_inf;
+                    __nv_bfloat16* xs = lsm.xs + (threadIdx.x >> 5) * 32 * mlp::kIn;
+                    float f[6] = {0, 0, 0, 0, 0, 0};
+                    if (want) {
+                        const dev::V3 d = dev::normalised(dev::V3{e.dx, e.dy, e.dz});
+                        dev::electron_features(P.geo, a.smap, e.px, e.py, e.pz, d.x, d.y, d.z, logf(e.E), e.mat, f);
+                    }
+                    const int lane = threadIdx.x & 31;
 #pragma unroll
-                for (int k = 0; k < mlp::kIn; ++k) xs[lane * mlp::kIn + k] = __float2bfloat16_rn(k < 6 ? f[k] : 0.0f);
-                __syncwarp();
-                const float logit = mlp::warp_forward(lsm.w, xs);
-                __syncwarp();
-                if (want) {
-                    const float pr = mlp::sigmoid(logit);
-                    if (pr < a.rr_threshold) {
-                        // Russian roulette: survive with q = p / threshold, weight / q.
-                        const float q = fmaxf(pr / a.rr_threshold, 1e-3f);
-                        const float u = dev::u01(dev::draw(P.seed, e, 2).x);
-                        if (u < q) {
-                            ex.w /= q;
-                        } else {
-                            alive = false;
-                            ++c_kill;
+                    for (int k = 0; k < mlp::kIn; ++k)
+                        xs[lane * mlp::kIn + k] = __float2bfloat16_rn(k < 6 ? f[k] : 0.0f);
+                    __syncwarp();
+                    const float logit = mlp::warp_forward(lsm.w, xs);
+                    __syncwarp();
+                    if (want) {
+                        // Weight window on the importance p: target weight
+                        // min(rr_threshold / p, w_max) below the threshold, 1
+                        // above it.  Lighter than half the target: Russian
+                        // roulette up to the target; heavier than twice it
+                        // and important (p > split_threshold): split in two.
+                        const float pr = mlp::sigmoid(logit);
+                        const float target =
+                            pr < a.rr_threshold ? fminf(a.rr_threshold / fmaxf(pr, 1e-12f), kMaxWeight) : 1.0f;
+                        if (ex.w < 0.5f * target) {
+                            const float q = ex.w / target;
+                            const float u = dev::u01(dev::draw(P.seed, e, 2).x);
+                            if (u < q) {
+                                ex.w = target;
+                            } else {
+                                alive = false;
+                                ++c_kill;
+                            }
+                        } else if (pr > a.split_threshold && ex.w > 2.0f * target && sp < kLocalStack) {
+                            ex.w *= 0.5f;
+                            stack[sp] = e;
+                            stack[sp].uid = dev::secondary_uid(e.uid ^ 0x5DEECE66Dull, e.step);
+                            exs[sp] = ex;
+                            ++sp;
+                            ++c_split;
                         }
-                    } else if (pr > a.split_threshold && !(ex.flags & 2u) && sp < kLocalStack) {
-                        // Split in two halves of the weight; the copy follows
-                        // its own random stream.
-                        ex.w *= 0.5f;
-                        ex.flags |= 2u;
-                        stack[sp] = e;
-                        stack[sp].uid = dev::secondary_uid(e.uid ^ 0x5DEECE66Dull, e.step);
-                        exs[sp] = ex;
-                        ++sp;
-                        ++c_split;
                     }
                 }
             }

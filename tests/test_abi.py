@@ -64,3 +64,12 @@ def test_cli_usage_and_errors(tmp_path):
     assert r.returncode == 1 and "Usage" in r.stderr
     r = subprocess.run([cli, "--bogus=1", "a", "b", "c"], capture_output=True, text=True)
     assert r.returncode != 0
+
+
+def test_stats_struct_matches_header():
+    """The ctypes mirror of nbx_stats lists the header's fields in order."""
+    text = open(os.path.join(ROOT, "include", "nbx.h")).read()
+    body = text[text.index("typedef struct {\n    uint64_t primaries_pushed;"):]
+    body = body[: body.index("} nbx_stats;")]
+    fields = re.findall(r"^\s*(?:uint64_t|double)\s+(\w+);", body, flags=re.M)
+    assert fields == [f for f, _ in nb.Stats._fields_]

@@ -233,14 +233,15 @@ def _chi2_two_sample(h1, h2):
 
 
 def test_whole_run_vs_reference_cpu(inputs, oracle_built, tmp_path):
-    """Cube, 10^4 primaries at 1 keV (the reference's CPU-sized config):
+    """Cube, 3 x 10^4 primaries at 1 keV (the reference's CPU-sized config):
     per-primary SE/BSE yields within 3 sigma, exit-energy spectrum chi-square
     within 3 sqrt(2 dof)."""
     tri = inputs["cube_tri"]
-    recs = g.point_beam(10000, 1000.0, pos=(0.0, 0.0, 1.0))
+    recs = g.point_beam(30000, 1000.0, pos=(0.0, 0.0, 1.0))
     pri = str(tmp_path / "c1.pri")
     formats.write_pri(pri, recs)
-    ref_recs, st, _ = oracle.ref_run(tri, pri, [inputs["si"]], seed=1, count_events=True)
+    # one reference thread: a deterministic sample for the fixed seed
+    ref_recs, st, _ = oracle.ref_run(tri, pri, [inputs["si"]], seed=1, threads=1, count_events=True)
     ctx = nb.setup(inputs["cube"], [inputs["si"]], device=0, seed=5, record_detected=True)
     s, se, bse = _run_gpu(ctx, recs)
     det = ctx.flush_detected()
@@ -303,7 +304,7 @@ def test_whole_run_grating_rows_vs_reference(inputs, oracle_built, tmp_path):
     tagged["py"] = 0
     pri = str(tmp_path / "c2.pri")
     formats.write_pri(pri, tagged)
-    ref_recs, st, _ = oracle.ref_run(tri, pri, [inputs["si"]], seed=2)
+    ref_recs, st, _ = oracle.ref_run(tri, pri, [inputs["si"]], seed=2, threads=1)
     rse, rbse = _per_primary_from_records(ref_recs, n)
     ctx = nb.setup(inputs["grating"], [inputs["si"]], device=0, seed=6)
     s, se, bse = _run_gpu(ctx, recs)
