@@ -230,6 +230,56 @@ def run_reference(args):
     return 0
 
 
+def learned_fom(args, tris, mat, local, rank, prim, tags, mean_plain, var_plain, fom_plain):
+    """SE-yield figure of merit of the learned roulette on the same scan.
+
+    A sample-mode pass over a 4-primaries-per-pixel scan (its own seed) gives
+    (features, label) pairs; the network is trained on them (8 epochs, batch
+    8192, Adam lr 1e-3); then the whole scan runs once in learned mode with one
+    tag per primary.  FOM = 1 / (sigma^2 t): sigma^2 = per-primary variance of
+    the weighted SE count / n, t = device time of that run.  `z` compares the
+    weighted SE yield with the plain yield of the timed steps (unbiasedness)."""
+    import nebula_b200 as nb
+    from nebula_b200 import generators as g
+    n = len(tags)
+    ctx = nb.setup(tris, [mat], device=local, seed=0x2545F491 + rank, blocks_per_sm=2, block_size=256)
+    try:
+        ctx.build_surface_map([-180, -180, -60], [180, 180, 60], 1.0, 20.0)
+        train = g.scan_beam(NX, NY, 4, ENERGY, seed=0x51ED + rank)
+        ctx.set_sample_capacity(1 << 23)
+        ctx.set_mode("sample")
+        ctx.set_tag_range(len(train))
+        ctx.reset_tallies()
+        ctx.push_records(train)
+        ctx.run()
+        f, y = ctx.get_samples(1 << 23)
+        ctx.mlp_set_params(nb.mlp_init_params(0))
+        t0 = time.perf_counter()
+        losses = ctx.mlp_train(f, y, epochs=8, batch=8192, lr=1e-3, seed=1)
+        t_train = time.perf_counter() - t0
+        ctx.set_tag_range(n)
+        ctx.set_mode("learned", rr_threshold=args.rr_threshold, split_threshold=2.0, rr_period=args.rr_period)
+        ctx.reset_tallies()
+        ctx.push(prim, tags)
+        ctx.run()
+        s = ctx.stats()
+        sw, bw = ctx.tag_weights(0, n)
+        sw = sw.astype(np.float64)
+        t = s["last_run_ms"] / 1000.0
+        var_l = float(np.var(sw))
+        fom_l = 1.0 / (var_l / n * t)
+        z = (float(sw.mean()) - mean_plain) / math.sqrt(var_l / n + var_plain / n)
+        return {"fom_se": fom_l, "fom_se_plain": fom_plain, "gain": fom_l / fom_plain if fom_plain else None,
+                "se_yield": float(sw.mean()), "z_vs_plain": z, "run_ms": s["last_run_ms"],
+                "rr_threshold": args.rr_threshold, "rr_period": args.rr_period, "split": "off",
+                "launch": {"blocks_per_sm_variant": 2, "block_size": 256},
+                "inferences": s["inferences"], "roulette_killed": s["roulette_killed"],
+                "steps": s["steps"], "train_samples": int(len(y)), "train_s": round(t_train, 3),
+                "train_loss": [round(float(v), 5) for v in losses]}
+    finally:
+        ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -240,6 +290,9 @@ def main():
     ap.add_argument("--rows", type=int, default=NY, help="pixel rows of the scan (profiling runs use fewer)")
     ap.add_argument("--variant", type=int, default=0, help="transport variant 2/3/4 (0: autotune)")
     ap.add_argument("--block", type=int, default=0, help="threads per block with --variant (0: 128)")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-roulette FOM comparison")
+    ap.add_argument("--rr-threshold", type=float, default=0.02)
+    ap.add_argument("--rr-period", type=int, default=32)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -344,6 +397,9 @@ def main():
     h2d = n * 7 * 4 + n * 4
     d2h = NX * NY * 5 * 8
 
+    learned = None if args.no_learned else learned_fom(args, tris, mat, local, rank, prim, tags, mean_se, var_primary,
+                                                       fom)
+
     line = None
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -366,6 +422,7 @@ def main():
             "events_per_primary": events / (n * args.steps),
             "se_yield": mean_se, "bse_yield": float(bse.sum()) / (n * args.steps),
             "fom_se_plain": fom,
+            "learned_rr": learned,
             "generations_per_step": gens,
             "gpu_launches": int(launches),
             "e2e": {"value": e2e_val, "unit": "events/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

@@ -471,3 +471,23 @@ def setup(tri_path_or_array, mat_paths, **ctx_kwargs):
     for p in mat_paths:
         ctx.add_material(HostMaterial(p))
     return ctx
+
+
+def mlp_init_params(seed=0) -> np.ndarray:
+    """Seeded Glorot-uniform parameters for the escape-probability network in
+    the include/nbx.h layout (W1[64][16] b1[64] W2[64][64] b2[64] W3[8][64]
+    b3[8]); biases and the padding columns/rows are zero."""
+    rng = np.random.default_rng(seed)
+    f, h, pin, pout = 6, 64, 16, 8
+    p = np.zeros(h * pin + h + h * h + h + pout * h + pout, np.float64)
+    w1 = np.zeros((h, pin))
+    lim1 = np.sqrt(6.0 / (f + h))
+    w1[:, :f] = rng.uniform(-lim1, lim1, (h, f))
+    p[0:h * pin] = w1.ravel()
+    o_w2 = h * pin + h
+    lim2 = np.sqrt(6.0 / (h + h))
+    p[o_w2:o_w2 + h * h] = rng.uniform(-lim2, lim2, h * h)
+    o_w3 = o_w2 + h * h + h
+    lim3 = np.sqrt(6.0 / (h + 1))
+    p[o_w3:o_w3 + h] = rng.uniform(-lim3, lim3, h)
+    return p.astype(np.float32)

@@ -74,7 +74,10 @@ struct TransportArgs {
 
 enum : int { kModePlain = 0, kModeSample = 1, kModeLearned = 2 };
 
-constexpr int kLocalStack = 16;  // per-thread stack of parked ancestors (depth-first cascades)
+#ifndef NBX_LOCAL_STACK
+#define NBX_LOCAL_STACK 16
+#endif
+constexpr int kLocalStack = NBX_LOCAL_STACK;  // per-thread stack of parked ancestors (depth-first cascades)
 
 // variant: resident blocks per SM the kernel was compiled for (2, 3 or 4);
 // mode: kModePlain, kModeSample or kModeLearned.

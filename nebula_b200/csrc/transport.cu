@@ -91,7 +91,11 @@ __device__ __forceinline__ uint32_t mix32(uint64_t x) {
 // inference, so lanes without work idle until the whole warp is done).
 template <int MinBlocks, int Mode>
 __global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Physics P, const TransportArgs a) {
-    __shared__ float leaf_cache[13 * 256];
+    // Leaf cache: 13 words per thread in dynamic shared memory sized by the
+    // launch (13 * 4 * blockDim.x bytes), so a 128-thread block does not hold
+    // a 256-thread allocation and the rest of the SM's L1 stays with the
+    // cascade stacks.
+    extern __shared__ float leaf_cache[];
     const dev::LeafCache cache{leaf_cache + threadIdx.x, int(blockDim.x)};
     cache.f(0) = 0.0f;   // location 0: empty
     cache.f(1) = 0.0f;
@@ -114,8 +118,11 @@ __global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Ph
     int warp_iter = 0;
     bool alive = false, drained = false;
     uint32_t carry_hit = 0;
-    unsigned long long c_steps = 0, c_el = 0, c_inel = 0, c_bd = 0, c_se = 0, c_det = 0, c_dse = 0, c_dbse = 0,
-                       c_term = 0, c_drop = 0, c_ovf = 0, c_pop = 0, c_inf = 0, c_kill = 0, c_split = 0, c_smp = 0;
+    // Per-thread tallies in 32 bits (a thread would need 2^32 steps in one
+    // launch to wrap); rare ones (dropped records, queue overflow) go straight
+    // to the global counters.
+    uint32_t c_steps = 0, c_el = 0, c_inel = 0, c_bd = 0, c_se = 0, c_dse = 0, c_dbse = 0, c_term = 0, c_pop = 0,
+             c_inf = 0, c_kill = 0, c_split = 0, c_smp = 0;
     for (;;) {
         if (!alive && !drained) {
             if (sp > 0) {
@@ -231,7 +238,13 @@ __global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Ph
         if (has_se) {
             // an inelastic step never ends its electron: st == kAlive here
             ++c_se;
-            if (sp < kLocalStack) {
+            if (dev::ends_at_init(P, se)) {
+                // The secondary's first step would only terminate it (about a
+                // quarter of them start below the barrier): tally that step
+                // here instead of parking the parent for it.
+                ++c_steps;
+                ++c_term;
+            } else if (sp < kLocalStack) {
                 stack[sp] = e;
                 if constexpr (kExtra) exs[sp] = ex;
                 ++sp;
@@ -241,18 +254,19 @@ __global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Ph
                     ex.flags = 0;   // the secondary inherits the weight only
                 }
                 continue;
-            }
-            // Deep cascade: hand the secondary to the next generation.
-            cg::coalesced_group g = cg::coalesced_threads();
-            uint32_t base = 0;
-            if (g.thread_rank() == 0) base = atomicAdd(a.out_tail, g.size());
-            base = g.shfl(base, 0);
-            const uint32_t slot = base + g.thread_rank();
-            if (slot < a.out_capacity) {
-                store_electron(a.out, slot, se);
-                if constexpr (Mode == kModeLearned) a.out.c[slot].w = __float_as_uint(ex.w);
             } else {
-                ++c_ovf;
+                // Deep cascade: hand the secondary to the next generation.
+                cg::coalesced_group g = cg::coalesced_threads();
+                uint32_t base = 0;
+                if (g.thread_rank() == 0) base = atomicAdd(a.out_tail, g.size());
+                base = g.shfl(base, 0);
+                const uint32_t slot = base + g.thread_rank();
+                if (slot < a.out_capacity) {
+                    store_electron(a.out, slot, se);
+                    if constexpr (Mode == kModeLearned) a.out.c[slot].w = __float_as_uint(ex.w);
+                } else {
+                    atomicAdd(a.counters + kCntOverflow, 1ull);
+                }
             }
         }
         if (st == dev::kAlive) continue;
@@ -262,7 +276,6 @@ __global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Ph
             ++c_term;
         } else {
             // detected
-            ++c_det;
             const bool is_se = e.E < 50;
             hit = is_se ? 1u : 0u;
             c_dse += is_se;
@@ -282,7 +295,7 @@ __global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Ph
                     a.rec_a[slot] = make_float4(e.px, e.py, e.pz, e.E);
                     a.rec_b[slot] = make_float4(e.dx, e.dy, e.dz, __uint_as_float(e.tag));
                 } else {
-                    ++c_drop;
+                    atomicAdd(a.counters + kCntRecordsDropped, 1ull);
                 }
             }
         }
@@ -299,12 +312,12 @@ __global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Ph
     v[kCntInelastic] = c_inel;
     v[kCntBoundary] = c_bd;
     v[kCntSecondaries] = c_se;
-    v[kCntDetected] = c_det;
+    v[kCntDetected] = c_dse + c_dbse;
     v[kCntDetectedSE] = c_dse;
     v[kCntDetectedBSE] = c_dbse;
     v[kCntTerminated] = c_term;
-    v[kCntRecordsDropped] = c_drop;
-    v[kCntOverflow] = c_ovf;
+    v[kCntRecordsDropped] = 0;
+    v[kCntOverflow] = 0;
     v[kCntPopped] = c_pop;
     v[kCntInferences] = c_inf;
     v[kCntRouletteKilled] = c_kill;
@@ -471,13 +484,18 @@ int grid_for(uint64_t n, int block) {
 
 }  // namespace
 
+// Dynamic shared memory of transport_kernel: the per-thread leaf cache.
+static size_t leaf_cache_bytes(int block) { return size_t(13) * sizeof(float) * size_t(block); }
+
 template <int Mode>
 static cudaError_t launch_mode(const dev::Physics& P, const TransportArgs& a, int grid, int block, int variant,
                                cudaStream_t s) {
+    if (block <= 0 || block > 256) return cudaErrorInvalidValue;
+    const size_t sm = leaf_cache_bytes(block);
     switch (variant) {
-    case 2: transport_kernel<2, Mode><<<grid, block, 0, s>>>(P, a); break;
-    case 4: transport_kernel<4, Mode><<<grid, block, 0, s>>>(P, a); break;
-    default: transport_kernel<3, Mode><<<grid, block, 0, s>>>(P, a); break;
+    case 2: transport_kernel<2, Mode><<<grid, block, sm, s>>>(P, a); break;
+    case 4: transport_kernel<4, Mode><<<grid, block, sm, s>>>(P, a); break;
+    default: transport_kernel<3, Mode><<<grid, block, sm, s>>>(P, a); break;
     }
     return cudaGetLastError();
 }
@@ -493,10 +511,11 @@ template <int Mode>
 static int max_blocks_mode(int block, int variant) {
     int n = 0;
     cudaError_t e;
+    const size_t sm = leaf_cache_bytes(block);
     switch (variant) {
-    case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<2, Mode>, block, 0); break;
-    case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<4, Mode>, block, 0); break;
-    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<3, Mode>, block, 0); break;
+    case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<2, Mode>, block, sm); break;
+    case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<4, Mode>, block, sm); break;
+    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<3, Mode>, block, sm); break;
     }
     if (e != cudaSuccess) return 1;
     return n > 0 ? n : 1;

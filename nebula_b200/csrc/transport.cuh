@@ -475,6 +475,19 @@ __device__ __forceinline__ int boundary(const Physics& P, Electron& e, float u) 
     return kAlive;
 }
 
+// The init pass's termination test (drivers/cpu/cpu_driver.inl:73-92): outside
+// the simulation domain, or inside a material with an energy outside
+// [barrier + min_energy, barrier + max_energy].  A step that ends here draws no
+// random numbers and changes nothing, so callers may apply it early.
+__device__ __forceinline__ bool ends_at_init(const Physics& P, const Electron& e) {
+    if (!in_domain(P.geo, V3{e.px, e.py, e.pz})) return true;
+    if (e.mat >= 0) {
+        const Material& m = P.mat[e.mat];
+        if (e.E < m.barrier + P.min_energy || e.E > m.barrier + P.max_energy) return true;
+    }
+    return false;
+}
+
 // One pass of init -> intersect -> scatter (drivers/cpu/cpu_driver.inl:73-161,
 // cpu_particle_manager.inl:214-235).  Uniforms of step k come from Philox
 // blocks (k, 0) and (k, 1) of the electron's stream: block 0 x/y feed the
@@ -486,14 +499,13 @@ __device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, E
                                     LeafCache cache = LeafCache{nullptr, 0}) {
     *event = kEvNone;
     *has_se = false;
-    if (!in_domain(P.geo, V3{e.px, e.py, e.pz})) return kTerminated;
+    if (ends_at_init(P, e)) return kTerminated;
     const uint4 r0 = draw(P.seed, e, 0);
     int type = 0;
     float dist = P.geo.max_extent;
     float logE = 0;
     if (e.mat >= 0) {
         const Material& m = P.mat[e.mat];
-        if (e.E < m.barrier + P.min_energy || e.E > m.barrier + P.max_energy) return kTerminated;
         logE = logf(e.E);
         dist = __int_as_float(0x7f800000);
         {
@@ -528,13 +540,13 @@ __device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, E
             e.last_tri = -1;
             const Material& m = P.mat[e.mat];
             const bool inel = (type == 1);
-            const uint4 r1 = draw(P.seed, e, 1);
             const float tv = table2d_get(inel ? m.in_icdf : m.el_icdf, logE, u01(r0.z));
             const V3 n = normalised(make_normal_vec(nd, (2 * kPi) * u01(r0.w)));
             if (!inel) {
                 elastic_finish(m, e, tv, nd, n);
                 *event = kEvElastic;
             } else {
+                const uint4 r1 = draw(P.seed, e, 1);
                 *has_se = inelastic_finish(m, e, tv, nd, n, u01(r1.x), u01(r1.y), u01(r1.z), u01(r1.w), se);
                 *event = kEvInelastic;
             }

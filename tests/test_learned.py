@@ -197,7 +197,10 @@ def test_learned_roulette_unbiased(inputs):
     c.mlp_train(f, y, epochs=4, batch=8192, lr=1e-3, seed=2)
     recs = g.scan_beam(16, 16, 40, 500.0, origin=(-8.0, -8.0), seed=12)
     sp, se_p, bse_p, _, _ = _run(c, recs, "plain")
-    sl, se_l, bse_l, sw, bw = _run(c, recs, "learned", rr_threshold=0.05, split_threshold=0.5, rr_period=8)
+    # A threshold well above the positive rate, so that the roulette acts even
+    # where the briefly trained network is close to constant.
+    th = max(0.1, 3.0 * float(y.mean()))
+    sl, se_l, bse_l, sw, bw = _run(c, recs, "learned", rr_threshold=th, split_threshold=0.5, rr_period=8)
     assert sl["roulette_killed"] > 0
     for plain, learned in ((se_p.astype(float), sw.astype(float)), (bse_p.astype(float), bw.astype(float))):
         z = (learned.mean() - plain.mean()) / np.sqrt(learned.var() / len(learned) + plain.var() / len(plain))
