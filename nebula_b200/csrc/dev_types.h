@@ -36,7 +36,8 @@ struct Material {
 // Triangles as three float4: (r0, mat_in bits), (e1, mat_out bits), (e2, 0).
 struct Geometry {
     const int32_t* octree;
-    const float4* tri;
+    const float4* tri;        // per triangle: (r0, mat_in), (e1, mat_out), (e2, 0)
+    const float4* tri_face;   // per triangle: (e1 x e2, (mat_out << 16) | (mat_in & 0xFFFF))
     float cx, cy, cz, hx, hy, hz;
     float max_extent;
     int n_tri;

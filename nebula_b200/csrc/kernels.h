@@ -84,6 +84,9 @@ constexpr int kLocalStack = NBX_LOCAL_STACK;  // per-thread stack of parked ance
 cudaError_t launch_transport(const dev::Physics& P, const TransportArgs& a, int grid, int block, int variant,
                              cudaStream_t s, int mode = kModePlain);
 int transport_max_blocks_per_sm(int block, int variant, int mode = kModePlain);
+// Per-triangle face records (normal e1 x e2 and packed materials) for
+// Geometry::tri_face; materials must fit in 16 bits.
+cudaError_t launch_triangle_faces(const float4* tri, float4* face, int n, cudaStream_t s);
 // Nearest-triangle map over [lo, lo + n * cell): candidates are triangle
 // indices; cells farther than d_max from all candidates get -1.
 cudaError_t launch_build_surface_map(const float4* tri, const int32_t* candidates, int n_candidates, int32_t* map,

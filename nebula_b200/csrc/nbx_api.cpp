@@ -95,6 +95,7 @@ struct nbx_ctx {
     // geometry
     DevBuf<int32_t> octree;
     DevBuf<float4> tris;
+    DevBuf<float4> tri_faces;
     bool have_geometry = false;
     // materials
     std::vector<DevBuf<float>*> tables;
@@ -471,6 +472,8 @@ int nbx_set_geometry(nbx_ctx* ctx, const nbx_octree* o) {
         std::vector<float4> t(3 * std::max<uint64_t>(o->n_triangles, 1));
         for (uint64_t i = 0; i < o->n_triangles; ++i) {
             const nbx_triangle& s = o->triangles[i];
+            if (s.mat_in < -32768 || s.mat_in > 32767 || s.mat_out < -32768 || s.mat_out > 32767)
+                throw ApiError(NBX_ERR_ARG, "triangle material index outside the 16-bit range");
             float a, b;
             std::memcpy(&a, &s.mat_in, 4);
             std::memcpy(&b, &s.mat_out, 4);
@@ -480,9 +483,13 @@ int nbx_set_geometry(nbx_ctx* ctx, const nbx_octree* o) {
         }
         ctx->tris.alloc(t.size());
         ck(cudaMemcpy(ctx->tris.p, t.data(), sizeof(float4) * t.size(), cudaMemcpyHostToDevice), "triangles");
+        ctx->tri_faces.alloc(std::max<uint64_t>(o->n_triangles, 1));
+        ck(nbx::launch_triangle_faces(ctx->tris.p, ctx->tri_faces.p, int(o->n_triangles), ctx->stream), "faces");
+        ck(cudaStreamSynchronize(ctx->stream), "faces");
         auto& g = ctx->phys.geo;
         g.octree = ctx->octree.p;
         g.tri = ctx->tris.p;
+        g.tri_face = ctx->tri_faces.p;
         g.cx = o->center[0];
         g.cy = o->center[1];
         g.cz = o->center[2];

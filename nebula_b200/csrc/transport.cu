@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Ph
         int ev;
         bool has_se;
         dev::Electron se;
-        const int st = dev::step(P, e, &ev, &se, &has_se, cache);
+        int st = dev::step(P, e, &ev, &se, &has_se, cache);
         ++c_steps;
         c_el += (ev == dev::kEvElastic);
         c_inel += (ev == dev::kEvInelastic);
@@ -269,7 +269,13 @@ __global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Ph
                 }
             }
         }
-        if (st == dev::kAlive) continue;
+        if (st == dev::kAlive) {
+            if (!dev::ends_at_init(P, e)) continue;
+            // The next init pass would only end the electron (energy below
+            // the barrier, or it left the domain): tally that step now.
+            ++c_steps;
+            st = dev::kTerminated;
+        }
         alive = false;
         uint32_t hit = 0;
         if (st == dev::kTerminated) {
@@ -461,6 +467,18 @@ __global__ void pixel_yields_kernel(const uint32_t* se, const uint32_t* bse, con
     }
 }
 
+// Face records: e1 x e2 computed with the transport's arithmetic (the same
+// expression propagate and boundary would evaluate) and both materials packed
+// as 16-bit halves.
+__global__ void triangle_faces_kernel(const float4* tri, float4* face, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 b = tri[3 * i + 1], c = tri[3 * i + 2];
+        const dev::V3 nrm = dev::cross(dev::V3{b.x, b.y, b.z}, dev::V3{c.x, c.y, c.z});
+        const uint32_t mi = uint32_t(__float_as_int(tri[3 * i].w)), mo = uint32_t(__float_as_int(b.w));
+        face[i] = make_float4(nrm.x, nrm.y, nrm.z, __uint_as_float((mo << 16) | (mi & 0xFFFFu)));
+    }
+}
+
 __global__ void fill_queue_kernel(Queue q, const float* particles, const uint32_t* tags, uint64_t uid_base, uint64_t n,
                                   uint64_t offset) {
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
@@ -559,6 +577,12 @@ __global__ void features_kernel(const dev::Geometry g, const dev::SurfaceMap S, 
     }
 }
 }  // namespace
+
+cudaError_t launch_triangle_faces(const float4* tri, float4* face, int n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    triangle_faces_kernel<<<grid_for(uint64_t(n), 256), 256, 0, s>>>(tri, face, n);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_build_surface_map(const float4* tri, const int32_t* candidates, int n_candidates, int32_t* map,
                                      float lox, float loy, float loz, float cell, int nx, int ny, int nz, float d_max,

@@ -4,7 +4,7 @@
 // operation by operation; the translation unit is compiled with
 // -fmad=false and IEEE division/square root, so octree ray queries and table
 // lookups are bit-identical to the reference CPU path.  Transcendentals are
-// CUDA's accurate (non-intrinsic) logf/expf/expm1f/sinf/cosf/atan2f.
+// CUDA's accurate (non-intrinsic) logf/expf/expm1f/sincospif.
 #pragma once
 
 #include <cstdint>
@@ -107,21 +107,29 @@ __device__ __forceinline__ V3 normalised(V3 a) {
     const float inv = 1.0f / sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
     return {a.x * inv, a.y * inv, a.z * inv};
 }
-// vector_math.h:171-186
-__device__ __forceinline__ V3 make_normal_vec(V3 dir, float phi) {
-    const float az = atan2f(dir.y, dir.x);
-    float sin_az, cos_az;
-    sincosf(az, &sin_az, &cos_az);
-    const V3 v{dir.z * cos_az, dir.z * sin_az, -sqrtf(dir.x * dir.x + dir.y * dir.y)};
+// make_normal_vec (vector_math.h:171-186) with the rotation angle given as a
+// uniform u (phi = 2 pi u).  The reference takes cos and sin of
+// atan2(dir.y, dir.x); here they are dir.x / r and dir.y / r with
+// r = |(dir.x, dir.y)| (azimuth 0 when r = 0), the same values without the
+// two transcendental calls, and sin/cos(2 pi u) come from sincospif(2 u).
+// Scattering angles are compared statistically, not bit for bit.
+__device__ __forceinline__ V3 make_normal_vec(V3 dir, float u_phi) {
+    const float r = sqrtf(dir.x * dir.x + dir.y * dir.y);
+    float sin_az = 0.0f, cos_az = 1.0f;
+    if (r > 0.0f) {
+        cos_az = dir.x / r;
+        sin_az = dir.y / r;
+    }
+    const V3 v{dir.z * cos_az, dir.z * sin_az, -r};
     const V3 u = cross(v, dir);
     float sp, cp;
-    sincosf(phi, &sp, &cp);
+    sincospif(2.0f * u_phi, &sp, &cp);
     return {u.x * cp + v.x * sp, u.y * cp + v.y * sp, u.z * cp + v.z * sp};
 }
-// vector_math.h:194-206
-__device__ __forceinline__ V3 make_unit_vec(float cos_theta, float phi) {
+// make_unit_vec (vector_math.h:194-206), phi = 2 pi u_phi as above.
+__device__ __forceinline__ V3 make_unit_vec(float cos_theta, float u_phi) {
     float sp, cp;
-    sincosf(phi, &sp, &cp);
+    sincospif(2.0f * u_phi, &sp, &cp);
     cos_theta = clampr(cos_theta, -1, 1);
     const float st = sqrtf(1 - cos_theta * cos_theta);
     return {st * cp, st * sp, cos_theta};
@@ -130,15 +138,23 @@ __device__ __forceinline__ V3 make_unit_vec(float cos_theta, float phi) {
 // ---------------------------------------------------------------------------
 // Geometry
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void load_tri(const Geometry& g, int ti, V3& r0, V3& e1, V3& e2, int& mi, int& mo) {
+__device__ __forceinline__ void load_tri_vertices(const Geometry& g, int ti, V3& r0, V3& e1, V3& e2) {
     const float4 a = __ldg(g.tri + 3 * ti);
     const float4 b = __ldg(g.tri + 3 * ti + 1);
     const float4 c = __ldg(g.tri + 3 * ti + 2);
     r0 = {a.x, a.y, a.z};
     e1 = {b.x, b.y, b.z};
     e2 = {c.x, c.y, c.z};
-    mi = __float_as_int(a.w);
-    mo = __float_as_int(b.w);
+}
+
+// Unnormalised normal e1 x e2 (triangle::get_normal, core/triangle.inl:71-74)
+// and the two materials, from the triangle's 16-byte face record.
+__device__ __forceinline__ V3 load_face(const Geometry& g, int ti, int& mi, int& mo) {
+    const float4 f = __ldg(g.tri_face + ti);
+    const int w = __float_as_int(f.w);
+    mi = int(int16_t(w & 0xFFFF));
+    mo = w >> 16;
+    return V3{f.x, f.y, f.z};
 }
 
 // triangle::intersect_ray (core/triangle.inl:7-29)
@@ -278,11 +294,15 @@ __device__ __forceinline__ float propagate(const Geometry& g, V3 start, V3 dir, 
             ++index;
             if (ti < 0) break;
             if (ti == ignore_tri) continue;
-            V3 r0, e1, e2;
+            // The face record alone decides the exit material (the normal is
+            // e1 x e2 as computed on the device, so the sign is the
+            // reference's); only candidates that survive load the vertices.
             int mi, mo;
-            load_tri(g, ti, r0, e1, e2, mi, mo);
-            const int mat_out = (dot(cross(e1, e2), dir) < 0) ? mi : mo;
+            const V3 nrm = load_face(g, ti, mi, mo);
+            const int mat_out = (dot(nrm, dir) < 0) ? mi : mo;
             if (mat_out == ignore_mat) continue;
+            V3 r0, e1, e2;
+            load_tri_vertices(g, ti, r0, e1, e2);
             const float t = intersect_ray(r0, e1, e2, cur, dir);
             if ((t > 0) && (t <= intersect + kEps)) {
                 intersect = t;
@@ -352,7 +372,9 @@ __device__ __forceinline__ bool inelastic_finish(const Material& m, Electron& e,
                                                  float u_bind, float u_omega, float u_v1, float u_v2, Electron* se) {
     const float K = e.E;
     const float omega0 = expf(log_omega0);
-    float binding = table2d_rounddown(m.ion, logf(omega0), u_bind);
+    // log(omega0) is the ICDF value itself (the reference takes the log of
+    // its exponential); the rounddown lookup sees the same coordinate.
+    float binding = table2d_rounddown(m.ion, log_omega0, u_bind);
     float omega;
     {
         const float omega_max = 0.5f * (K + omega0 - m.fermi);
@@ -390,7 +412,7 @@ __device__ __forceinline__ bool inelastic_finish(const Material& m, Electron& e,
     V3 s{d.x * cos_theta + n.x * sin_theta, d.y * cos_theta + n.y * sin_theta, d.z * cos_theta + n.z * sin_theta};
     s = normalised(s);
     {
-        const V3 uv = make_unit_vec(2 * u_v1 - 1, (2 * kPi) * u_v2);
+        const V3 uv = make_unit_vec(2 * u_v1 - 1, u_v2);
         const float a = sqrtf(binding / dK);
         s.x += a * uv.x;
         s.y += a * uv.y;
@@ -421,11 +443,10 @@ __device__ __forceinline__ bool inelastic_finish(const Material& m, Electron& e,
 // boundary_intersect<quantum transmission, refraction, no absorption>::execute
 // (physics/boundary_intersect.h:40-156)
 __device__ __forceinline__ int boundary(const Physics& P, Electron& e, float u) {
-    V3 r0, e1, e2;
     int mi, mo;
-    load_tri(P.geo, e.last_tri, r0, e1, e2, mi, mo);
+    const V3 face = load_face(P.geo, e.last_tri, mi, mo);
     const V3 nd = normalised(V3{e.dx, e.dy, e.dz});
-    const V3 n = normalised(cross(e1, e2));
+    const V3 n = normalised(face);
     const float cos_theta = dot(n, nd);
     int in, out;
     if (cos_theta > 0) {
@@ -508,17 +529,20 @@ __device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, E
         const Material& m = P.mat[e.mat];
         logE = logf(e.E);
         dist = __int_as_float(0x7f800000);
+        // Mean free path exp(-log imfp) rather than 1 / exp(log imfp): the
+        // same exponential sampling (scatter_list.h:106-132, random.h
+        // exponential) without a division per mechanism.
         {
-            const float imfp = expf(table1d_get(m.in_imfp, logE));
-            const float path = -(1 / imfp) * logf(u01(r0.x));
+            const float mfp = expf(-table1d_get(m.in_imfp, logE));
+            const float path = -mfp * logf(u01(r0.x));
             if (path < dist) {
                 type = 1;
                 dist = path;
             }
         }
         {
-            const float imfp = expf(table1d_get(m.el_imfp, logE));
-            const float path = -(1 / imfp) * logf(u01(r0.y));
+            const float mfp = expf(-table1d_get(m.el_imfp, logE));
+            const float path = -mfp * logf(u01(r0.y));
             if (path < dist) {
                 type = 2;
                 dist = path;
@@ -541,7 +565,7 @@ __device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, E
             const Material& m = P.mat[e.mat];
             const bool inel = (type == 1);
             const float tv = table2d_get(inel ? m.in_icdf : m.el_icdf, logE, u01(r0.z));
-            const V3 n = normalised(make_normal_vec(nd, (2 * kPi) * u01(r0.w)));
+            const V3 n = normalised(make_normal_vec(nd, u01(r0.w)));
             if (!inel) {
                 elastic_finish(m, e, tv, nd, n);
                 *event = kEvElastic;
