@@ -288,7 +288,7 @@ def main():
     ap.add_argument("--impl", default="nbx", choices=["nbx", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=NY, help="pixel rows of the scan (profiling runs use fewer)")
-    ap.add_argument("--variant", type=int, default=0, help="transport variant 2/3/4 (0: autotune)")
+    ap.add_argument("--variant", type=int, default=0, help="transport variant 2/3/4/7 (0: autotune)")
     ap.add_argument("--block", type=int, default=0, help="threads per block with --variant (0: 128)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-roulette FOM comparison")
     ap.add_argument("--rr-threshold", type=float, default=0.02)

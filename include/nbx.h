@@ -152,7 +152,8 @@ typedef struct {
     int32_t record_detected;   /* keep per-electron detected records */
     uint64_t record_capacity;  /* detected records held on the device; 0 = auto */
     int32_t block_size;        /* threads per block of the transport kernel; 0 = 256 */
-    int32_t blocks_per_sm;     /* transport variant: 2, 3 or 4 resident blocks per SM; 0 = 3 */
+    int32_t blocks_per_sm;     /* transport variant: 2, 3 or 4 resident 256-thread blocks per SM, or 7
+                                  128-thread blocks (block_size capped at 128); 0 = 3 */
 } nbx_config;
 
 typedef struct {
@@ -222,9 +223,10 @@ int nbx_reset_tallies(nbx_ctx* ctx);
 
 /* Autotuner (no counterpart in the reference, whose launch shape is fixed at
  * 32-thread blocks over the whole capacity, drivers/gpu/gpu_driver.inl:64):
- * runs the given sample once per transport variant (2, 3, 4 resident blocks
- * per SM) and block size (256, 128), keeps the fastest, and resets the
- * tallies.  Random streams of later pushes are unaffected. */
+ * runs the given sample once per transport variant (2, 3, 4 resident
+ * 256-thread blocks per SM, 7 resident 128-thread blocks) and block size
+ * (256, 128), keeps the fastest, and resets the tallies.  Random streams of
+ * later pushes are unaffected. */
 int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n,
                  int32_t* blocks_per_sm, int32_t* block_size);
 

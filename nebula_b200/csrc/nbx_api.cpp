@@ -432,9 +432,11 @@ int nbx_create(nbx_ctx** out, const nbx_config* cfg) {
         ck(cudaMemset(ctx->rec_count.p, 0, 4), "memset");
         ctx->block = c.block_size > 0 ? c.block_size : 256;
         if (ctx->block % 32 != 0 || ctx->block > 256) throw ApiError(NBX_ERR_ARG, "block_size must be a multiple of 32, <= 256");
-        // Kernel variant = resident 256-thread blocks per SM it was register-
-        // limited for (2, 3 or 4); default 3 (80 registers).
-        ctx->variant = (c.blocks_per_sm >= 2 && c.blocks_per_sm <= 4) ? c.blocks_per_sm : 3;
+        // Kernel variant = resident blocks per SM it was register-limited for:
+        // 2, 3 or 4 blocks of 256 threads, or 7 blocks of 128 (72 registers;
+        // block size capped at 128); default 3 (80 registers).
+        ctx->variant = ((c.blocks_per_sm >= 2 && c.blocks_per_sm <= 4) || c.blocks_per_sm == 7) ? c.blocks_per_sm : 3;
+        if (ctx->variant == 7 && ctx->block > 128) ctx->block = 128;
         ctx->bpsm = nbx::transport_max_blocks_per_sm(ctx->block, ctx->variant);
         if (c.record_detected) {
             ctx->rec_cap = c.record_capacity ? c.record_capacity : (1ull << 24);
@@ -903,13 +905,14 @@ int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* ta
     if (!ctx || !particles || !tags || n == 0) return NBX_ERR_ARG;
     if (!ctx->have_geometry) return fail(ctx, NBX_ERR_STATE, "nbx_autotune before nbx_set_geometry");
     if (ctx->n_queued) return fail(ctx, NBX_ERR_STATE, "nbx_autotune with primaries queued");
-    const int variants[3] = {2, 3, 4};
+    const int variants[4] = {2, 3, 4, 7};
     const int blocks[2] = {256, 128};
     double best = 1e300;
     int best_v = ctx->variant, best_b = ctx->block;
     const uint64_t uid_save = ctx->uid_next;
     for (int v : variants) {
         for (int b : blocks) {
+            if (v == 7 && b > 128) continue;   // 128-thread variant
             ctx->variant = v;
             ctx->block = b;
             ctx->bpsm = nbx::transport_max_blocks_per_sm(b, v);

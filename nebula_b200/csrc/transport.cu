@@ -15,8 +15,11 @@
 // records are optional.
 #include <cooperative_groups.h>
 
+#include <algorithm>
 #include <mutex>
 #include <type_traits>
+#include <utility>
+#include <vector>
 
 #include "features.cuh"
 #include "kernels.h"
@@ -82,15 +85,16 @@ __device__ __forceinline__ uint32_t mix32(uint64_t x) {
     return uint32_t(x);
 }
 
-// MinBlocks: resident 256-thread blocks per SM the register allocation must
-// allow (2: 128 registers, 3: 80, 4: 64); the host picks the variant.
+// MinBlocks: resident blocks per SM the register allocation must allow --
+// 256-thread blocks for 2 (128 registers), 3 (80) and 4 (64); 128-thread
+// blocks for 7 (72 registers, 28 warps); the host picks the variant.
 // Mode: kModePlain (analogue transport), kModeSample (plain transport that
 // also records one (features, label) training sample per sampled electron)
 // or kModeLearned (weighted roulette / splitting with the network as the
 // importance function; the warp stays converged for the tensor-core
 // inference, so lanes without work idle until the whole warp is done).
 template <int MinBlocks, int Mode>
-__global__ void __launch_bounds__(256, MinBlocks) transport_kernel(const dev::Physics P, const TransportArgs a) {
+__global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transport_kernel(const dev::Physics P, const TransportArgs a) {
     // Leaf cache: 13 words per thread in dynamic shared memory sized by the
     // launch (13 * 4 * blockDim.x bytes), so a 128-thread block does not hold
     // a 256-thread allocation and the rest of the SM's L1 stays with the
@@ -505,14 +509,63 @@ int grid_for(uint64_t n, int block) {
 // Dynamic shared memory of transport_kernel: the per-thread leaf cache.
 static size_t leaf_cache_bytes(int block) { return size_t(13) * sizeof(float) * size_t(block); }
 
+// Shared-memory carveout that just fits the blocks the registers allow on an
+// SM, so the rest of the unified L1 caches what the transport gathers
+// (octree words, triangles, tables) and the register spills.  Left to itself
+// the driver may pick a larger carveout.  Applied once per (kernel, block
+// size, device); the occupancy is checked afterwards and the default restored
+// if the hint would cost resident blocks.
+template <typename Kernel>
+static void fit_carveout(Kernel kernel, int block) {
+    static std::mutex mu;
+    static std::vector<std::pair<const void*, int>> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const void* key = reinterpret_cast<const void*>(kernel);
+    const int tag = block * 64 + dev;
+    std::lock_guard<std::mutex> lock(mu);
+    for (const auto& d : done)
+        if (d.first == key && d.second == tag) return;
+    done.emplace_back(key, tag);
+    const size_t dyn = leaf_cache_bytes(block);
+    int before = 0, after = 0, smem_sm = 0;
+    cudaFuncAttributes fa{};
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&before, kernel, block, dyn) != cudaSuccess ||
+        cudaFuncGetAttributes(&fa, kernel) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        before <= 0 || smem_sm <= 0) {
+        cudaGetLastError();
+        return;
+    }
+    // per resident block: dynamic + static shared memory + 1 KB the runtime reserves
+    const size_t need = size_t(before) * (dyn + fa.sharedSizeBytes + 1024);
+    const int pct = int(std::min<size_t>(100, (need * 100 + size_t(smem_sm) - 1) / size_t(smem_sm)));
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&after, kernel, block, dyn) != cudaSuccess || after < before) {
+        cudaGetLastError();
+        cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, -1);
+        cudaGetLastError();
+    }
+}
+
 template <int Mode>
 static cudaError_t launch_mode(const dev::Physics& P, const TransportArgs& a, int grid, int block, int variant,
                                cudaStream_t s) {
-    if (block <= 0 || block > 256) return cudaErrorInvalidValue;
+    if (block <= 0 || block > (variant == 7 ? 128 : 256)) return cudaErrorInvalidValue;
     const size_t sm = leaf_cache_bytes(block);
+    switch (variant) {
+    case 2: fit_carveout(transport_kernel<2, Mode>, block); break;
+    case 4: fit_carveout(transport_kernel<4, Mode>, block); break;
+    case 7: fit_carveout(transport_kernel<7, Mode>, block); break;
+    default: fit_carveout(transport_kernel<3, Mode>, block); break;
+    }
     switch (variant) {
     case 2: transport_kernel<2, Mode><<<grid, block, sm, s>>>(P, a); break;
     case 4: transport_kernel<4, Mode><<<grid, block, sm, s>>>(P, a); break;
+    case 7: transport_kernel<7, Mode><<<grid, block, sm, s>>>(P, a); break;
     default: transport_kernel<3, Mode><<<grid, block, sm, s>>>(P, a); break;
     }
     return cudaGetLastError();
@@ -533,6 +586,7 @@ static int max_blocks_mode(int block, int variant) {
     switch (variant) {
     case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<2, Mode>, block, sm); break;
     case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<4, Mode>, block, sm); break;
+    case 7: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<7, Mode>, block, sm); break;
     default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<3, Mode>, block, sm); break;
     }
     if (e != cudaSuccess) return 1;
