@@ -43,6 +43,12 @@ ENERGY = 500.0
 WORKLOAD = "grating 256x256 px x 100 primaries @ 500 eV (6,553,600 primaries), 5,136 triangles, Si-like Kieft tables"
 
 
+def workload_name(args):
+    if args.inelastic == "penn":
+        return WORKLOAD.replace("Kieft tables", "full Penn inelastic + Kieft elastic tables")
+    return WORKLOAD
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -151,12 +157,15 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def algorithmic_bytes_per_event(tris, mat_path, recs, seed):
+def algorithmic_bytes_per_event(tris, mat_path, recs, seed, penn=False):
     """Section-8(d) algorithmic bytes per event, counted by the instrumented
-    CPU restatement on a fixed sample of the workload."""
+    CPU restatement on a fixed sample of the workload.  An inelastic event
+    reads a 2-D ICDF (16 B) and a rounddown value (4 B) under Kieft, and the
+    2-D ICDF, a trilinear 3-D q lookup (32 B) and a 3-D rounddown (4 B) under
+    full Penn."""
     import oracle
     pg = oracle.PortGeometry(tris)
-    rm = oracle.RefMaterial(mat_path)
+    rm = oracle.RefMaterial(mat_path, penn=penn)
     pms, arr = oracle.port_materials([rm])
     sample = recs[:: max(1, len(recs) // 2000)][:2000]
     prim = np.zeros((len(sample), 7), np.float32)
@@ -164,10 +173,11 @@ def algorithmic_bytes_per_event(tris, mat_path, recs, seed):
     prim[:, 3:6] = sample["dir"]
     prim[:, 6] = sample["E"]
     c, _, _, _, gc = oracle.port_run(pg, arr, prim, np.arange(len(sample), dtype=np.uint32), seed,
-                                     max_energy=rm.max_energy)
+                                     max_energy=rm.max_energy, penn=penn)
     ev = c["n_elastic"] + c["n_inelastic"] + c["n_boundary"]
     b_state = 88.0
-    b_tables = 16.0 + (16.0 * c["n_elastic"] + 20.0 * c["n_inelastic"] + 52.0 * c["n_boundary"]) / ev
+    b_inel = 52.0 if penn else 20.0
+    b_tables = 16.0 + (16.0 * c["n_elastic"] + b_inel * c["n_inelastic"] + 52.0 * c["n_boundary"]) / ev
     b_geom = (4.0 * float(gc[0]) + 44.0 * float(gc[1])) / ev
     return b_state + b_tables + b_geom, {"state": b_state, "tables": round(b_tables, 2), "geom": round(b_geom, 2),
                                          "octree_words_per_event": round(float(gc[0]) / ev, 2),
@@ -175,18 +185,19 @@ def algorithmic_bytes_per_event(tris, mat_path, recs, seed):
                                          "sample_primaries": len(sample), "sample_events": ev}
 
 
-def cpu_baseline(tri_path, mat_path, recs, tmp, rows=16):
-    """The reference's own CPU path (oracle/_ref, cpu_mt_main-style driver) on
-    the first `rows` pixel rows of the scan, all host cores."""
+def cpu_baseline(tri_path, mat_path, recs, tmp, rows=16, penn=False):
+    """The reference's own CPU path (oracle/_ref, cpu_mt_main-style driver;
+    the stock full Penn build with `penn`) on the first `rows` pixel rows of
+    the scan, all host cores."""
     import oracle
     from nebula_b200 import formats
-    if not oracle.have_ref():
+    if not oracle.have_ref(penn):
         return None
     sub = recs[recs["py"] < rows]
     pri = os.path.join(tmp, "cpu_sample.pri")
     formats.write_pri(pri, sub)
     cores = os.cpu_count() or 1
-    _, st, secs = oracle.ref_run(tri_path, pri, [mat_path], threads=cores, count_events=True)
+    _, st, secs = oracle.ref_run(tri_path, pri, [mat_path], threads=cores, count_events=True, penn=penn)
     ev = st["n_intersect"] + st["n_elastic"] + st["n_inelastic"]
     return {"value": ev / secs, "unit": "events/s", "cores": cores, "kind": "reference",
             "sample": "%d pixel rows x 256 px x 100 primaries = %d primaries (%d events) in %.2f s"
@@ -199,9 +210,10 @@ def run_reference(args):
     if rank != 0:
         return 0
     import oracle
+    penn = args.inelastic == "penn"
     with tempfile.TemporaryDirectory() as tmp:
-        if not oracle.have_ref():
-            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libnbref.so not built"}))
+        if not oracle.have_ref(penn):
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref reference library not built"}))
             return 0
         from nebula_b200 import formats
         mat, tris, tri_path, recs = make_workload(tmp)
@@ -212,7 +224,8 @@ def run_reference(args):
         cores = os.cpu_count() or 1
         total_ev, total_s, total_p = 0, 0.0, 0
         for i in range(args.warmup + args.steps):
-            _, st, secs = oracle.ref_run(tri_path, pri, [mat], seed=0x78C7E39B + i, threads=cores, count_events=True)
+            _, st, secs = oracle.ref_run(tri_path, pri, [mat], seed=0x78C7E39B + i, threads=cores, count_events=True,
+                                         penn=penn)
             if i >= args.warmup:
                 total_ev += st["n_intersect"] + st["n_elastic"] + st["n_inelastic"]
                 total_s += secs
@@ -222,7 +235,8 @@ def run_reference(args):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total_s / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic", "primaries_per_s": total_p / total_s,
-                "config": {"workload": WORKLOAD, "step_sample": "%d pixel rows (%d primaries) per step" % (rows, len(sub))},
+                "config": {"workload": workload_name(args), "inelastic": args.inelastic,
+                           "step_sample": "%d pixel rows (%d primaries) per step" % (rows, len(sub))},
                 "cpu_baseline": {"value": v, "unit": "events/s", "cores": cores, "kind": "reference",
                                  "sample": "%d primaries per step, %d steps" % (len(sub), args.steps)},
                 "e2e": {"value": v, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -242,7 +256,8 @@ def learned_fom(args, tris, mat, local, rank, prim, tags, mean_plain, var_plain,
     import nebula_b200 as nb
     from nebula_b200 import generators as g
     n = len(tags)
-    ctx = nb.setup(tris, [mat], device=local, seed=0x2545F491 + rank, blocks_per_sm=2, block_size=256)
+    ctx = nb.setup(tris, [mat], device=local, seed=0x2545F491 + rank, blocks_per_sm=2, block_size=256,
+                   inelastic=args.inelastic)
     try:
         ctx.build_surface_map([-180, -180, -60], [180, 180, 60], 1.0, 20.0)
         train = g.scan_beam(NX, NY, 4, ENERGY, seed=0x51ED + rank)
@@ -293,6 +308,8 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-roulette FOM comparison")
     ap.add_argument("--rr-threshold", type=float, default=0.02)
     ap.add_argument("--rr-period", type=int, default=32)
+    ap.add_argument("--inelastic", default="kieft", choices=["kieft", "penn"],
+                    help="inelastic model: Kieft & Bosch (the headline workload) or full Penn (the reference's stock build)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -303,7 +320,7 @@ def main():
 
     tmp = tempfile.mkdtemp(prefix="nbx_bench_")
     mat, tris, tri_path, recs = make_workload(tmp, rank, rows=None if args.rows >= NY else range(args.rows))
-    ctx = nb.setup(tris, [mat], device=local, seed=0x78C7E39B + rank)
+    ctx = nb.setup(tris, [mat], device=local, seed=0x78C7E39B + rank, inelastic=args.inelastic)
     n = len(recs)
     prim = np.zeros((n, 7), np.float32)
     prim[:, 0:3] = recs["pos"]
@@ -327,7 +344,7 @@ def main():
     if args.variant:
         ctx.close()
         ctx = nb.setup(tris, [mat], device=local, seed=0x78C7E39B + rank, blocks_per_sm=args.variant,
-                       block_size=args.block or 128)
+                       block_size=args.block or 128, inelastic=args.inelastic)
         ctx.set_tag_range(n)
         tuned = (args.variant, args.block or 128)
     else:
@@ -403,19 +420,20 @@ def main():
     line = None
     if rank == 0:
         peak, peak_kind = measured_peaks()
-        b_event, b_parts = algorithmic_bytes_per_event(tris, mat, recs, 0x78C7E39B)
+        b_event, b_parts = algorithmic_bytes_per_event(tris, mat, recs, 0x78C7E39B, penn=args.inelastic == "penn")
         achieved = events * b_event / (sum(dev_ms) / 1000.0) / 1e9
         traffic = None
         tp = os.path.join(ROOT, "profiles", "transport_kernel_traffic.json")
-        if os.path.exists(tp):
+        if os.path.exists(tp) and args.inelastic == "kieft":   # captured on the Kieft workload
             with open(tp) as f:
                 traffic = json.load(f).get("dram_bytes_per_launch")
-        cpu = None if args.no_cpu_baseline else cpu_baseline(tri_path, mat, recs, tmp)
+        cpu = None if args.no_cpu_baseline else cpu_baseline(tri_path, mat, recs, tmp, penn=args.inelastic == "penn")
         line = {
             "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "parallelism": "replicas x%d" % world,
+            "config": {"workload": workload_name(args), "inelastic": args.inelastic,
+                       "parallelism": "replicas x%d" % world,
                        "l2": "inputs larger than L2 (primary queue %.0f MB per step)" % (n * 48 / 1e6),
                        "autotuned": {"blocks_per_sm_variant": tuned[0], "block_size": tuned[1]}},
             "primaries_per_s": prim_all / t_dev,

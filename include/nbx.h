@@ -14,9 +14,11 @@
  *   nbx_octree_build      octree_builder::linearized_octree(octree_root(tris))
  *                                                       geometry/octree/octree_builder.cpp:171-352
  *   nbx_material_load     material<...>::create(hdf5_file) with kieft_elastic /
- *                         kieft_inelastic loaders      core/material.inl:25-34,
+ *                         kieft_inelastic / full_penn loaders
+ *                                                       core/material.inl:25-34,
  *                                                       physics/kieft/elastic.h:120-166,
- *                                                       physics/kieft/inelastic.h:212-327
+ *                                                       physics/kieft/inelastic.h:212-327,
+ *                                                       physics/full_penn.h:296-392
  *   nbx_create            gpu_driver constructor       drivers/gpu/gpu_driver.inl:51-89
  *   nbx_set_geometry      octree<true>::create         geometry/octree.inl:280-313
  *   nbx_add_material      gpu_material_manager::create core/gpu_material_manager.inl:5-26
@@ -30,6 +32,7 @@
  *   nbx_table_query       table_1D::get, table_2D::get / get_rounddown
  *                                                       common/util/table_1D.inl:66-80,
  *                                                       common/util/table_2D.inl:74-104
+ *   nbx_table3_query      table_3D::get / get_rounddown common/util/table_3D.inl:79-122
  */
 #ifndef NBX_H
 #define NBX_H
@@ -126,9 +129,20 @@ typedef struct {
     const float* data;
 } nbx_table2d;
 
-/* Kieft & Bosch material, tables already transformed as the reference
- * loaders do (log IMFP, clamped cos-theta ICDF, log omega' ICDF, rebuilt
- * ionisation table). */
+/* util::table_3D (common/util/table_3D.inl:66-122): data[(x * height + y) *
+ * depth + z]. */
+typedef struct {
+    int32_t width, height, depth;
+    float x_min, x_step, y_min, y_step, z_min, z_step;
+    const float* data;
+} nbx_table3d;
+
+/* Material tables already transformed as the reference loaders do: Kieft
+ * elastic (log IMFP, clamped cos-theta ICDF) and the Kieft inelastic model
+ * (log IMFP, log omega' ICDF, rebuilt ionisation table;
+ * physics/kieft/inelastic.h:212-327) and/or the full Penn model (log IMFP,
+ * log omega ICDF, q ICDF in eV^1/2, 3-D ionisation table with -1 for "no
+ * inner shell"; physics/full_penn.h:296-392). */
 typedef struct {
     float barrier;
     nbx_table1d elastic_imfp;
@@ -140,9 +154,21 @@ typedef struct {
     nbx_table2d ionisation;
     float fermi;
     float band_gap;
-    float max_energy; /* min over mechanisms of exp(IMFP axis maximum) */
+    float max_energy; /* min over mechanisms of exp(IMFP axis maximum), Kieft model (Penn if no Kieft tables) */
     char name[64];
+    int32_t has_kieft_inelastic;
+    int32_t has_full_penn;
+    nbx_table1d penn_imfp;
+    nbx_table2d penn_omega_icdf;
+    nbx_table3d penn_q_icdf;
+    nbx_table3d penn_ionisation;
+    float penn_max_energy; /* as max_energy, full Penn model */
 } nbx_material;
+
+/* Inelastic model of a context (physics_config.h:21-33 selects it at compile
+ * time in the reference; the stock build uses full Penn). */
+#define NBX_INELASTIC_KIEFT 0
+#define NBX_INELASTIC_FULL_PENN 1
 
 typedef struct {
     int32_t device;            /* CUDA device ordinal */
@@ -154,6 +180,7 @@ typedef struct {
     int32_t block_size;        /* threads per block of the transport kernel; 0 = 256 */
     int32_t blocks_per_sm;     /* transport variant: 2, 3 or 4 resident 256-thread blocks per SM, or 7
                                   128-thread blocks (block_size capped at 128); 0 = 3 */
+    int32_t inelastic_model;   /* NBX_INELASTIC_KIEFT (0, default) or NBX_INELASTIC_FULL_PENN */
 } nbx_config;
 
 typedef struct {
@@ -283,9 +310,16 @@ int nbx_mlp_predict(nbx_ctx* ctx, const float* features, uint64_t n, float* out)
 int nbx_ray_query(nbx_ctx* ctx, const float* pos, const float* dir, const float* dist, const int32_t* ignore_tri,
                   const int32_t* ignore_mat, uint64_t n, float* out_dist, int32_t* out_tri);
 /* table: 0 elastic log-IMFP, 1 elastic cos-theta ICDF, 2 inelastic log-IMFP,
- *        3 inelastic log-omega' ICDF, 4 ionisation (rounddown). */
+ *        3 inelastic log-omega' ICDF (log-omega under full Penn),
+ *        4 Kieft ionisation (rounddown; not under full Penn). */
 int nbx_table_query(nbx_ctx* ctx, int32_t material, int32_t table, const float* x, const float* y, uint64_t n,
                     float* out);
+/* Full Penn 3-D tables of a context created with NBX_INELASTIC_FULL_PENN
+ * (table_3D::get / get_rounddown, common/util/table_3D.inl:79-122):
+ * table 0 q ICDF at (log E, omega / E, P), 1 ionisation at
+ * (log E, log(omega / E), P). */
+int nbx_table3_query(nbx_ctx* ctx, int32_t material, int32_t table, const float* x, const float* y, const float* z,
+                     uint64_t n, float* out);
 /* Philox4x32-10 blocks: ctr n x 4, key n x 2, out n x 4. */
 int nbx_philox(nbx_ctx* ctx, const uint32_t* ctr, const uint32_t* key, uint64_t n, uint32_t* out);
 

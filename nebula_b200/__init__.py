@@ -50,17 +50,29 @@ class Table2D(C.Structure):
                 ("y_min", C.c_float), ("y_step", C.c_float), ("data", C.POINTER(C.c_float))]
 
 
+class Table3D(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("depth", C.c_int32), ("x_min", C.c_float),
+                ("x_step", C.c_float), ("y_min", C.c_float), ("y_step", C.c_float), ("z_min", C.c_float),
+                ("z_step", C.c_float), ("data", C.POINTER(C.c_float))]
+
+
 class Material(C.Structure):
     _fields_ = [("barrier", C.c_float), ("elastic_imfp", Table1D), ("elastic_icdf", Table2D),
                 ("phonon_loss", C.c_float), ("recoil_const", C.c_float), ("inelastic_imfp", Table1D),
                 ("inelastic_icdf", Table2D), ("ionisation", Table2D), ("fermi", C.c_float),
-                ("band_gap", C.c_float), ("max_energy", C.c_float), ("name", C.c_char * 64)]
+                ("band_gap", C.c_float), ("max_energy", C.c_float), ("name", C.c_char * 64),
+                ("has_kieft_inelastic", C.c_int32), ("has_full_penn", C.c_int32), ("penn_imfp", Table1D),
+                ("penn_omega_icdf", Table2D), ("penn_q_icdf", Table3D), ("penn_ionisation", Table3D),
+                ("penn_max_energy", C.c_float)]
+
+
+INELASTIC_MODELS = {"kieft": 0, "penn": 1, "full_penn": 1}
 
 
 class Config(C.Structure):
     _fields_ = [("device", C.c_int32), ("seed", C.c_uint32), ("energy_threshold", C.c_float),
                 ("capacity", C.c_uint64), ("record_detected", C.c_int32), ("record_capacity", C.c_uint64),
-                ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32)]
+                ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("inelastic_model", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -125,6 +137,7 @@ def lib():
         "nbx_reset_tallies": (C.c_int, [_vp]),
         "nbx_ray_query": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_uint64, _vp, _vp]),
         "nbx_table_query": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp, _vp, C.c_uint64, _vp]),
+        "nbx_table3_query": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp, _vp, _vp, C.c_uint64, _vp]),
         "nbx_philox": (C.c_int, [_vp, _vp, _vp, C.c_uint64, _vp]),
         "nbx_step_query": (C.c_int, [_vp, _vp, C.c_uint64, _vp, _vp, _vp, _vp]),
         "nbx_set_uid_base": (C.c_int, [_vp, C.c_uint64]),
@@ -230,8 +243,19 @@ class HostMaterial:
             a = np.ctypeslib.as_array(t.data, (t.width * t.height,)).copy().reshape(t.width, t.height)
             return a, (t.x_min, t.x_step, t.y_min, t.y_step)
 
-        self.tables = {"el_imfp": t1(m.elastic_imfp), "in_imfp": t1(m.inelastic_imfp), "el_icdf": t2(m.elastic_icdf),
-                       "in_icdf": t2(m.inelastic_icdf), "ion": t2(m.ionisation)}
+        def t3(t):
+            a = np.ctypeslib.as_array(t.data, (t.width * t.height * t.depth,)).copy()
+            return a.reshape(t.width, t.height, t.depth), (t.x_min, t.x_step, t.y_min, t.y_step, t.z_min, t.z_step)
+
+        self.has_kieft_inelastic, self.has_penn = bool(m.has_kieft_inelastic), bool(m.has_full_penn)
+        self.penn_max_energy = m.penn_max_energy
+        self.tables = {"el_imfp": t1(m.elastic_imfp), "el_icdf": t2(m.elastic_icdf)}
+        if self.has_kieft_inelastic:
+            self.tables.update({"in_imfp": t1(m.inelastic_imfp), "in_icdf": t2(m.inelastic_icdf),
+                                "ion": t2(m.ionisation)})
+        if self.has_penn:
+            self.tables.update({"penn_imfp": t1(m.penn_imfp), "penn_omega_icdf": t2(m.penn_omega_icdf),
+                                "penn_q_icdf": t3(m.penn_q_icdf), "penn_ion": t3(m.penn_ionisation)})
 
     def __del__(self):
         if getattr(self, "_p", None):
@@ -246,13 +270,14 @@ class Context:
     """One simulation context on one GPU (the reference's gpu_driver)."""
 
     def __init__(self, device=0, seed=0x78C7E39B, energy_threshold=0.0, record_detected=False,
-                 record_capacity=0, capacity=0, block_size=0, blocks_per_sm=0):
+                 record_capacity=0, capacity=0, block_size=0, blocks_per_sm=0, inelastic="kieft"):
         L = lib()
         cfg = Config()
         L.nbx_config_default(C.byref(cfg))
         cfg.device, cfg.seed, cfg.energy_threshold = device, seed, energy_threshold
         cfg.record_detected, cfg.record_capacity, cfg.capacity = int(record_detected), record_capacity, capacity
         cfg.block_size, cfg.blocks_per_sm = block_size, blocks_per_sm
+        cfg.inelastic_model = INELASTIC_MODELS.get(inelastic, inelastic)
         self.h = _vp()
         _check(L.nbx_create(C.byref(self.h), C.byref(cfg)))
         self.L = L
@@ -363,6 +388,16 @@ class Context:
         out = np.zeros_like(x)
         self._ck(self.L.nbx_table_query(self.h, material, TABLE_IDS.get(table, table), _ptr(x), _ptr(y), len(x),
                                         _ptr(out)))
+        return out
+
+    def table3_query(self, material, table, x, y, z):
+        """Full Penn 3-D tables: table "q" (or 0) / "ion3" (or 1)."""
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        z = np.ascontiguousarray(z, np.float32)
+        out = np.zeros_like(x)
+        t = {"q": 0, "ion3": 1}.get(table, table)
+        self._ck(self.L.nbx_table3_query(self.h, material, t, _ptr(x), _ptr(y), _ptr(z), len(x), _ptr(out)))
         return out
 
     def philox(self, ctr, key):

@@ -26,12 +26,21 @@ struct Table2D {
     int w, h;
     float x_min, x_step, y_min, y_step;
 };
+struct Table3D {
+    const float* data;
+    int w, h, d;
+    float x_min, x_step, y_min, y_step, z_min, z_step;
+};
+// in_imfp / in_icdf hold the chosen inelastic model's log-IMFP and
+// log-energy-loss ICDF (Kieft: omega', full Penn: omega); ion is Kieft's
+// rebuilt 2-D ionisation table, q and ion3 the full Penn 3-D tables.
 struct Material {
     float barrier;
     float phonon_loss, recoil_const;
     float fermi, band_gap;
     Table1D el_imfp, in_imfp;
     Table2D el_icdf, in_icdf, ion;
+    Table3D q, ion3;
 };
 // Triangles as three float4: (r0, mat_in bits), (e1, mat_out bits), (e2, 0).
 struct Geometry {
@@ -48,6 +57,7 @@ struct Physics {
     int n_mat;
     uint32_t seed;
     float min_energy, max_energy;
+    int penn;   // inelastic model: 0 Kieft & Bosch, 1 full Penn
 };
 
 struct Electron {

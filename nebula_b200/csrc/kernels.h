@@ -101,6 +101,9 @@ cudaError_t launch_ray_query(const dev::Geometry& g, const float* pos, const flo
                              int32_t* out_tri, cudaStream_t s);
 cudaError_t launch_table_query(const dev::Material& m, int table, const float* x, const float* y, uint64_t n,
                                float* out, cudaStream_t s);
+// table 0: full Penn q ICDF (table_3D::get), 1: full Penn ionisation (get_rounddown)
+cudaError_t launch_table3_query(const dev::Material& m, int table, const float* x, const float* y, const float* z,
+                                uint64_t n, float* out, cudaStream_t s);
 cudaError_t launch_philox(const uint32_t* ctr, const uint32_t* key, uint64_t n, uint32_t* out, cudaStream_t s);
 // electrons: 56-byte nbx_electron records
 cudaError_t launch_step_query(const dev::Physics& P, void* electrons, uint64_t n, int32_t* status, int32_t* event,

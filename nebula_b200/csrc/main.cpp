@@ -119,6 +119,8 @@ int main(int argc, char** argv) {
     p.add("seed", "Random seed", std::to_string(0x78c7e39b));
     p.add("sort-primaries", "Sort primary electrons before simulation", "0");
     p.add("device", "CUDA device ordinal", "0");
+    p.add("inelastic", "Inelastic model: kieft (Kieft & Bosch) or penn (full Penn, the reference's stock build)",
+          "kieft");
     try {
         p.parse(argc, argv);
     } catch (const std::exception& e) {
@@ -133,7 +135,9 @@ int main(int argc, char** argv) {
     const uint32_t seed = p.get<uint32_t>("seed");
     const bool sort_primaries = p.get<bool>("sort-primaries");
     const int device = p.get<int>("device");
-    if (p.positional.size() < 3 || capacity == 0 || prescan == 0 || batch_factor <= 0) {
+    const std::string inelastic = p.get<std::string>("inelastic");
+    if (p.positional.size() < 3 || capacity == 0 || prescan == 0 || batch_factor <= 0 ||
+        (inelastic != "kieft" && inelastic != "penn")) {
         p.usage(std::cerr);
         return 1;
     }
@@ -184,7 +188,7 @@ int main(int argc, char** argv) {
             return 1;
         }
         std::fprintf(stderr, "  Material %zu:\n    Name: %s\n", i - 2, m->name);
-        max_energy = std::min(max_energy, m->max_energy);
+        max_energy = std::min(max_energy, inelastic == "penn" ? m->penn_max_energy : m->max_energy);
         mats.push_back(m);
     }
     timer.stop("Loading materials");
@@ -253,6 +257,7 @@ int main(int argc, char** argv) {
     cfg.device = device;
     cfg.seed = seed;
     cfg.energy_threshold = energy_threshold;
+    cfg.inelastic_model = inelastic == "penn" ? NBX_INELASTIC_FULL_PENN : NBX_INELASTIC_KIEFT;
     cfg.record_detected = 1;
     cfg.record_capacity = 1ull << 24;
     nbx_ctx* ctx = nullptr;

@@ -90,9 +90,12 @@ struct Axis {
     double first = 0, step = 0;
     bool log = false;
     size_t n = 0;
+    Quantity dim;   // the scale's unit dimension (value 1)
     double at(size_t i) const { return log ? first * std::exp(i * step) : first + i * step; }
     double front() const { return first; }
     double back() const { return at(n - 1); }
+    Quantity unit_front() const { Quantity q = dim; q.value = front(); return q; }
+    Quantity unit_back() const { Quantity q = dim; q.value = back(); return q; }
 };
 
 Axis dimscale(const h5::File& f, const std::string& path, int dim, int n_expected, bool logarithmic) {
@@ -110,6 +113,8 @@ Axis dimscale(const h5::File& f, const std::string& path, int dim, int n_expecte
     }
     if (values.size() != size_t(n_expected)) throw std::runtime_error("Dimension scale has unexpected size.");
     const Quantity u = parse_unit(units);
+    a.dim = u;
+    a.dim.value = 1;
     // Spacing check on the raw values (one-sided, as the reference does).
     Axis chk;
     chk.n = values.size();
@@ -153,6 +158,35 @@ Table2D read_table2d(const h5::File& f, const std::string& path) {
     return t;
 }
 
+Table3D read_table3d(const h5::File& f, const std::string& path) {
+    std::vector<uint64_t> dims;
+    auto v = f.read_dataset(path, &dims);
+    if (dims.size() != 3) throw std::runtime_error("Dataspace has unexpected dimension");
+    Table3D t;
+    t.width = int(dims[0]);
+    t.height = int(dims[1]);
+    t.depth = int(dims[2]);
+    t.data.resize(v.size());
+    for (size_t i = 0; i < v.size(); ++i) t.data[i] = float(v[i]);
+    return t;
+}
+
+// table_3D::set_scale (source/common/util/table_3D.inl:155-166)
+void set_scale(Table3D& t, float x_min, float x_max, float y_min, float y_max, float z_min, float z_max) {
+    t.x_min = x_min;
+    t.x_step = (t.width - 1) / (x_max - x_min);
+    t.y_min = y_min;
+    t.y_step = (t.height - 1) / (y_max - y_min);
+    t.z_min = z_min;
+    t.z_step = (t.depth - 1) / (z_max - z_min);
+}
+
+// units::quantity -> scalar conversion (source/common/units/quantity.h:32-37)
+double scalar(const Quantity& q, const std::string& what) {
+    if (!q.dimensionless()) throw std::runtime_error("Can only convert dimensionless quantity to scalar (" + what + ")");
+    return q.value;
+}
+
 void set_scale(Table1D& t, const Axis& x) {
     const float x_min = float(std::log(x.front() / kEV.value));
     const float x_max = float(std::log(x.back() / kEV.value));
@@ -174,6 +208,64 @@ void load_log_imfp(const h5::File& f, const std::string& path, Table1D* t) {
     const Quantity u = mul(dataset_unit(f, path), kNM);
     const float unit = float(as_double(u, path + " units"));
     for (int x = 0; x < t->n; ++x) t->data[size_t(x)] = std::log(t->data[size_t(x)] * unit);
+}
+
+// full_penn::create (source/physics/full_penn.h:296-392), operation for
+// operation: float products where the reference multiplies two reals, double
+// where it works on quantities.
+void load_penn(const h5::File& f, const Quantity& fermi_q, MaterialTables* m) {
+    load_log_imfp(f, "/full_penn/imfp", &m->penn_imfp);
+    {
+        const std::string path = "/full_penn/omega_icdf";
+        Table2D& t = m->penn_omega_icdf;
+        t = read_table2d(f, path);
+        const Axis K = dimscale(f, path, 0, t.width, true);
+        const Axis P = dimscale(f, path, 1, t.height, false);
+        set_scale(t, float(std::log(K.front() / kEV.value)), float(std::log(K.back() / kEV.value)),
+                  float(P.front()), float(P.back()));
+        const float unit = float(as_double(div(dataset_unit(f, path), kEV), path + " units"));
+        for (int x = 0; x < t.width; ++x) {
+            const double K_x = K.at(size_t(x));
+            for (int y = 0; y < t.height; ++y) {
+                float& v = t.data[size_t(x) * t.height + y];
+                const double a = (K_x - fermi_q.value) / kEV.value;
+                const double b = double(v * unit);
+                v = float(std::log(std::max(0.0, std::min<double>(a, b))));
+            }
+        }
+    }
+    {
+        const std::string path = "/full_penn/q_icdf";
+        Table3D& t = m->penn_q_icdf;
+        t = read_table3d(f, path);
+        const Axis K = dimscale(f, path, 0, t.width, true);
+        const Axis W = dimscale(f, path, 1, t.height, false);
+        const Axis P = dimscale(f, path, 2, t.depth, false);
+        set_scale(t, float(std::log(K.front() / kEV.value)), float(std::log(K.back() / kEV.value)),
+                  float(W.front()), float(W.back()), float(P.front()), float(P.back()));
+        // hbar / sqrt(2 m_e) = 0.19519 nm eV^1/2; the product must be dimensionless
+        Quantity u = dataset_unit(f, path);
+        u.value = u.value * 0.19519;
+        const float unit = float(scalar(mul(u, kNM), path + " units"));
+        for (auto& v : t.data) v = v * unit;
+    }
+    {
+        const std::string path = "/ionization/binding_icdf";
+        Table3D& t = m->penn_ionisation;
+        t = read_table3d(f, path);
+        const Axis K = dimscale(f, path, 0, t.width, true);
+        const Axis O = dimscale(f, path, 1, t.height, true);
+        const Axis P = dimscale(f, path, 2, t.depth, false);
+        set_scale(t, float(std::log(K.front() / kEV.value)), float(std::log(K.back() / kEV.value)),
+                  float(std::log(scalar(O.unit_front(), path + " omega axis"))),
+                  float(std::log(scalar(O.unit_back(), path + " omega axis"))), float(P.front()), float(P.back()));
+        const float unit = float(as_double(div(dataset_unit(f, path), kEV), path + " units"));
+        for (auto& v : t.data) {
+            float binding = v * unit;
+            if (binding < 50 || !std::isfinite(binding)) binding = -1;
+            v = binding;
+        }
+    }
 }
 }  // namespace
 
@@ -218,9 +310,9 @@ float table2d_get_rounddown(const Table2D& t, float x, float y) {
     return t.at(low_x, low_y);
 }
 
-float MaterialTables::max_energy() const {
+float MaterialTables::max_energy(bool penn) const {
     float e = std::numeric_limits<float>::infinity();
-    const float ein = std::exp(in_imfp.get_scalemax());
+    const float ein = std::exp((penn ? penn_imfp : in_imfp).get_scalemax());
     if (ein < e) e = ein;
     const float eel = std::exp(el_imfp.get_scalemax());
     if (eel < e) e = eel;
@@ -260,15 +352,20 @@ MaterialTables load_material(const std::string& filename) {
         m.recoil_const = 2 * float(as_double(r, "effective_A"));
     }
 
-    // kieft_inelastic::create (source/physics/kieft/inelastic.h:212-327)
-    if (!f.exists("kieft/inelastic"))
-        throw std::runtime_error("Kieft inelastic model not found in material file " + filename);
     const Quantity fermi_q = property(f, "fermi");
     m.fermi = float(as_double(div(fermi_q, kEV), "fermi"));
     if (f.has_attribute("/", "band_gap"))
         m.band_gap = float(as_double(div(property(f, "band_gap"), kEV), "band_gap"));
     else
         m.band_gap = float(-1.0 * kEV.value / kEV.value);
+    m.has_penn = f.exists("/full_penn");
+    m.has_kieft_inelastic = f.exists("kieft/inelastic");
+    if (!m.has_kieft_inelastic && !m.has_penn)
+        throw std::runtime_error("No inelastic model (Kieft or full Penn) found in material file " + filename);
+    if (m.has_penn) load_penn(f, fermi_q, &m);
+    if (!m.has_kieft_inelastic) return m;
+
+    // kieft_inelastic::create (source/physics/kieft/inelastic.h:212-327)
     load_log_imfp(f, "/kieft/inelastic/imfp", &m.in_imfp);
     {
         const std::string path = "/kieft/inelastic/w0_icdf";

@@ -1,4 +1,5 @@
-// Material tables for the Kieft & Bosch physics, loaded from a Nebula .mat file.
+// Material tables for the Kieft & Bosch physics (and the full Penn inelastic
+// model when the file has it), loaded from a Nebula .mat file.
 //
 // The table transforms mirror the reference loaders exactly (same float/double
 // operations in the same order), so the device tables are bit-identical to the
@@ -8,7 +9,9 @@
 //                                                phonon loss, recoil constant
 //   * source/physics/kieft/inelastic.h:212-327   log-IMFP, log omega' ICDF,
 //                                                rebuilt ionisation table
-//   * source/io/hdf5_file.cpp:291-375            axis reconstruction and units
+//   * source/physics/full_penn.h:296-392         log-IMFP, log omega ICDF, q ICDF,
+//                                                3-D ionisation table
+//   * source/io/hdf5_file.cpp:269-375            3-D tables, axis reconstruction and units
 #pragma once
 
 #include <string>
@@ -32,6 +35,13 @@ struct Table2D {
     float at(int x, int y) const { return data[size_t(x) * height + y]; }
 };
 
+// util::table_3D, data[(x * height + y) * depth + z] (source/common/util/table_3D.inl:66-70).
+struct Table3D {
+    int width = 0, height = 0, depth = 0;
+    float x_min = 0, x_step = 0, y_min = 0, y_step = 0, z_min = 0, z_step = 0;
+    std::vector<float> data;
+};
+
 struct MaterialTables {
     std::string filename, name, cstool_version;
     float barrier = 0;
@@ -46,8 +56,16 @@ struct MaterialTables {
     Table2D ionisation;       // binding / eV vs (log omega', P), use rounddown
     float fermi = 0;
     float band_gap = -1;
-    // min over the mechanisms of exp(imfp scale max)
-    float max_energy() const;
+    bool has_kieft_inelastic = false;
+    // full_penn (source/physics/full_penn.h:296-392), when the file has it
+    bool has_penn = false;
+    Table1D penn_imfp;        // log(imfp * nm) vs log(E / eV)
+    Table2D penn_omega_icdf;  // log(omega / eV) vs (log E, P)
+    Table3D penn_q_icdf;      // hbar q / sqrt(2m) in eV^1/2 vs (log E, omega / E, P)
+    Table3D penn_ionisation;  // binding / eV (-1: none) vs (log E, log(omega / E), P), use rounddown
+    // min over the mechanisms of exp(imfp scale max), for the Kieft or the
+    // full Penn inelastic model
+    float max_energy(bool penn = false) const;
 };
 
 // Dimensioned unit value in Nebula's unit system (eV, nm, ns, K, e), as parsed

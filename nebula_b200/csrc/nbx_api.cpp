@@ -194,6 +194,17 @@ nbx::dev::Table2D upload2d(nbx_ctx* ctx, const nbx_table2d& t) {
     return nbx::dev::Table2D{b->p, t.width, t.height, t.x_min, t.x_step, t.y_min, t.y_step};
 }
 
+nbx::dev::Table3D upload3d(nbx_ctx* ctx, const nbx_table3d& t) {
+    if (t.width < 2 || t.height < 2 || t.depth < 2 || !t.data)
+        throw ApiError(NBX_ERR_ARG, "3D table needs at least 2x2x2 points");
+    auto* b = new DevBuf<float>();
+    ctx->tables.push_back(b);
+    const size_t n = size_t(t.width) * size_t(t.height) * size_t(t.depth);
+    b->alloc(n);
+    ck(cudaMemcpy(b->p, t.data, sizeof(float) * n, cudaMemcpyHostToDevice), "table upload");
+    return nbx::dev::Table3D{b->p, t.width, t.height, t.depth, t.x_min, t.x_step, t.y_min, t.y_step, t.z_min, t.z_step};
+}
+
 void ensure_tags(nbx_ctx* ctx, uint64_t n_tags) {
     if (n_tags <= ctx->n_tags) return;
     DevBuf<uint32_t> s, b;
@@ -250,8 +261,21 @@ void fill_material(const nbx::MaterialTables& m, nbx_material* out) {
                        m.ionisation.y_min, m.ionisation.y_step, dup(m.ionisation.data)};
     out->fermi = m.fermi;
     out->band_gap = m.band_gap;
-    out->max_energy = m.max_energy();
+    out->max_energy = m.max_energy(!m.has_kieft_inelastic);
     std::snprintf(out->name, sizeof(out->name), "%s", m.name.c_str());
+    out->has_kieft_inelastic = m.has_kieft_inelastic ? 1 : 0;
+    out->has_full_penn = m.has_penn ? 1 : 0;
+    auto t3 = [&](const nbx::Table3D& t) {
+        return nbx_table3d{t.width, t.height, t.depth, t.x_min, t.x_step, t.y_min, t.y_step, t.z_min, t.z_step,
+                           dup(t.data)};
+    };
+    out->penn_imfp = {m.penn_imfp.n, m.penn_imfp.x_min, m.penn_imfp.x_step, dup(m.penn_imfp.data)};
+    out->penn_omega_icdf = {m.penn_omega_icdf.width, m.penn_omega_icdf.height, m.penn_omega_icdf.x_min,
+                            m.penn_omega_icdf.x_step, m.penn_omega_icdf.y_min, m.penn_omega_icdf.y_step,
+                            dup(m.penn_omega_icdf.data)};
+    out->penn_q_icdf = t3(m.penn_q_icdf);
+    out->penn_ionisation = t3(m.penn_ionisation);
+    out->penn_max_energy = m.has_penn ? m.max_energy(true) : 0.0f;
 }
 
 }  // namespace
@@ -394,6 +418,10 @@ void nbx_material_free(nbx_material* m) {
     std::free(const_cast<float*>(m->inelastic_imfp.data));
     std::free(const_cast<float*>(m->inelastic_icdf.data));
     std::free(const_cast<float*>(m->ionisation.data));
+    std::free(const_cast<float*>(m->penn_imfp.data));
+    std::free(const_cast<float*>(m->penn_omega_icdf.data));
+    std::free(const_cast<float*>(m->penn_q_icdf.data));
+    std::free(const_cast<float*>(m->penn_ionisation.data));
     std::free(m);
 }
 
@@ -445,6 +473,9 @@ int nbx_create(nbx_ctx** out, const nbx_config* cfg) {
         }
         ctx->phys.seed = c.seed;
         ctx->phys.min_energy = c.energy_threshold;
+        if (c.inelastic_model != NBX_INELASTIC_KIEFT && c.inelastic_model != NBX_INELASTIC_FULL_PENN)
+            throw ApiError(NBX_ERR_ARG, "inelastic_model must be NBX_INELASTIC_KIEFT or NBX_INELASTIC_FULL_PENN");
+        ctx->phys.penn = c.inelastic_model == NBX_INELASTIC_FULL_PENN ? 1 : 0;
         ctx->phys.max_energy = std::numeric_limits<float>::infinity();
         return NBX_OK;
     });
@@ -517,14 +548,29 @@ int nbx_add_material(nbx_ctx* ctx, const nbx_material* m) {
         d.fermi = m->fermi;
         d.band_gap = m->band_gap;
         d.el_imfp = upload1d(ctx, m->elastic_imfp);
-        d.in_imfp = upload1d(ctx, m->inelastic_imfp);
         d.el_icdf = upload2d(ctx, m->elastic_icdf);
-        d.in_icdf = upload2d(ctx, m->inelastic_icdf);
-        d.ion = upload2d(ctx, m->ionisation);
+        float max_energy = m->max_energy;
+        if (ctx->phys.penn) {
+            // full_penn (physics/full_penn.h): log-IMFP and log-omega ICDF in
+            // the inelastic slots, plus the two 3-D tables
+            if (!m->has_full_penn)
+                throw ApiError(NBX_ERR_FORMAT, std::string("material has no full Penn tables: ") + m->name);
+            d.in_imfp = upload1d(ctx, m->penn_imfp);
+            d.in_icdf = upload2d(ctx, m->penn_omega_icdf);
+            d.q = upload3d(ctx, m->penn_q_icdf);
+            d.ion3 = upload3d(ctx, m->penn_ionisation);
+            max_energy = m->penn_max_energy;
+        } else {
+            if (!m->has_kieft_inelastic && m->inelastic_imfp.n < 2)
+                throw ApiError(NBX_ERR_FORMAT, std::string("material has no Kieft inelastic tables: ") + m->name);
+            d.in_imfp = upload1d(ctx, m->inelastic_imfp);
+            d.in_icdf = upload2d(ctx, m->inelastic_icdf);
+            d.ion = upload2d(ctx, m->ionisation);
+        }
         ctx->phys.mat[ctx->n_mat++] = d;
         ctx->phys.n_mat = ctx->n_mat;
         // cpu_material_manager::get_max_energy (core/cpu_material_manager.inl:43-55)
-        if (m->max_energy < ctx->max_energy) ctx->max_energy = m->max_energy;
+        if (max_energy < ctx->max_energy) ctx->max_energy = max_energy;
         ctx->phys.max_energy = ctx->max_energy;
         return NBX_OK;
     });
@@ -839,6 +885,7 @@ int nbx_table_query(nbx_ctx* ctx, int32_t material, int32_t table, const float* 
                     float* out) {
     if (!ctx || (n && (!x || !out))) return NBX_ERR_ARG;
     if (material < 0 || material >= ctx->n_mat || table < 0 || table > 4) return fail(ctx, NBX_ERR_ARG, "bad material/table");
+    if (table == 4 && ctx->phys.penn) return fail(ctx, NBX_ERR_ARG, "no Kieft ionisation table under full Penn");
     return guarded(ctx, [&] {
         if (n == 0) return NBX_OK;
         DevBuf<float> dx, dy, dout;
@@ -848,6 +895,26 @@ int nbx_table_query(nbx_ctx* ctx, int32_t material, int32_t table, const float* 
         if (y) ck(cudaMemcpyAsync(dy.p, y, 4 * n, cudaMemcpyHostToDevice, s), "H2D");
         else ck(cudaMemsetAsync(dy.p, 0, 4 * n, s), "memset");
         ck(nbx::launch_table_query(ctx->phys.mat[material], table, dx.p, dy.p, n, dout.p, s), "table query");
+        ck(cudaMemcpyAsync(out, dout.p, 4 * n, cudaMemcpyDeviceToHost, s), "D2H");
+        ck(cudaStreamSynchronize(s), "sync");
+        return NBX_OK;
+    });
+}
+
+int nbx_table3_query(nbx_ctx* ctx, int32_t material, int32_t table, const float* x, const float* y, const float* z,
+                     uint64_t n, float* out) {
+    if (!ctx || (n && (!x || !y || !z || !out))) return NBX_ERR_ARG;
+    if (material < 0 || material >= ctx->n_mat || table < 0 || table > 1) return fail(ctx, NBX_ERR_ARG, "bad material/table");
+    if (!ctx->phys.penn) return fail(ctx, NBX_ERR_STATE, "3-D tables are loaded only for the full Penn model");
+    return guarded(ctx, [&] {
+        if (n == 0) return NBX_OK;
+        DevBuf<float> dx, dy, dz, dout;
+        dx.alloc(n); dy.alloc(n); dz.alloc(n); dout.alloc(n);
+        auto s = ctx->stream;
+        ck(cudaMemcpyAsync(dx.p, x, 4 * n, cudaMemcpyHostToDevice, s), "H2D");
+        ck(cudaMemcpyAsync(dy.p, y, 4 * n, cudaMemcpyHostToDevice, s), "H2D");
+        ck(cudaMemcpyAsync(dz.p, z, 4 * n, cudaMemcpyHostToDevice, s), "H2D");
+        ck(nbx::launch_table3_query(ctx->phys.mat[material], table, dx.p, dy.p, dz.p, n, dout.p, s), "table query");
         ck(cudaMemcpyAsync(out, dout.p, 4 * n, cudaMemcpyDeviceToHost, s), "D2H");
         ck(cudaStreamSynchronize(s), "sync");
         return NBX_OK;

@@ -379,6 +379,12 @@ __global__ void table_query_kernel(const dev::Material m, int table, const float
     }
 }
 
+__global__ void table3_query_kernel(const dev::Material m, int table, const float* x, const float* y, const float* z,
+                                    uint64_t n, float* out) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+        out[i] = table == 0 ? dev::table3d_get(m.q, x[i], y[i], z[i]) : dev::table3d_rounddown(m.ion3, x[i], y[i], z[i]);
+}
+
 __global__ void philox_kernel(const uint32_t* ctr, const uint32_t* key, uint64_t n, uint32_t* out) {
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
         const uint4 c = make_uint4(ctr[4 * i], ctr[4 * i + 1], ctr[4 * i + 2], ctr[4 * i + 3]);
@@ -669,6 +675,13 @@ cudaError_t launch_table_query(const dev::Material& m, int table, const float* x
                                float* out, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     table_query_kernel<<<grid_for(n, 256), 256, 0, s>>>(m, table, x, y, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_table3_query(const dev::Material& m, int table, const float* x, const float* y, const float* z,
+                                uint64_t n, float* out, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    table3_query_kernel<<<grid_for(n, 256), 256, 0, s>>>(m, table, x, y, z, n, out);
     return cudaGetLastError();
 }
 

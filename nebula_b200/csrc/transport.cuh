@@ -92,6 +92,40 @@ __device__ __forceinline__ float table2d_rounddown(const Table2D& t, float x, fl
     return __ldg(t.data + size_t(lx) * t.h + ly);
 }
 
+// table_3D::get / get_rounddown (common/util/table_3D.inl:79-122); element
+// (i, j, k) at data[(j + i * height) * depth + k] (table_3D.inl:66-70).
+__device__ __forceinline__ float table3d_get(const Table3D& t, float x, float y, float z) {
+    const float xi = (x - t.x_min) * t.x_step;
+    const float yi = (y - t.y_min) * t.y_step;
+    const float zi = (z - t.z_min) * t.z_step;
+    const int lx = clampi(floor_to_int(xi), 0, t.w - 2);
+    const int ly = clampi(floor_to_int(yi), 0, t.h - 2);
+    const int lz = clampi(floor_to_int(zi), 0, t.d - 2);
+    const float* p00 = t.data + (size_t(lx) * t.h + ly) * t.d + lz;   // (lx,   ly)
+    const float* p10 = p00 + size_t(t.h) * t.d;                        // (lx+1, ly)
+    const float* p01 = p00 + t.d;                                      // (lx,   ly+1)
+    const float* p11 = p10 + t.d;                                      // (lx+1, ly+1)
+    const float v000 = __ldg(p00), v001 = __ldg(p00 + 1);
+    const float v100 = __ldg(p10), v101 = __ldg(p10 + 1);
+    const float v010 = __ldg(p01), v011 = __ldg(p01 + 1);
+    const float v110 = __ldg(p11), v111 = __ldg(p11 + 1);
+    const float fx = xi - float(lx);
+    const float fy = yi - float(ly);
+    const float fz = zi - float(lz);
+    return (1 - fx) * (1 - fy) * (1 - fz) * v000 + fx * (1 - fy) * (1 - fz) * v100 + (1 - fx) * fy * (1 - fz) * v010 +
+           fx * fy * (1 - fz) * v110 + (1 - fx) * (1 - fy) * fz * v001 + fx * (1 - fy) * fz * v101 +
+           (1 - fx) * fy * fz * v011 + fx * fy * fz * v111;
+}
+__device__ __forceinline__ float table3d_rounddown(const Table3D& t, float x, float y, float z) {
+    const float xi = (x - t.x_min) * t.x_step;
+    const float yi = (y - t.y_min) * t.y_step;
+    const float zi = (z - t.z_min) * t.z_step;
+    const int lx = clampi(floor_to_int(xi), 0, t.w - 1);
+    const int ly = clampi(floor_to_int(yi), 0, t.h - 1);
+    const int lz = clampi(floor_to_int(zi), 0, t.d - 1);
+    return __ldg(t.data + (size_t(lx) * t.h + ly) * t.d + lz);
+}
+
 // ---------------------------------------------------------------------------
 // Vector helpers (common/vector_math.h, CPU branches)
 // ---------------------------------------------------------------------------
@@ -440,6 +474,125 @@ __device__ __forceinline__ bool inelastic_finish(const Material& m, Electron& e,
     return true;
 }
 
+// Plasmon-decay rejection loop: at most this many rounds (the acceptance
+// ratio sqrt(x^2 + x) / (x + 1/2) is above 1/2 for x > 0.08, so 64 rounds
+// fail with probability far below one in 2^40); the last draw is kept then.
+constexpr uint32_t kMaxPlasmonRounds = 64;
+
+// full_penn<gpu, true>::execute (physics/full_penn.h:63-289) after the
+// log-omega ICDF lookup (log_omega), with d = normalised(dir) and
+// n = normalised(make_normal_vec(d, phi)) from the shared half.  Uniforms:
+// block 1 x binding, y q, z q-normal azimuth, w single-excitation radius or
+// the f < 0.1 plasmon draw; block 3 x, y the secondary's uniform_vector;
+// blocks 4, 5, ... the plasmon rejection rounds (U1, U2, U3).
+__device__ __forceinline__ bool penn_finish(const Physics& P, const Material& m, Electron& e, float log_omega,
+                                            float logE, V3 d, V3 n, uint4 r1, Electron* se) {
+    const float K = e.E;
+    const float omega = expf(log_omega);
+    // ionisation table at (log K, log(omega / K), P)
+    const float binding = table3d_rounddown(m.ion3, logE, logf(omega / K), u01(r1.x));
+    V3 sdir;
+    float se_E;
+    if (binding <= 0) {
+        if (!(omega > m.band_gap)) {
+            // sub-band-gap loss (longitudinal optical phonon): energy only; the
+            // reference stores the direction it normalised
+            e.dx = d.x;
+            e.dy = d.y;
+            e.dz = d.z;
+            e.E = K - omega;
+            return false;
+        }
+        // Fermi-sea excitation; q = hbar q / sqrt(2m) in eV^1/2
+        const float q = table3d_get(m.q, logE, omega / K, u01(r1.y));
+        const float c1 = clampr((omega + q * q) / (2 * sqrtf(K) * q), -1, 1);
+        const float s1 = sqrtf(1 - c1 * c1);
+        const V3 q_dir = normalised(V3{d.x * c1 + n.x * s1, d.y * c1 + n.y * s1, d.z * c1 + n.z * s1});
+        const V3 q_normal = normalised(make_normal_vec(q_dir, u01(r1.z)));
+        const float c2 = clampr((2 * K - omega - q * q) / (2 * sqrtf(K * (K - omega))), -1, 1);
+        const float s2 = sqrtf(1 - c2 * c2);
+        e.E = K - omega;
+        e.dx = d.x * c2 + n.x * s2;
+        e.dy = d.y * c2 + n.y * s2;
+        e.dz = d.z * c2 + n.z * s2;
+        const float k_fermi = sqrtf(m.fermi);
+        const float k_fermi_omega = sqrtf(m.fermi + omega);
+        if (q < k_fermi_omega - k_fermi) {
+            // plasmon decay: x = E_i / omega from p(x) ~ sqrt(x (x + 1)) on [0, f]
+            const float f = m.fermi / omega;
+            float x;
+            if (f < 0.1f) {
+                const float U = cbrtf(u01(r1.w));
+                x = f * U * U;
+            } else {
+                const float lower = max_ref(0, f - 1);
+                const float upper = f;
+                const float d1 = upper - lower;
+                const float d2 = upper * upper - lower * lower;
+                const float alpha = d2 / (d1 + d2);
+                for (uint32_t k = 0;; ++k) {
+                    const uint4 rk = draw(P.seed, e, 4 + k);
+                    const float U1 = u01(rk.x);
+                    const float U2 = u01(rk.y);
+                    x = (U1 < alpha) ? sqrtf(d2 * U2 + lower * lower) : d1 * U2 + lower;
+                    if (!(u01(rk.z) > sqrtf(x * x + x) / (x + 0.5f)) || k + 1 == kMaxPlasmonRounds) break;
+                }
+            }
+            se_E = x * omega + omega;
+            const uint4 r3 = draw(P.seed, e, 3);
+            sdir = make_unit_vec(2 * u01(r3.x) - 1, u01(r3.y));
+        } else if (q < k_fermi_omega + k_fermi) {
+            // single excitation from the annulus of allowed initial k around q
+            const float ki_parr = (omega - q * q) / (2 * q);
+            const float kf_parr = ki_parr + q;
+            const float ki_perp_min_sq = max_ref(0, m.fermi - kf_parr * kf_parr);
+            const float ki_perp_max_sq = m.fermi - ki_parr * ki_parr;
+            const float ki_perp_sq = max_ref(0, ki_perp_min_sq + (ki_perp_max_sq - ki_perp_min_sq) * u01(r1.w));
+            const float kp = sqrtf(ki_perp_sq);
+            const V3 ki{ki_parr * q_dir.x + kp * q_normal.x, ki_parr * q_dir.y + kp * q_normal.y,
+                        ki_parr * q_dir.z + kp * q_normal.z};
+            se_E = (ki.x * ki.x + ki.y * ki.y + ki.z * ki.z) + omega;
+            sdir = V3{ki.x + q * q_dir.x, ki.y + q * q_dir.y, ki.z + q * q_dir.z};
+        } else {
+            return false;   // q too large for either: no secondary
+        }
+    } else {
+        // inner-shell excitation (Ivanchenko angles, as kieft_inelastic)
+        const float Kp = K - m.fermi + 2 * binding;
+        const float dK = binding + omega;
+        const float cos_theta = sqrtf(dK / Kp);
+        const float sin_theta = sqrtf(1 - clampr(cos_theta * cos_theta, 0, 1));
+        V3 s{d.x * cos_theta + n.x * sin_theta, d.y * cos_theta + n.y * sin_theta, d.z * cos_theta + n.z * sin_theta};
+        s = normalised(s);
+        const uint4 r3 = draw(P.seed, e, 3);
+        const V3 uv = make_unit_vec(2 * u01(r3.x) - 1, u01(r3.y));
+        const float a = sqrtf(binding / dK);
+        s.x += a * uv.x;
+        s.y += a * uv.y;
+        s.z += a * uv.z;
+        s = normalised(s);
+        se_E = m.fermi + omega - binding;
+        sdir = s;
+        e.E = K - omega;
+        e.dx = d.x - cos_theta * s.x;
+        e.dy = d.y - cos_theta * s.y;
+        e.dz = d.z - cos_theta * s.z;
+    }
+    se->px = e.px;
+    se->py = e.py;
+    se->pz = e.pz;
+    se->dx = sdir.x;
+    se->dy = sdir.y;
+    se->dz = sdir.z;
+    se->E = se_E;
+    se->mat = e.mat;
+    se->last_tri = -1;
+    se->tag = e.tag;
+    se->uid = secondary_uid(e.uid, e.step);
+    se->step = 0;
+    return true;
+}
+
 // boundary_intersect<quantum transmission, refraction, no absorption>::execute
 // (physics/boundary_intersect.h:40-156)
 __device__ __forceinline__ int boundary(const Physics& P, Electron& e, float u) {
@@ -571,7 +724,10 @@ __device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, E
                 *event = kEvElastic;
             } else {
                 const uint4 r1 = draw(P.seed, e, 1);
-                *has_se = inelastic_finish(m, e, tv, nd, n, u01(r1.x), u01(r1.y), u01(r1.z), u01(r1.w), se);
+                if (P.penn)
+                    *has_se = penn_finish(P, m, e, tv, logE, nd, n, r1, se);
+                else
+                    *has_se = inelastic_finish(m, e, tv, nd, n, u01(r1.x), u01(r1.y), u01(r1.z), u01(r1.w), se);
                 *event = kEvInelastic;
             }
         }

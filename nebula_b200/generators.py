@@ -117,14 +117,15 @@ MATERIALS = {
 }
 
 
-def make_material(path, kind="si", nK=128, nP=256, Kmin=1.0, Kmax=1.0e4, seed=0):
+def make_material(path, kind="si", nK=128, nP=256, Kmin=1.0, Kmax=1.0e4, seed=0, penn=True, nW=32, nPq=32):
     """Write a synthetic ``.mat`` file for one of ``MATERIALS``.
 
     The energy axis is written as the exact ``geomspace`` values the reader
     reconstructs, so the logarithmic-spacing check of
     ``source/io/hdf5_file.cpp:345-351`` passes.  ``seed`` is recorded in the
     file; the tables themselves are deterministic functions of the model
-    parameters."""
+    parameters.  With ``penn`` the file also carries the full Penn groups,
+    so the same file serves both inelastic models."""
     Z, n_at, A, wp, gam, fermi, wf, gap, phonon, dens = MATERIALS[kind]
     K = _geomspace(Kmin, Kmax, nK)
     P = _linspace(0.0, 1.0, nP)
@@ -175,8 +176,69 @@ def make_material(path, kind="si", nK=128, nP=256, Kmin=1.0, Kmax=1.0e4, seed=0)
     d.attach_scale(1, p_io)
     g.dataset("outer_shells", np.array([100.0, 149.7, 1839.0]), units="eV")
 
+    if penn:
+        _write_penn(m, K, P, imfp_in, w0, nW=nW, nPq=nPq)
+
     m.write(path)
     return path
+
+
+def q_icdf_table(K, W, Pq):
+    """Momentum-transfer inverse CDF (nm^-1) on (K, omega/K, P).
+
+    Between the kinematic limits q-/+ = sqrt(K) -/+ sqrt(K - omega) (in
+    units of sqrt(eV), hbar^2 / 2m = 1) the density is taken as 1/q (dipole
+    form), floored at 1e-3 sqrt(K); the result is stored in nm^-1 as the
+    reference's loader expects (it multiplies by hbar / sqrt(2m) =
+    0.19519 nm eV^1/2)."""
+    out = np.zeros((len(K), len(W), len(Pq)))
+    for i, k in enumerate(K):
+        for j, w in enumerate(W):
+            om = min(w, 1.0) * k
+            q_hi = math.sqrt(k) + math.sqrt(max(k - om, 0.0))
+            q_lo = max(math.sqrt(k) - math.sqrt(max(k - om, 0.0)), 1e-3 * math.sqrt(k))
+            q_lo = min(q_lo, q_hi)
+            out[i, j] = q_lo * (q_hi / q_lo) ** Pq / 0.19519
+    return out
+
+
+def _write_penn(m, K, P, imfp_in, omega_icdf, nW=32, nPq=32, nO=32):
+    """Full Penn groups (source/physics/full_penn.h:296-392): /full_penn/imfp
+    and /full_penn/omega_icdf from the same dielectric model as the Kieft
+    tables, /full_penn/q_icdf on (K, omega/K, P), and the 3-D
+    /ionization/binding_icdf on (K, omega/K log-spaced, P) with one inner
+    shell (99.8 eV) above 10 % of the omega-cumulative range."""
+    g = m.group("/full_penn")
+    k_p = g.dataset("energy", K, units="eV")
+    p_p = g.dataset("probability", P, units="")
+    d = g.dataset("imfp", imfp_in.astype(np.float32), units="nm^-1")
+    d.attach_scale(0, k_p)
+    d = g.dataset("omega_icdf", omega_icdf.astype(np.float32), units="eV")
+    d.attach_scale(0, k_p)
+    d.attach_scale(1, p_p)
+    W = _linspace(0.0, 1.0, nW)
+    Pq = _linspace(0.0, 1.0, nPq)
+    w_q = g.dataset("omega_fraction", W, units="")
+    p_q = g.dataset("q_probability", Pq, units="")
+    d = g.dataset("q_icdf", q_icdf_table(K, W, Pq).astype(np.float32), units="nm^-1")
+    d.attach_scale(0, k_p)
+    d.attach_scale(1, w_q)
+    d.attach_scale(2, p_q)
+
+    g = m.group("/ionization")
+    k_i = g.dataset("energy", K, units="eV")
+    O = _geomspace(1e-4, 1.0, nO)
+    Pb = _linspace(0.0, 1.0, nPq)
+    o_i = g.dataset("omega_fraction", O, units="")
+    p_i = g.dataset("probability", Pb, units="")
+    binding = np.full((len(K), nO, nPq), 5.0, np.float32)          # valence (< 50 eV)
+    omega = K[:, None] * O[None, :]
+    shell = (omega >= 99.8)[:, :, None] & (Pb >= 0.9)[None, None, :]
+    binding[shell] = 99.8
+    d = g.dataset("binding_icdf", binding, units="eV")
+    d.attach_scale(0, k_i)
+    d.attach_scale(1, o_i)
+    d.attach_scale(2, p_i)
 
 
 # ----------------------------------------------------------------------------

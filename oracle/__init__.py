@@ -5,7 +5,9 @@ Two CPU implementations the CUDA kernels are compared against:
 * ``ref``  -- the reference's own CPU code compiled from its source tree by
   ``oracle/Makefile`` into ``oracle/_ref/libnbref.so`` (octree builder,
   ``octree<false>::propagate``, Kieft material loaders and table lookups, and
-  a cpu_mt_main-style multi-threaded run).
+  a cpu_mt_main-style multi-threaded run) and, on the reference's stock
+  physics configuration (full Penn inelastic model), into
+  ``oracle/_ref/libnbref_penn.so``.
 * ``port`` -- the plain-C restatement ``oracle/nbx_oracle.c``
   (``oracle/libnbx_oracle.so``), which shares the product's per-electron
   Philox random-number scheme so single events can be compared directly.
@@ -22,14 +24,16 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "libnbref.so")
+REF_PENN_SO = os.path.join(HERE, "_ref", "libnbref_penn.so")
 PORT_SO = os.path.join(HERE, "libnbx_oracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "nebula_cpu_mt_kieft")
+REF_BIN_PENN = os.path.join(HERE, "_ref", "nebula_cpu_mt")
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 
-_ref = None
+_ref = {}
 _port = None
 
 
@@ -41,14 +45,15 @@ def build(reference_dir="/root/reference/source"):
         subprocess.run(["make", "-s", "-C", HERE, "ref", "REF=" + reference_dir], check=True)
 
 
-def have_ref():
-    return os.path.exists(REF_SO)
+def have_ref(penn=False):
+    return os.path.exists(REF_PENN_SO if penn else REF_SO)
 
 
-def ref():
-    global _ref
-    if _ref is None:
-        lib = C.CDLL(REF_SO)
+def ref(penn=False):
+    """The compiled reference: Kieft inelastic model, or with ``penn`` the
+    stock full Penn model."""
+    if penn not in _ref:
+        lib = C.CDLL(REF_PENN_SO if penn else REF_SO)
         lib.nbref_build_octree.restype = C.c_int
         lib.nbref_build_octree.argtypes = [_f32p, _i32p, C.c_int64, C.POINTER(C.POINTER(C.c_int32)),
                                            C.POINTER(C.c_int64), C.POINTER(C.POINTER(C.c_float)),
@@ -67,13 +72,17 @@ def ref():
         lib.nbref_material_info.argtypes = [C.c_void_p, _f32p]
         lib.nbref_material_eval.argtypes = [C.c_void_p, C.c_int, _f32p, _f32p, C.c_int64, _f32p]
         lib.nbref_material_table.argtypes = [C.c_void_p, C.c_int, C.c_void_p, _i32p, _f32p]
+        lib.nbref_material_eval3.restype = C.c_int
+        lib.nbref_material_eval3.argtypes = [C.c_void_p, C.c_int, _f32p, _f32p, _f32p, C.c_int64, _f32p]
+        lib.nbref_material_table3.restype = C.c_int
+        lib.nbref_material_table3.argtypes = [C.c_void_p, C.c_int, C.c_void_p, _i32p, _f32p]
         lib.nbref_run.restype = C.c_int
         lib.nbref_run.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(C.c_char_p), C.c_int, C.c_uint32, C.c_float,
                                   C.c_int, C.c_int, C.c_int64, C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
                                   np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS"),
                                   C.POINTER(C.c_double)]
-        _ref = lib
-    return _ref
+        _ref[penn] = lib
+    return _ref[penn]
 
 
 def port():
@@ -128,10 +137,16 @@ class Table2D(C.Structure):
                 ("y_min", C.c_float), ("y_step", C.c_float), ("data", C.c_void_p)]
 
 
+class Table3D(C.Structure):
+    _fields_ = [("w", C.c_int), ("h", C.c_int), ("d", C.c_int), ("x_min", C.c_float), ("x_step", C.c_float),
+                ("y_min", C.c_float), ("y_step", C.c_float), ("z_min", C.c_float), ("z_step", C.c_float),
+                ("data", C.c_void_p)]
+
+
 class Material(C.Structure):
     _fields_ = [("barrier", C.c_float), ("el_imfp", Table1D), ("el_icdf", Table2D), ("phonon_loss", C.c_float),
                 ("recoil_const", C.c_float), ("in_imfp", Table1D), ("in_icdf", Table2D), ("ion", Table2D),
-                ("fermi", C.c_float), ("band_gap", C.c_float)]
+                ("fermi", C.c_float), ("band_gap", C.c_float), ("q", Table3D), ("ion3", Table3D)]
 
 
 class Electron(C.Structure):
@@ -140,7 +155,7 @@ class Electron(C.Structure):
 
 
 class Params(C.Structure):
-    _fields_ = [("seed", C.c_uint32), ("min_energy", C.c_float), ("max_energy", C.c_float)]
+    _fields_ = [("seed", C.c_uint32), ("min_energy", C.c_float), ("max_energy", C.c_float), ("penn", C.c_int)]
 
 
 class Counts(C.Structure):
@@ -210,12 +225,17 @@ class RefGeometry:
 
 
 class RefMaterial:
-    """A .mat file loaded by the reference's own Kieft loaders."""
+    """A .mat file loaded by the reference's own loaders: Kieft elastic with
+    the Kieft inelastic model, or with ``penn`` the full Penn model (whose
+    ``in_imfp`` / ``in_icdf`` are the Penn log-IMFP and log-omega ICDF, and
+    whose 3-D tables are read with ``table3`` / ``eval3``)."""
 
     TABLES = {"el_imfp": 0, "el_icdf": 1, "in_imfp": 2, "in_icdf": 3, "ion": 4}
+    TABLES3 = {"q": 0, "ion3": 1}
 
-    def __init__(self, path):
-        self.lib = ref()
+    def __init__(self, path, penn=False):
+        self.penn = penn
+        self.lib = ref(penn)
         self.h = self.lib.nbref_material_load(str(path).encode())
         if not self.h:
             raise RuntimeError("reference material load failed: %s" % path)
@@ -242,6 +262,25 @@ class RefMaterial:
         vals = out.reshape(int(dims[0]), int(dims[1])) if which not in ("el_imfp", "in_imfp") else out
         return vals, tuple(float(v) for v in sc)
 
+    def eval3(self, which, x, y, z):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        z = np.ascontiguousarray(z, np.float32)
+        out = np.zeros_like(x)
+        if self.lib.nbref_material_eval3(self.h, self.TABLES3[which], x, y, z, len(x), out) != 0:
+            raise RuntimeError("3-D tables exist only in the full Penn build")
+        return out
+
+    def table3(self, which):
+        """(values[w][h][d], (x_min, x_step, y_min, y_step, z_min, z_step))."""
+        dims = np.zeros(3, np.int32)
+        sc = np.zeros(6, np.float32)
+        if self.lib.nbref_material_table3(self.h, self.TABLES3[which], None, dims, sc) != 0:
+            raise RuntimeError("3-D tables exist only in the full Penn build")
+        out = np.zeros(int(np.prod(dims.astype(np.int64))), np.float32)
+        self.lib.nbref_material_table3(self.h, self.TABLES3[which], out.ctypes.data, dims, sc)
+        return out.reshape(tuple(int(d) for d in dims)), tuple(float(v) for v in sc)
+
     def __del__(self):
         if getattr(self, "h", None):
             self.lib.nbref_material_destroy(self.h)
@@ -249,11 +288,12 @@ class RefMaterial:
 
 
 def ref_run(tri_path, pri_path, mat_paths, seed=0x78C7E39B, energy_threshold=0.0, threads=0, count_events=False,
-            max_primaries=-1):
-    """cpu_mt_main-style run of the reference CPU path.  Returns
-    (records[RECORD_DTYPE], stats dict, seconds)."""
+            max_primaries=-1, penn=False):
+    """cpu_mt_main-style run of the reference CPU path (Kieft build, or the
+    stock full Penn build with ``penn``).  Returns (records[RECORD_DTYPE],
+    stats dict, seconds)."""
     from nebula_b200 import formats
-    lib = ref()
+    lib = ref(penn)
     arr = (C.c_char_p * len(mat_paths))(*[str(p).encode() for p in mat_paths])
     recs = C.c_void_p()
     nrec = C.c_int64()
@@ -314,13 +354,24 @@ class PortMaterial:
             a = np.ascontiguousarray(a, np.float32)
             self.arrays[name] = a
             t[name] = Table1D(len(a), xm, xs, a.ctypes.data)
-        for name in ("el_icdf", "in_icdf", "ion"):
+        for name in ("el_icdf", "in_icdf") + (() if ref_mat.penn else ("ion",)):
             a, (xm, xs, ym, ys) = ref_mat.table(name)
             a = np.ascontiguousarray(a, np.float32)
             self.arrays[name] = a
             t[name] = Table2D(a.shape[0], a.shape[1], xm, xs, ym, ys, a.ctypes.data)
+        if ref_mat.penn:
+            # full Penn build: in_imfp / in_icdf above are the Penn tables
+            t["ion"] = Table2D()
+            for name in ("q", "ion3"):
+                a, (xm, xs, ym, ys, zm, zs) = ref_mat.table3(name)
+                a = np.ascontiguousarray(a, np.float32)
+                self.arrays[name] = a
+                t[name] = Table3D(a.shape[0], a.shape[1], a.shape[2], xm, xs, ym, ys, zm, zs, a.ctypes.data)
+        else:
+            t["q"] = Table3D()
+            t["ion3"] = Table3D()
         self.s = Material(ref_mat.barrier, t["el_imfp"], t["el_icdf"], ref_mat.phonon_loss, ref_mat.recoil_const,
-                          t["in_imfp"], t["in_icdf"], t["ion"], ref_mat.fermi, ref_mat.band_gap)
+                          t["in_imfp"], t["in_icdf"], t["ion"], ref_mat.fermi, ref_mat.band_gap, t["q"], t["ion3"])
 
 
 def port_materials(ref_mats):
@@ -337,12 +388,12 @@ def philox(ctr, key):
 
 
 def port_run(pg: "PortGeometry", mats_arr, primaries_7f, tags, seed, max_energy, min_energy=0.0,
-             uid_base=0, records_cap=0, per_primary=True):
+             uid_base=0, records_cap=0, per_primary=True, penn=False):
     """Run the C restatement; returns (counts dict, se_count, bse_count, records, geom_counters)."""
     from nebula_b200 import formats
     P = port()
     n = len(tags)
-    prm = Params(seed, min_energy, max_energy)
+    prm = Params(seed, min_energy, max_energy, 1 if penn else 0)
     se = np.zeros(n, np.uint32) if per_primary else None
     bse = np.zeros(n, np.uint32) if per_primary else None
     recs = np.zeros(max(records_cap, 1), formats.RECORD_DTYPE)

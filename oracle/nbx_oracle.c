@@ -281,6 +281,43 @@ float nbo_table2d_get_rounddown(const nbo_table2d* t, float x, float y) {
     return t->data[(size_t)lx * t->h + ly];
 }
 
+/* table_3D::get / get_rounddown (common/util/table_3D.inl:79-122) */
+static float t3at(const nbo_table3d* t, int i, int j, int k) { return t->data[((size_t)i * t->h + j) * t->d + k]; }
+
+float nbo_table3d_get(const nbo_table3d* t, float x, float y, float z) {
+    const float x_index = (x - t->x_min) * t->x_step;
+    const float y_index = (y - t->y_min) * t->y_step;
+    const float z_index = (z - t->z_min) * t->z_step;
+    const int low_x = clampi_ref((int)floorf(x_index), 0, t->w - 2);
+    const int low_y = clampi_ref((int)floorf(y_index), 0, t->h - 2);
+    const int low_z = clampi_ref((int)floorf(z_index), 0, t->d - 2);
+    const float v000 = t3at(t, low_x, low_y, low_z);
+    const float v100 = t3at(t, low_x + 1, low_y, low_z);
+    const float v010 = t3at(t, low_x, low_y + 1, low_z);
+    const float v110 = t3at(t, low_x + 1, low_y + 1, low_z);
+    const float v001 = t3at(t, low_x, low_y, low_z + 1);
+    const float v101 = t3at(t, low_x + 1, low_y, low_z + 1);
+    const float v011 = t3at(t, low_x, low_y + 1, low_z + 1);
+    const float v111 = t3at(t, low_x + 1, low_y + 1, low_z + 1);
+    const float frac_x = x_index - (float)low_x;
+    const float frac_y = y_index - (float)low_y;
+    const float frac_z = z_index - (float)low_z;
+    return (1 - frac_x) * (1 - frac_y) * (1 - frac_z) * v000 + frac_x * (1 - frac_y) * (1 - frac_z) * v100 +
+           (1 - frac_x) * frac_y * (1 - frac_z) * v010 + frac_x * frac_y * (1 - frac_z) * v110 +
+           (1 - frac_x) * (1 - frac_y) * frac_z * v001 + frac_x * (1 - frac_y) * frac_z * v101 +
+           (1 - frac_x) * frac_y * frac_z * v011 + frac_x * frac_y * frac_z * v111;
+}
+
+float nbo_table3d_get_rounddown(const nbo_table3d* t, float x, float y, float z) {
+    const float x_index = (x - t->x_min) * t->x_step;
+    const float y_index = (y - t->y_min) * t->y_step;
+    const float z_index = (z - t->z_min) * t->z_step;
+    const int low_x = clampi_ref((int)floorf(x_index), 0, t->w - 1);
+    const int low_y = clampi_ref((int)floorf(y_index), 0, t->h - 1);
+    const int low_z = clampi_ref((int)floorf(z_index), 0, t->d - 1);
+    return t3at(t, low_x, low_y, low_z);
+}
+
 /* ---------------------------------------------------------------------------
  * Physics
  * ------------------------------------------------------------------------- */
@@ -365,6 +402,126 @@ int nbo_inelastic(const nbo_material* m, nbo_electron* e, const float u[6], nbo_
 
     e->E -= omega;
     for (int i = 0; i < 3; ++i) e->dir[i] -= cos_theta * sd[i];
+    return 1;
+}
+
+static void philox_block(const nbo_params* p, const nbo_electron* e, uint32_t block, uint32_t out[4]) {
+    const uint32_t key[2] = {p->seed, 0u};
+    const uint32_t c[4] = {e->step, block, (uint32_t)e->uid, (uint32_t)(e->uid >> 32)};
+    nbo_philox4x32_10(c, key, out);
+}
+
+/* full_penn<cpu, true>::execute (physics/full_penn.h:63-289).  Uniform slots
+ * (shared with the GPU): omega ICDF <- block 0 z (done by the caller),
+ * primary normal azimuth <- block 0 w (u_phi), binding <- block 1 x, q <-
+ * block 1 y, q-normal azimuth <- block 1 z, single-excitation radius or the
+ * f < 0.1 plasmon draw <- block 1 w, secondary uniform_vector <- block 3 x, y,
+ * plasmon rejection round k <- block 4 + k (x, y, z), at most 64 rounds. */
+int nbo_penn_inelastic(const nbo_material* m, const nbo_params* p, nbo_electron* e, float log_omega, float u_phi,
+                       const uint32_t r1[4], nbo_electron* se) {
+    const float K = e->E;
+    const float omega = expf(log_omega);
+    const float binding = nbo_table3d_get_rounddown(&m->ion3, logf(K), logf(omega / K), nbo_u01(r1[0]));
+    normalise3(e->dir);
+    float sdir[3];
+    float se_E;
+    if (binding <= 0) {
+        if (!(omega > m->band_gap)) {
+            e->E -= omega; /* sub-band-gap loss: energy only */
+            return 0;
+        }
+        const float q = nbo_table3d_get(&m->q, logf(K), omega / K, nbo_u01(r1[1]));
+        float prim_normal[3];
+        make_normal_vec(e->dir, (2 * NBO_PI) * u_phi, prim_normal);
+        normalise3(prim_normal);
+        float q_dir[3], q_normal[3];
+        {
+            const float c = clampf_ref((omega + q * q) / (2 * sqrtf(K) * q), -1, 1);
+            const float sn = sqrtf(1 - c * c);
+            for (int i = 0; i < 3; ++i) q_dir[i] = e->dir[i] * c + prim_normal[i] * sn;
+            normalise3(q_dir);
+            make_normal_vec(q_dir, (2 * NBO_PI) * nbo_u01(r1[2]), q_normal);
+            normalise3(q_normal);
+        }
+        const float c2 = clampf_ref((2 * K - omega - q * q) / (2 * sqrtf(K * (K - omega))), -1, 1);
+        const float s2 = sqrtf(1 - c2 * c2);
+        e->E -= omega;
+        for (int i = 0; i < 3; ++i) e->dir[i] = e->dir[i] * c2 + prim_normal[i] * s2;
+        const float k_fermi = sqrtf(m->fermi);
+        const float k_fermi_omega = sqrtf(m->fermi + omega);
+        if (q < k_fermi_omega - k_fermi) {
+            /* plasmon decay */
+            const float f = m->fermi / omega;
+            float x;
+            if (f < 0.1f) {
+                const float U = cbrtf(nbo_u01(r1[3]));
+                x = f * U * U;
+            } else {
+                const float lower = maxf_ref(0, f - 1);
+                const float upper = f;
+                const float d1 = upper - lower;
+                const float d2 = upper * upper - lower * lower;
+                const float alpha = d2 / (d1 + d2);
+                for (uint32_t k = 0;; ++k) {
+                    uint32_t rk[4];
+                    philox_block(p, e, 4 + k, rk);
+                    const float U1 = nbo_u01(rk[0]);
+                    const float U2 = nbo_u01(rk[1]);
+                    x = (U1 < alpha) ? sqrtf(d2 * U2 + lower * lower) : d1 * U2 + lower;
+                    if (!(nbo_u01(rk[2]) > sqrtf(x * x + x) / (x + 0.5f)) || k + 1 == 64) break;
+                }
+            }
+            se_E = x * omega + omega;
+            uint32_t r3[4];
+            philox_block(p, e, 3, r3);
+            make_unit_vec(2 * nbo_u01(r3[0]) - 1, (2 * NBO_PI) * nbo_u01(r3[1]), sdir);
+        } else if (q < k_fermi_omega + k_fermi) {
+            /* single excitation */
+            const float ki_parr = (omega - q * q) / (2 * q);
+            const float kf_parr = ki_parr + q;
+            const float ki_perp_min_sq = maxf_ref(0, m->fermi - kf_parr * kf_parr);
+            const float ki_perp_max_sq = m->fermi - ki_parr * ki_parr;
+            const float ki_perp_sq =
+                maxf_ref(0, ki_perp_min_sq + (ki_perp_max_sq - ki_perp_min_sq) * nbo_u01(r1[3]));
+            float ki[3];
+            for (int i = 0; i < 3; ++i) ki[i] = ki_parr * q_dir[i] + sqrtf(ki_perp_sq) * q_normal[i];
+            se_E = (ki[0] * ki[0] + ki[1] * ki[1] + ki[2] * ki[2]) + omega;
+            for (int i = 0; i < 3; ++i) sdir[i] = ki[i] + q * q_dir[i];
+        } else {
+            return 0;
+        }
+    } else {
+        /* inner-shell excitation */
+        float nd[3];
+        make_normal_vec(e->dir, (2 * NBO_PI) * u_phi, nd);
+        normalise3(nd);
+        const float _K = K - m->fermi + 2 * binding;
+        const float dK = binding + omega;
+        const float cos_theta = sqrtf(dK / _K);
+        const float sin_theta = sqrtf(1 - clampf_ref(cos_theta * cos_theta, 0, 1));
+        for (int i = 0; i < 3; ++i) sdir[i] = e->dir[i] * cos_theta + nd[i] * sin_theta;
+        normalise3(sdir);
+        {
+            uint32_t r3[4];
+            philox_block(p, e, 3, r3);
+            float uv[3];
+            make_unit_vec(2 * nbo_u01(r3[0]) - 1, (2 * NBO_PI) * nbo_u01(r3[1]), uv);
+            const float a = sqrtf(binding / dK);
+            for (int i = 0; i < 3; ++i) sdir[i] += a * uv[i];
+        }
+        normalise3(sdir);
+        se_E = m->fermi + omega - binding;
+        e->E -= omega;
+        for (int i = 0; i < 3; ++i) e->dir[i] -= cos_theta * sdir[i];
+    }
+    se->E = se_E;
+    memcpy(se->pos, e->pos, sizeof se->pos);
+    memcpy(se->dir, sdir, sizeof se->dir);
+    se->mat = e->mat;
+    se->last_tri = -1;
+    se->tag = e->tag;
+    se->uid = nbo_secondary_uid(e->uid, e->step);
+    se->step = 0;
     return 1;
 }
 
@@ -483,11 +640,19 @@ int nbo_step(const nbo_geometry* g, const nbo_material* mats, const nbo_params* 
             uint32_t r1c[4] = {e->step, 1u, (uint32_t)e->uid, (uint32_t)(e->uid >> 32)};
             const uint32_t key[2] = {p->seed, 0u};
             nbo_philox4x32_10(r1c, key, r1);
-            /* slots: omega' ICDF <- block 0 z, binding <- block 1 x, energy loss
-             * <- block 1 y, azimuth <- block 0 w, unit vector <- block 1 z, w */
-            const float u[6] = {nbo_u01(r0[2]), nbo_u01(r1[0]), nbo_u01(r1[1]),
-                                nbo_u01(r0[3]), nbo_u01(r1[2]), nbo_u01(r1[3])};
-            *has_se = nbo_inelastic(&mats[e->mat], e, u, se);
+            if (p->penn) {
+                /* full_penn: log omega ICDF <- block 0 z, the rest as listed
+                 * at nbo_penn_inelastic */
+                const float log_omega = nbo_table2d_get(&mats[e->mat].in_icdf, logf(e->E), nbo_u01(r0[2]));
+                *has_se = nbo_penn_inelastic(&mats[e->mat], p, e, log_omega, nbo_u01(r0[3]), r1, se);
+            } else {
+                /* slots: omega' ICDF <- block 0 z, binding <- block 1 x, energy
+                 * loss <- block 1 y, azimuth <- block 0 w, unit vector <- block
+                 * 1 z, w */
+                const float u[6] = {nbo_u01(r0[2]), nbo_u01(r1[0]), nbo_u01(r1[1]),
+                                    nbo_u01(r0[3]), nbo_u01(r1[2]), nbo_u01(r1[3])};
+                *has_se = nbo_inelastic(&mats[e->mat], e, u, se);
+            }
             *event = NBO_EV_INELASTIC;
         }
     } else {

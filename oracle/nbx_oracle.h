@@ -48,6 +48,15 @@ typedef struct {
 } nbo_table2d;
 
 typedef struct {
+    int w, h, d;
+    float x_min, x_step, y_min, y_step, z_min, z_step;
+    const float* data; /* data[(x * h + y) * d + z] */
+} nbo_table3d;
+
+/* in_imfp / in_icdf: the inelastic model's log-IMFP and log-energy-loss ICDF
+ * (Kieft omega', full Penn omega); ion: Kieft's 2-D ionisation table;
+ * q / ion3: full Penn's 3-D tables. */
+typedef struct {
     float barrier;
     nbo_table1d el_imfp;
     nbo_table2d el_icdf;
@@ -56,6 +65,7 @@ typedef struct {
     nbo_table2d in_icdf;
     nbo_table2d ion;
     float fermi, band_gap;
+    nbo_table3d q, ion3;
 } nbo_material;
 
 typedef struct {
@@ -91,6 +101,8 @@ void nbo_geom_counters_reset(void);
 float nbo_table1d_get(const nbo_table1d* t, float x);
 float nbo_table2d_get(const nbo_table2d* t, float x, float y);
 float nbo_table2d_get_rounddown(const nbo_table2d* t, float x, float y);
+float nbo_table3d_get(const nbo_table3d* t, float x, float y, float z);
+float nbo_table3d_get_rounddown(const nbo_table3d* t, float x, float y, float z);
 
 /* Events, with their uniforms given explicitly. */
 void nbo_elastic(const nbo_material* m, nbo_electron* e, float u_cos, float u_phi);
@@ -102,7 +114,14 @@ int nbo_boundary(const nbo_geometry* g, const nbo_material* mats, nbo_electron* 
 typedef struct {
     uint32_t seed;
     float min_energy, max_energy;
+    int penn; /* inelastic model: 0 Kieft & Bosch, 1 full Penn */
 } nbo_params;
+
+/* full_penn::execute (physics/full_penn.h:63-289) after the log-omega ICDF
+ * lookup; r1 = Philox block 1 of this step, further uniforms from blocks 3
+ * and 4, 5, ... of the electron's stream (same slots as the GPU). */
+int nbo_penn_inelastic(const nbo_material* m, const nbo_params* p, nbo_electron* e, float log_omega, float u_phi,
+                       const uint32_t r1[4], nbo_electron* se);
 
 /* One pass of init -> intersect -> scatter for one electron
  * (source/drivers/cpu/cpu_driver.inl:73-161).  Returns the status; *event

@@ -4,8 +4,14 @@
 //
 //   nbref_build_octree   octree_builder::linearized_octree (octree_builder.cpp:252-352)
 //   nbref_propagate      octree<false>::propagate (geometry/octree.inl:33-192)
-//   nbref_material_*     material<scatter_list<kieft_inelastic, kieft_elastic>>::create
-//                        and the reference table lookups (table_1D.inl:66, table_2D.inl:74,97)
+//   nbref_material_*     material<scatter_list<inelastic, kieft_elastic>>::create
+//                        and the reference table lookups (table_1D.inl:66, table_2D.inl:74,97,
+//                        table_3D.inl:79,114)
+//
+// Built twice: with the Kieft inelastic model (kieft_physics_config.h, the
+// commented block of physics_config.h:27-33) as libnbref.so, and with
+// -DNBREF_PENN against the reference's own physics_config.h (full Penn, the
+// stock build) as libnbref_penn.so.
 //   nbref_run            cpu_mt_main.cpp:158-203 (one simple_cpu_driver per thread pulling
 //                        one primary at a time), optionally counting events
 #include <atomic>
@@ -17,7 +23,12 @@
 #include <thread>
 #include <vector>
 
+#ifdef NBREF_PENN
+#include "config/config.h"   // as cpu_mt_main.cpp includes it before physics_config.h
+#include "physics_config.h"
+#else
 #include "kieft_physics_config.h"
+#endif
 #include "common/work_pool.h"
 #include "drivers/cpu/simple_cpu_driver.h"
 #include "geometry/octree.h"
@@ -27,7 +38,11 @@
 using geometry_t = nbl::geometry::octree<false>;
 using material_t = material<scatter_physics<false>>;
 using elastic_t = nbl::scatter::kieft_elastic<false, true, true>;
+#ifdef NBREF_PENN
+using inelastic_t = nbl::scatter::full_penn<false, true>;
+#else
 using inelastic_t = nbl::scatter::kieft_inelastic<false, true, true, true, true>;
+#endif
 
 // The reference classes keep their tables private and befriend every
 // specialisation of their own template; these two explicit specialisations
@@ -41,6 +56,18 @@ public:
     static real phonon(elastic_t const& e) { return e._phonon_loss; }
     static real recoil(elastic_t const& e) { return e._recoil_const; }
 };
+#ifdef NBREF_PENN
+template<>
+class full_penn<true, false> {
+public:
+    static util::table_1D<real, false> const& imfp(inelastic_t const& e) { return e._log_imfp_table; }
+    static util::table_2D<real, false> const& icdf(inelastic_t const& e) { return e._log_omega_icdf_table; }
+    static util::table_3D<real, false> const& q(inelastic_t const& e) { return e._q_icdf_table; }
+    static util::table_3D<real, false> const& ion3(inelastic_t const& e) { return e._ionisation_table; }
+    static real fermi(inelastic_t const& e) { return e._fermi; }
+    static real gap(inelastic_t const& e) { return e._band_gap; }
+};
+#else
 template<>
 class kieft_inelastic<true, false, false, false, false> {
 public:
@@ -50,6 +77,7 @@ public:
     static real fermi(inelastic_t const& e) { return e._fermi; }
     static real gap(inelastic_t const& e) { return e._band_gap; }
 };
+#endif
 }}  // namespace nbl::scatter
 // The table classes befriend their other-device counterpart; these
 // specialisations (never instantiated on a device in this CPU build) read
@@ -69,9 +97,21 @@ public:
         out[0] = t._x_min; out[1] = t._x_step; out[2] = t._y_min; out[3] = t._y_step;
     }
 };
+template<>
+class table_3D<real, true> {
+public:
+    static void scales(table_3D<real, false> const& t, float out[6]) {
+        out[0] = t._x_min; out[1] = t._x_step; out[2] = t._y_min; out[3] = t._y_step;
+        out[4] = t._z_min; out[5] = t._z_step;
+    }
+};
 }}  // namespace nbl::util
 using el_spy = nbl::scatter::kieft_elastic<true, false, false>;
+#ifdef NBREF_PENN
+using in_spy = nbl::scatter::full_penn<true, false>;
+#else
 using in_spy = nbl::scatter::kieft_inelastic<true, false, false, false, false>;
+#endif
 
 namespace {
 // Byte-layout mirrors of two reference classes, read with memcpy.
@@ -245,7 +285,11 @@ void nbref_material_eval(void* m, int which, const float* x, const float* y, int
         case 1: out[i] = el_spy::icdf(el).get(x[i], y[i]); break;
         case 2: out[i] = in_spy::imfp(inel).get(x[i]); break;
         case 3: out[i] = in_spy::icdf(inel).get(x[i], y[i]); break;
+#ifdef NBREF_PENN
+        default: out[i] = 0; break;
+#else
         default: out[i] = in_spy::ion(inel).get_rounddown(x[i], y[i]); break;
+#endif
         }
     }
 }
@@ -265,7 +309,12 @@ int nbref_material_table(void* m, int which, float* out, int32_t dims[2], float 
             for (int i = 0; i < t.width(); ++i) out[i] = t(i);
         return 0;
     }
+#ifdef NBREF_PENN
+    if (which == 4) return -1;
+    auto const& t = which == 1 ? el_spy::icdf(el) : in_spy::icdf(inel);
+#else
     auto const& t = which == 1 ? el_spy::icdf(el) : which == 3 ? in_spy::icdf(inel) : in_spy::ion(inel);
+#endif
     dims[0] = t.width();
     dims[1] = t.height();
     nbl::util::table_2D<real, true>::scales(t, scales);
@@ -273,6 +322,43 @@ int nbref_material_table(void* m, int which, float* out, int32_t dims[2], float 
         for (int i = 0; i < t.width(); ++i)
             for (int j = 0; j < t.height(); ++j) out[size_t(i) * t.height() + j] = t(i, j);
     return 0;
+}
+
+// Full Penn 3-D tables (libnbref_penn.so only; the Kieft build returns -1):
+// which 0 = q ICDF (table_3D::get), 1 = ionisation (table_3D::get_rounddown).
+int nbref_material_eval3(void* m, int which, const float* x, const float* y, const float* z, int64_t n, float* out) {
+#ifdef NBREF_PENN
+    auto* mat = static_cast<material_t*>(m);
+    auto const& inel = nbl::tuple::get<0>(*mat);
+    for (int64_t i = 0; i < n; ++i)
+        out[i] = which == 0 ? in_spy::q(inel).get(x[i], y[i], z[i]) : in_spy::ion3(inel).get_rounddown(x[i], y[i], z[i]);
+    return 0;
+#else
+    (void)m; (void)which; (void)x; (void)y; (void)z; (void)n; (void)out;
+    return -1;
+#endif
+}
+
+// Full contents of a Penn 3-D table: data[(x * height + y) * depth + z] (out
+// may be null to query sizes) and {x_min, x_step, y_min, y_step, z_min, z_step}.
+int nbref_material_table3(void* m, int which, float* out, int32_t dims[3], float scales[6]) {
+#ifdef NBREF_PENN
+    auto* mat = static_cast<material_t*>(m);
+    auto const& inel = nbl::tuple::get<0>(*mat);
+    auto const& t = which == 0 ? in_spy::q(inel) : in_spy::ion3(inel);
+    dims[0] = t.width();
+    dims[1] = t.height();
+    dims[2] = t.depth();
+    nbl::util::table_3D<real, true>::scales(t, scales);
+    if (out)
+        for (int i = 0; i < t.width(); ++i)
+            for (int j = 0; j < t.height(); ++j)
+                for (int k = 0; k < t.depth(); ++k) out[(size_t(i) * t.height() + j) * t.depth() + k] = t(i, j, k);
+    return 0;
+#else
+    (void)m; (void)which; (void)out; (void)dims; (void)scales;
+    return -1;
+#endif
 }
 
 // cpu_mt_main-style run.  Writes detected 36-byte records (malloc'd) and

@@ -73,3 +73,30 @@ def test_stats_struct_matches_header():
     body = body[: body.index("} nbx_stats;")]
     fields = re.findall(r"^\s*(?:uint64_t|double)\s+(\w+);", body, flags=re.M)
     assert fields == [f for f, _ in nb.Stats._fields_]
+
+
+def _header_fields(text, first_line, closing):
+    body = text[text.index(first_line):]
+    body = re.sub(r"/\*.*?\*/", "", body[: body.index(closing)], flags=re.S)
+    names = []
+    for line in body.splitlines()[1:]:
+        line = line.strip()
+        if not line or line.startswith("typedef") or line.startswith("}"):
+            continue
+        decl = line.rstrip(";")
+        parts = decl.split(",")
+        names.append(parts[0].split()[-1].split("[")[0].lstrip("*"))
+        names += [p.strip().split("[")[0].lstrip("*") for p in parts[1:]]
+    return names
+
+
+def test_material_and_config_structs_match_header():
+    """The ctypes mirrors of nbx_material, nbx_table3d and nbx_config list
+    the header's fields in order (the full Penn fields are appended)."""
+    text = open(os.path.join(ROOT, "include", "nbx.h")).read()
+    mat = _header_fields(text, "typedef struct {\n    float barrier;", "} nbx_material;")
+    assert mat == [f for f, _ in nb.Material._fields_]
+    t3 = _header_fields(text, "typedef struct {\n    int32_t width, height, depth;", "} nbx_table3d;")
+    assert t3 == [f for f, _ in nb.Table3D._fields_]
+    cfg = _header_fields(text, "typedef struct {\n    int32_t device;", "} nbx_config;")
+    assert cfg == [f for f, _ in nb.Config._fields_]

@@ -70,3 +70,30 @@ def test_material_tables_identical(oracle_built, inputs, mat):
         assert np.array_equal(np.float32(sa), np.float32(sb)), name
     for k, v in zip(("barrier", "fermi", "band_gap", "phonon_loss", "recoil_const", "max_energy"), rm.info):
         assert np.float32(getattr(hm, k)) == np.float32(v), k
+
+
+@pytest.mark.parametrize("mat", ["si", "sio2", "w"])
+def test_penn_tables_identical(oracle_built, inputs, mat):
+    """Full Penn tables of the host loader against the stock reference build's
+    full_penn::create (physics/full_penn.h:296-392): bit-identical values and
+    axis parameters, including the 3-D q ICDF and ionisation tables."""
+    if not oracle_built.have_ref(penn=True):
+        pytest.skip("reference full Penn build unavailable")
+    rm = oracle_built.RefMaterial(inputs[mat], penn=True)
+    hm = nb.HostMaterial(inputs[mat])
+    assert hm.has_penn and hm.has_kieft_inelastic
+    for ref_name, host_name in (("in_imfp", "penn_imfp"), ("in_icdf", "penn_omega_icdf")):
+        a, sa = rm.table(ref_name)
+        b, sb = hm.tables[host_name]
+        assert a.shape == b.shape, host_name
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), host_name
+        assert np.array_equal(np.float32(sa), np.float32(sb)), host_name
+    for ref_name, host_name in (("q", "penn_q_icdf"), ("ion3", "penn_ion")):
+        a, sa = rm.table3(ref_name)
+        b, sb = hm.tables[host_name]
+        assert a.shape == b.shape, host_name
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), host_name
+        assert np.array_equal(np.float32(sa), np.float32(sb)), host_name
+    # the reference's max energy is the minimum over the stock mechanisms
+    assert np.float32(hm.penn_max_energy) == np.float32(rm.max_energy)
+    assert np.float32(hm.fermi) == np.float32(rm.fermi) and np.float32(hm.band_gap) == np.float32(rm.band_gap)

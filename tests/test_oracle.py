@@ -116,3 +116,74 @@ def test_whole_run_statistics(oracle_built, inputs, tmp_path):
     ev_o = (c["n_elastic"] + c["n_inelastic"] + c["n_boundary"]) / n
     ev_r = (st["n_intersect"] + st["n_elastic"] + st["n_inelastic"]) / n
     assert abs(ev_o - ev_r) / ev_r < 0.05
+
+
+def test_penn_tables_bit_exact(oracle_built, inputs):
+    """Full Penn tables: the restatement's 1-D/2-D/3-D lookups against the
+    stock reference build's table_1D/2D/3D get and get_rounddown, at random
+    points including extrapolation outside every axis."""
+    if not oracle_built.have_ref(penn=True):
+        pytest.skip("reference full Penn build unavailable")
+    rm = oracle_built.RefMaterial(inputs["si"], penn=True)
+    pm = oracle_built.PortMaterial(rm)
+    P = oracle_built.port()
+    P.nbo_table3d_get.restype = C.c_float
+    P.nbo_table3d_get.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float]
+    P.nbo_table3d_get_rounddown.restype = C.c_float
+    P.nbo_table3d_get_rounddown.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float]
+    rng = np.random.default_rng(5)
+    n = 4000
+    x = rng.uniform(-1.0, 10.5, n).astype(np.float32)
+    y = rng.uniform(-0.2, 1.2, n).astype(np.float32)
+    ylog = rng.uniform(-11.0, 0.5, n).astype(np.float32)
+    z = rng.uniform(-0.1, 1.1, n).astype(np.float32)
+    for name, fn, two in (("in_imfp", P.nbo_table1d_get, False), ("in_icdf", P.nbo_table2d_get, True)):
+        t = C.byref(getattr(pm.s, name))
+        got = np.array([fn(t, float(a), float(b)) if two else fn(t, float(a)) for a, b in zip(x, z)], np.float32)
+        assert np.array_equal(got.view(np.uint32), rm.eval(name, x, z).view(np.uint32)), name
+    tq = C.byref(pm.s.q)
+    got = np.array([P.nbo_table3d_get(tq, float(a), float(b), float(c)) for a, b, c in zip(x, y, z)], np.float32)
+    assert np.array_equal(got.view(np.uint32), rm.eval3("q", x, y, z).view(np.uint32))
+    ti = C.byref(pm.s.ion3)
+    got = np.array([P.nbo_table3d_get_rounddown(ti, float(a), float(b), float(c)) for a, b, c in zip(x, ylog, z)],
+                   np.float32)
+    ref = rm.eval3("ion3", x, ylog, z)
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+    assert set(np.unique(ref)) == {np.float32(-1.0), np.float32(99.8)}
+
+
+def test_penn_whole_run_statistics(oracle_built, inputs, tmp_path):
+    """Full Penn: the C restatement against the reference's stock build
+    (physics_config.h full_penn + kieft_elastic) on the cube at 1 keV:
+    SE/BSE yields within 3 sigma, spectra by chi-square, events within 5 %."""
+    if not oracle_built.have_ref(penn=True):
+        pytest.skip("reference full Penn build unavailable")
+    n = 20000
+    recs = g.point_beam(n, 1000.0, pos=(0.0, 0.0, 1.0))
+    recs["px"] = np.arange(n)
+    pri = str(tmp_path / "penn.pri")
+    formats.write_pri(pri, recs)
+    ref_recs, st, _ = oracle_built.ref_run(inputs["cube_tri"], pri, [inputs["si"]], seed=11, count_events=True,
+                                           penn=True)
+    pg = oracle_built.PortGeometry(inputs["cube"])
+    rm = oracle_built.RefMaterial(inputs["si"], penn=True)
+    pms, arr = oracle_built.port_materials([rm])
+    prim = np.zeros((n, 7), np.float32)
+    prim[:, 0:3] = recs["pos"]
+    prim[:, 3:6] = recs["dir"]
+    prim[:, 6] = recs["E"]
+    c, se, bse, orecs, _ = oracle_built.port_run(pg, arr, prim, np.arange(n, dtype=np.uint32), 13,
+                                                 max_energy=rm.max_energy, records_cap=200000, penn=True)
+    # per-primary reference counts from the pixel column (one pixel per primary)
+    px = ref_recs["px"].astype(np.int64)
+    se_r = np.bincount(px[ref_recs["E"] < 50], minlength=n).astype(float)
+    bse_r = np.bincount(px[ref_recs["E"] >= 50], minlength=n).astype(float)
+    for mine, ref in ((se.astype(float), se_r), (bse.astype(float), bse_r)):
+        zv = (mine.mean() - ref.mean()) / np.sqrt(mine.var() / n + ref.var() / n)
+        assert abs(zv) < 3, zv
+    bins = np.concatenate([np.arange(0, 50, 2.0), np.arange(50, 1001, 50.0)])
+    chi2, dof = _chi2(np.histogram(orecs["E"], bins)[0].astype(float), np.histogram(ref_recs["E"], bins)[0].astype(float))
+    assert abs(chi2 - dof) <= 3 * np.sqrt(2 * dof), (chi2, dof)
+    ev_o = (c["n_elastic"] + c["n_inelastic"] + c["n_boundary"]) / n
+    ev_r = (st["n_intersect"] + st["n_elastic"] + st["n_inelastic"]) / n
+    assert abs(ev_o - ev_r) / ev_r < 0.05
