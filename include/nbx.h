@@ -28,6 +28,8 @@
  *   nbx_get_running_count gpu_driver::get_running_count drivers/gpu/gpu_driver.h:100-110
  *   nbx_flush_detected    gpu_driver::flush_detected / flush_buffered
  *                                                       drivers/gpu/gpu_driver.inl:259-306
+ *   nbx_flush_deposits    energydeposit_cpu_driver's deposit callback
+ *                                                       drivers/cpu/energydeposit_cpu_driver.h:74-96
  *   nbx_ray_query         octree::propagate            geometry/octree.inl:33-192
  *   nbx_table_query       table_1D::get, table_2D::get / get_rounddown
  *                                                       common/util/table_1D.inl:66-80,
@@ -181,7 +183,20 @@ typedef struct {
     int32_t blocks_per_sm;     /* transport variant: 2, 3 or 4 resident 256-thread blocks per SM, or 7
                                   128-thread blocks (block_size capped at 128); 0 = 3 */
     int32_t inelastic_model;   /* NBX_INELASTIC_KIEFT (0, default) or NBX_INELASTIC_FULL_PENN */
+    int32_t record_deposits;   /* keep energy-deposit records (plain mode; cpu_energydep.cpp) */
+    uint64_t deposit_capacity; /* deposit records held on the device; 0 = 2^27 (3.2 GB) */
 } nbx_config;
+
+/* One energy deposit (drivers/cpu/energydeposit_cpu_driver.h:74-96,
+ * cpu_energydep.cpp:189-207): a scattering event (not a boundary crossing)
+ * that changed the electron's energy; position after the event, energy
+ * before it, energy lost, and the primary's tag. */
+typedef struct {
+    float pos[3];
+    float E;
+    float dE;
+    uint32_t tag;
+} nbx_deposit;
 
 typedef struct {
     uint64_t primaries_pushed;
@@ -204,6 +219,8 @@ typedef struct {
     uint64_t samples;         /* training samples recorded (sample mode) */
     double last_run_ms;       /* device time of the last nbx_run (CUDA events) */
     double last_kernel_ms;    /* device time of its transport launches only */
+    uint64_t deposits;        /* energy-deposit records written (record_deposits) */
+    uint64_t deposits_dropped; /* deposits lost to a full deposit buffer */
 } nbx_stats;
 
 /* ---- host-side helpers (no GPU needed) ---------------------------------- */
@@ -237,6 +254,15 @@ int nbx_set_uid_base(nbx_ctx* ctx, uint64_t base);
 int nbx_run(nbx_ctx* ctx);
 int nbx_get_running_count(nbx_ctx* ctx, uint64_t* n);
 int nbx_get_stats(nbx_ctx* ctx, nbx_stats* out);
+/* Energy-deposit records of the runs since the last full flush, compacted,
+ * in no particular order (replaces the deposit callback of
+ * energydeposit_cpu_driver::simulate_to_end, drivers/cpu/
+ * energydeposit_cpu_driver.h:74-96).  Copies up to `capacity` records into
+ * `out`; call again until *n comes back 0.  A run while records are still
+ * pending appends to them.  The context must be created with
+ * record_deposits; runs whose records overflow deposit_capacity count the
+ * lost ones in nbx_stats.deposits_dropped. */
+int nbx_flush_deposits(nbx_ctx* ctx, nbx_deposit* out, uint64_t capacity, uint64_t* n);
 /* Copy out (and remove) up to cap detected electrons. */
 int nbx_flush_detected(nbx_ctx* ctx, nbx_detected* out, uint64_t cap, uint64_t* n);
 /* Detections per primary tag below / at-or-above 50 eV. */

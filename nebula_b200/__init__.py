@@ -72,7 +72,8 @@ INELASTIC_MODELS = {"kieft": 0, "penn": 1, "full_penn": 1}
 class Config(C.Structure):
     _fields_ = [("device", C.c_int32), ("seed", C.c_uint32), ("energy_threshold", C.c_float),
                 ("capacity", C.c_uint64), ("record_detected", C.c_int32), ("record_capacity", C.c_uint64),
-                ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("inelastic_model", C.c_int32)]
+                ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("inelastic_model", C.c_int32),
+                ("record_deposits", C.c_int32), ("deposit_capacity", C.c_uint64)]
 
 
 class Stats(C.Structure):
@@ -80,13 +81,15 @@ class Stats(C.Structure):
         "primaries_pushed", "primaries_done", "steps", "events_elastic", "events_inelastic", "events_boundary",
         "secondaries", "detected", "detected_se", "detected_bse", "terminated", "records_dropped", "generations",
         "queue_overflow", "inferences", "roulette_killed", "splits", "samples")] + [
-        ("last_run_ms", C.c_double), ("last_kernel_ms", C.c_double)]
+        ("last_run_ms", C.c_double), ("last_kernel_ms", C.c_double), ("deposits", C.c_uint64),
+        ("deposits_dropped", C.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 DETECTED_DTYPE = np.dtype([("pos", "<f4", (3,)), ("dir", "<f4", (3,)), ("E", "<f4"), ("tag", "<u4")])
+DEPOSIT_DTYPE = np.dtype([("pos", "<f4", (3,)), ("E", "<f4"), ("dE", "<f4"), ("tag", "<u4")])
 ELECTRON_DTYPE = np.dtype([("pos", "<f4", (3,)), ("dir", "<f4", (3,)), ("E", "<f4"), ("mat", "<i4"),
                            ("last_tri", "<i4"), ("tag", "<u4"), ("uid", "<u8"), ("step", "<u4"), ("pad", "<u4")])
 assert ELECTRON_DTYPE.itemsize == 56
@@ -131,6 +134,7 @@ def lib():
         "nbx_get_running_count": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
         "nbx_get_stats": (C.c_int, [_vp, C.POINTER(Stats)]),
         "nbx_flush_detected": (C.c_int, [_vp, _vp, C.c_uint64, C.POINTER(C.c_uint64)]),
+        "nbx_flush_deposits": (C.c_int, [_vp, _vp, C.c_uint64, C.POINTER(C.c_uint64)]),
         "nbx_get_tag_counts": (C.c_int, [_vp, C.c_uint64, C.c_uint64, _vp, _vp]),
         "nbx_pixel_yields": (C.c_int, [_vp, _vp, C.c_uint64, C.c_uint64, _vp]),
         "nbx_get_spectrum": (C.c_int, [_vp, _vp, C.c_uint32, C.POINTER(C.c_float)]),
@@ -270,7 +274,8 @@ class Context:
     """One simulation context on one GPU (the reference's gpu_driver)."""
 
     def __init__(self, device=0, seed=0x78C7E39B, energy_threshold=0.0, record_detected=False,
-                 record_capacity=0, capacity=0, block_size=0, blocks_per_sm=0, inelastic="kieft"):
+                 record_capacity=0, capacity=0, block_size=0, blocks_per_sm=0, inelastic="kieft",
+                 record_deposits=False, deposit_capacity=0):
         L = lib()
         cfg = Config()
         L.nbx_config_default(C.byref(cfg))
@@ -278,6 +283,7 @@ class Context:
         cfg.record_detected, cfg.record_capacity, cfg.capacity = int(record_detected), record_capacity, capacity
         cfg.block_size, cfg.blocks_per_sm = block_size, blocks_per_sm
         cfg.inelastic_model = INELASTIC_MODELS.get(inelastic, inelastic)
+        cfg.record_deposits, cfg.deposit_capacity = int(record_deposits), deposit_capacity
         self.h = _vp()
         _check(L.nbx_create(C.byref(self.h), C.byref(cfg)))
         self.L = L
@@ -347,6 +353,18 @@ class Context:
         n = C.c_uint64()
         self._ck(self.L.nbx_flush_detected(self.h, _ptr(out), cap, C.byref(n)))
         return out[: n.value]
+
+    def flush_deposits(self, chunk=1 << 22) -> np.ndarray:
+        """All energy-deposit records pending on the device (DEPOSIT_DTYPE)."""
+        parts = []
+        while True:
+            out = np.zeros(chunk, DEPOSIT_DTYPE)
+            n = C.c_uint64()
+            self._ck(self.L.nbx_flush_deposits(self.h, _ptr(out), chunk, C.byref(n)))
+            if n.value == 0:
+                break
+            parts.append(out[: n.value])
+        return np.concatenate(parts) if parts else np.zeros(0, DEPOSIT_DTYPE)
 
     def tag_counts(self, first, n):
         se = np.zeros(n, np.uint32)

@@ -35,6 +35,8 @@ enum Counter : int {
     kCntRouletteKilled,
     kCntSplit,
     kCntSamples,
+    kCntDeposits,
+    kCntDepositsDropped,
     kNumCounters
 };
 
@@ -70,9 +72,21 @@ struct TransportArgs {
     float split_threshold;
     int rr_period;              // infer every rr_period steps of an electron
     dev::SurfaceMap smap;
+    // deposit mode: one record per scattering event that changed the energy
+    // (drivers/cpu/energydeposit_cpu_driver.h:74-96), kDepositWords floats
+    // each: position after the event, energy before, energy lost, tag bits
+    float* dep;
+    unsigned long long* dep_cursor;   // records handed out (chunks of kDepositChunk)
+    unsigned long long dep_capacity;  // records the buffer holds
 };
 
-enum : int { kModePlain = 0, kModeSample = 1, kModeLearned = 2 };
+// Deposit records: x, y, z, E_before, E_before - E_after, tag; unused slots of
+// a thread's last chunk carry tag kDepositEmpty.
+constexpr int kDepositWords = 6;
+constexpr uint32_t kDepositChunk = 32;
+constexpr uint32_t kDepositEmpty = 0xFFFFFFFFu;
+
+enum : int { kModePlain = 0, kModeSample = 1, kModeLearned = 2, kModeDeposit = 3 };
 
 #ifndef NBX_LOCAL_STACK
 #define NBX_LOCAL_STACK 16

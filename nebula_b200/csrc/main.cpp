@@ -121,6 +121,9 @@ int main(int argc, char** argv) {
     p.add("device", "CUDA device ordinal", "0");
     p.add("inelastic", "Inelastic model: kieft (Kieft & Bosch) or penn (full Penn, the reference's stock build)",
           "kieft");
+    p.add("energy-deposit", "Also write energy deposits, as the reference's nebula_cpu_energydep", "0");
+    p.add("detect-filename", "With --energy-deposit: file for detected electrons", "detected.bin");
+    p.add("deposit-filename", "With --energy-deposit: file for energy deposits", "stdout");
     try {
         p.parse(argc, argv);
     } catch (const std::exception& e) {
@@ -136,6 +139,9 @@ int main(int argc, char** argv) {
     const bool sort_primaries = p.get<bool>("sort-primaries");
     const int device = p.get<int>("device");
     const std::string inelastic = p.get<std::string>("inelastic");
+    const bool energy_deposit = p.get<bool>("energy-deposit");
+    const std::string detect_filename = p.get<std::string>("detect-filename");
+    const std::string deposit_filename = p.get<std::string>("deposit-filename");
     if (p.positional.size() < 3 || capacity == 0 || prescan == 0 || batch_factor <= 0 ||
         (inelastic != "kieft" && inelastic != "penn")) {
         p.usage(std::cerr);
@@ -260,6 +266,7 @@ int main(int argc, char** argv) {
     cfg.inelastic_model = inelastic == "penn" ? NBX_INELASTIC_FULL_PENN : NBX_INELASTIC_KIEFT;
     cfg.record_detected = 1;
     cfg.record_capacity = 1ull << 24;
+    cfg.record_deposits = energy_deposit ? 1 : 0;
     nbx_ctx* ctx = nullptr;
     rc = nbx_create(&ctx, &cfg);
     if (rc != NBX_OK) return die(nullptr, rc, "nbx_create");
@@ -270,8 +277,32 @@ int main(int argc, char** argv) {
                  (unsigned long long)oct->n_triangles, (unsigned long long)n_pri, mats.size());
 
     // Simulation: batches of `capacity` primaries, detected records streamed out.
+    // With --energy-deposit (cpu_energydep.cpp:156-214): detected electrons go
+    // to --detect-filename and 28-byte deposit records {x, y, z, E, dE, px, py}
+    // to --deposit-filename; the first batch (--prescan-size primaries) measures
+    // deposits per primary, and later batches are sized to fit the device's
+    // deposit buffer (times --batch-factor).
+    FILE* detect_out = stdout;
+    FILE* deposit_out = nullptr;
+    if (energy_deposit) {
+        detect_out = detect_filename == "stdout" ? stdout : std::fopen(detect_filename.c_str(), "wb");
+        deposit_out = deposit_filename == "stdout" ? stdout : std::fopen(deposit_filename.c_str(), "wb");
+        if (!detect_out || !deposit_out) {
+            std::fprintf(stderr, "Error: could not open the output files\n");
+            return 1;
+        }
+    }
+    struct DepositRecord {
+        float x, y, z, E, dE;
+        int32_t px, py;
+    };
+    static_assert(sizeof(DepositRecord) == 28, "deposit record layout");
+    const uint64_t dep_capacity = uint64_t(1) << 27;   // nbx_config default
+    std::vector<nbx_deposit> dep(energy_deposit ? (1u << 20) : 0);
+    std::vector<DepositRecord> dep_out;
     timer.start();
-    const uint64_t batch = std::max<uint64_t>(capacity, 1);
+    uint64_t batch = std::max<uint64_t>(capacity, 1);
+    if (energy_deposit) batch = std::min<uint64_t>(batch, std::max<uint32_t>(prescan, 1));
     std::vector<nbx_particle> part;
     std::vector<uint32_t> tags;
     std::vector<nbx_detected> det(1u << 20);
@@ -302,12 +333,43 @@ int main(int argc, char** argv) {
                 out[i].px = pri[det[i].tag].px;
                 out[i].py = pri[det[i].tag].py;
             }
-            std::fwrite(out.data(), sizeof(nbx_record), got, stdout);
+            std::fwrite(out.data(), sizeof(nbx_record), got, detect_out);
+        }
+        if (energy_deposit) {
+            uint64_t n_dep = 0;
+            for (;;) {
+                uint64_t got = 0;
+                if ((rc = nbx_flush_deposits(ctx, dep.data(), dep.size(), &got)) != NBX_OK)
+                    return die(ctx, rc, "flush deposits");
+                if (got == 0) break;
+                n_dep += got;
+                dep_out.resize(got);
+                for (uint64_t i = 0; i < got; ++i) {
+                    const nbx_deposit& d = dep[i];
+                    dep_out[i] = {d.pos[0], d.pos[1], d.pos[2], d.E, d.dE, pri[d.tag].px, pri[d.tag].py};
+                }
+                std::fwrite(dep_out.data(), sizeof(DepositRecord), got, deposit_out);
+            }
+            nbx_stats st;
+            nbx_get_stats(ctx, &st);
+            if (st.deposits_dropped) {
+                std::fprintf(stderr, "\nError: %llu energy deposits did not fit the device buffer; lower --batch-factor\n",
+                             (unsigned long long)st.deposits_dropped);
+                return die(ctx, NBX_ERR_CAPACITY, "deposit buffer");
+            }
+            // size the next batches from the deposits per primary seen so far
+            const double per_primary = double(n_dep) / double(n);
+            const double fit = batch_factor * double(dep_capacity) / std::max(per_primary, 1.0);
+            batch = std::max<uint64_t>(1, std::min<uint64_t>(std::max<uint64_t>(capacity, 1), uint64_t(fit)));
         }
         done += n;
         std::fprintf(stderr, " \rProgress %.2f%%", 100.0 * double(done) / double(n_pri));
     }
     std::fflush(stdout);
+    if (energy_deposit) {
+        if (detect_out != stdout) std::fclose(detect_out);
+        if (deposit_out != stdout) std::fclose(deposit_out);
+    }
     timer.stop("Simulation");
     nbx_stats st;
     nbx_get_stats(ctx, &st);

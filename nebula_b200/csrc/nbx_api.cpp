@@ -96,6 +96,10 @@ struct nbx_ctx {
     DevBuf<int32_t> octree;
     DevBuf<float4> tris;
     DevBuf<float4> tri_faces;
+    // energy-deposit records (kDepositWords floats each) and the device cursor
+    DevBuf<float> dep;
+    DevBuf<unsigned long long> dep_cursor;
+    uint64_t dep_cap = 0, dep_flushed = 0;
     bool have_geometry = false;
     // materials
     std::vector<DevBuf<float>*> tables;
@@ -466,6 +470,12 @@ int nbx_create(nbx_ctx** out, const nbx_config* cfg) {
         ctx->variant = ((c.blocks_per_sm >= 2 && c.blocks_per_sm <= 4) || c.blocks_per_sm == 7) ? c.blocks_per_sm : 3;
         if (ctx->variant == 7 && ctx->block > 128) ctx->block = 128;
         ctx->bpsm = nbx::transport_max_blocks_per_sm(ctx->block, ctx->variant);
+        if (c.record_deposits) {
+            ctx->dep_cap = c.deposit_capacity ? c.deposit_capacity : (1ull << 27);
+            ctx->dep.alloc(ctx->dep_cap * nbx::kDepositWords);
+            ctx->dep_cursor.alloc(1);
+            ck(cudaMemset(ctx->dep_cursor.p, 0, sizeof(unsigned long long)), "memset");
+        }
         if (c.record_detected) {
             ctx->rec_cap = c.record_capacity ? c.record_capacity : (1ull << 24);
             ctx->rec_a.alloc(ctx->rec_cap);
@@ -683,7 +693,16 @@ int nbx_run(nbx_ctx* ctx) {
             a.split_threshold = ctx->split_threshold;
             a.rr_period = ctx->rr_period;
         }
-        const int bpsm = nbx::transport_max_blocks_per_sm(ctx->block, ctx->variant, ctx->mode);
+        int mode = ctx->mode;
+        if (ctx->cfg.record_deposits) {
+            // energy-deposit records (cpu_energydep.cpp's driver) ride on plain transport
+            if (mode != nbx::kModePlain) throw ApiError(NBX_ERR_STATE, "energy deposits need the plain mode");
+            mode = nbx::kModeDeposit;
+            a.dep = ctx->dep.p;
+            a.dep_cursor = ctx->dep_cursor.p;
+            a.dep_capacity = ctx->dep_cap;
+        }
+        const int bpsm = nbx::transport_max_blocks_per_sm(ctx->block, ctx->variant, mode);
         const int grid = ctx->sms * bpsm;
 
         ck(cudaEventRecord(ctx->ev0, ctx->stream), "event");
@@ -700,7 +719,7 @@ int nbx_run(nbx_ctx* ctx) {
                 a.out_tail = ctl + kMaxGenerations + g;
                 a.out_capacity = cap;
                 a.in_capacity = uint32_t(std::min<uint64_t>(in->cap, 0xFFFFFFF0ull));
-                ck(nbx::launch_transport(ctx->phys, a, grid, ctx->block, ctx->variant, ctx->stream, ctx->mode),
+                ck(nbx::launch_transport(ctx->phys, a, grid, ctx->block, ctx->variant, ctx->stream, mode),
                    "transport launch");
             }
             uint32_t last = 0;
@@ -753,6 +772,8 @@ int nbx_get_stats(nbx_ctx* ctx, nbx_stats* out) {
         out->roulette_killed = c[nbx::kCntRouletteKilled];
         out->splits = c[nbx::kCntSplit];
         out->samples = c[nbx::kCntSamples];
+        out->deposits = c[nbx::kCntDeposits];
+        out->deposits_dropped = c[nbx::kCntDepositsDropped];
         out->generations = ctx->generations;
         out->last_run_ms = ctx->last_run_ms;
         out->last_kernel_ms = ctx->last_kernel_ms;
@@ -917,6 +938,51 @@ int nbx_table3_query(nbx_ctx* ctx, int32_t material, int32_t table, const float*
         ck(nbx::launch_table3_query(ctx->phys.mat[material], table, dx.p, dy.p, dz.p, n, dout.p, s), "table query");
         ck(cudaMemcpyAsync(out, dout.p, 4 * n, cudaMemcpyDeviceToHost, s), "D2H");
         ck(cudaStreamSynchronize(s), "sync");
+        return NBX_OK;
+    });
+}
+
+int nbx_flush_deposits(nbx_ctx* ctx, nbx_deposit* out, uint64_t capacity, uint64_t* n_out) {
+    if (!ctx || !n_out || (capacity && !out)) return NBX_ERR_ARG;
+    if (!ctx->cfg.record_deposits) return fail(ctx, NBX_ERR_STATE, "context created without record_deposits");
+    return guarded(ctx, [&] {
+        *n_out = 0;
+        unsigned long long cursor = 0;
+        ck(cudaMemcpyAsync(&cursor, ctx->dep_cursor.p, sizeof cursor, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        ck(cudaStreamSynchronize(ctx->stream), "sync");
+        const uint64_t end = std::min<uint64_t>(cursor, ctx->dep_cap);
+        // copy slot ranges from where the last call stopped, dropping the
+        // unused tails of the threads' chunks, until `capacity` records
+        std::vector<float> stage;
+        const uint64_t kStage = 1ull << 20;
+        while (ctx->dep_flushed < end && *n_out < capacity) {
+            const uint64_t take = std::min<uint64_t>(kStage, end - ctx->dep_flushed);
+            stage.resize(take * nbx::kDepositWords);
+            ck(cudaMemcpyAsync(stage.data(), ctx->dep.p + ctx->dep_flushed * nbx::kDepositWords,
+                               sizeof(float) * stage.size(), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+            ck(cudaStreamSynchronize(ctx->stream), "sync");
+            uint64_t used = 0;
+            for (; used < take && *n_out < capacity; ++used) {
+                const float* r = stage.data() + used * nbx::kDepositWords;
+                uint32_t tag;
+                std::memcpy(&tag, r + 5, 4);
+                if (tag == nbx::kDepositEmpty) continue;
+                nbx_deposit& d = out[(*n_out)++];
+                d.pos[0] = r[0];
+                d.pos[1] = r[1];
+                d.pos[2] = r[2];
+                d.E = r[3];
+                d.dE = r[4];
+                d.tag = tag;
+            }
+            ctx->dep_flushed += used;
+        }
+        if (ctx->dep_flushed >= end) {
+            // everything handed out: start the buffer over
+            ck(cudaMemsetAsync(ctx->dep_cursor.p, 0, sizeof(unsigned long long), ctx->stream), "memset");
+            ck(cudaStreamSynchronize(ctx->stream), "sync");
+            ctx->dep_flushed = 0;
+        }
         return NBX_OK;
     });
 }

@@ -92,8 +92,10 @@ __device__ __forceinline__ uint32_t mix32(uint64_t x) {
 // also records one (features, label) training sample per sampled electron)
 // or kModeLearned (weighted roulette / splitting with the network as the
 // importance function; the warp stays converged for the tensor-core
-// inference, so lanes without work idle until the whole warp is done).
-template <int MinBlocks, int Mode>
+// inference, so lanes without work idle until the whole warp is done), or
+// kModeDeposit (plain transport that also appends an energy-deposit record
+// per energy-changing scattering event).
+template <int MinBlocks, int Mode, bool Penn>
 __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transport_kernel(const dev::Physics P, const TransportArgs a) {
     // Leaf cache: 13 words per thread in dynamic shared memory sized by the
     // launch (13 * 4 * blockDim.x bytes), so a 128-thread block does not hold
@@ -126,7 +128,11 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
     // launch to wrap); rare ones (dropped records, queue overflow) go straight
     // to the global counters.
     uint32_t c_steps = 0, c_el = 0, c_inel = 0, c_bd = 0, c_se = 0, c_dse = 0, c_dbse = 0, c_term = 0, c_pop = 0,
-             c_inf = 0, c_kill = 0, c_split = 0, c_smp = 0;
+             c_inf = 0, c_kill = 0, c_split = 0, c_smp = 0, c_dep = 0, c_dep_drop = 0;
+    // Deposit mode: this thread's current chunk [dep_pos, dep_end) of the
+    // record buffer, taken kDepositChunk records at a time with one atomic.
+    unsigned long long dep_pos = 0, dep_end = 0;
+    bool dep_full = false;
     for (;;) {
         if (!alive && !drained) {
             if (sp > 0) {
@@ -234,8 +240,38 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
         int ev;
         bool has_se;
         dev::Electron se;
-        int st = dev::step(P, e, &ev, &se, &has_se, cache);
+        [[maybe_unused]] const float E_before = e.E;
+        int st = dev::step<Penn>(P, e, &ev, &se, &has_se, cache);
         ++c_steps;
+        if constexpr (Mode == kModeDeposit) {
+            // energydeposit_cpu_driver::simulate_to_end (drivers/cpu/
+            // energydeposit_cpu_driver.h:74-96): scattering events only, and
+            // only when the energy changed; position after the event.
+            if ((ev == dev::kEvElastic || ev == dev::kEvInelastic) && e.E != E_before) {
+                if (dep_pos == dep_end && !dep_full) {
+                    const unsigned long long base = atomicAdd(a.dep_cursor, (unsigned long long)kDepositChunk);
+                    if (base + kDepositChunk <= a.dep_capacity) {
+                        dep_pos = base;
+                        dep_end = base + kDepositChunk;
+                    } else {
+                        dep_full = true;
+                    }
+                }
+                if (dep_pos < dep_end) {
+                    float* r = a.dep + dep_pos * kDepositWords;
+                    r[0] = e.px;
+                    r[1] = e.py;
+                    r[2] = e.pz;
+                    r[3] = E_before;
+                    r[4] = E_before - e.E;
+                    r[5] = __uint_as_float(e.tag);
+                    ++dep_pos;
+                    ++c_dep;
+                } else {
+                    ++c_dep_drop;
+                }
+            }
+        }
         c_el += (ev == dev::kEvElastic);
         c_inel += (ev == dev::kEvInelastic);
         c_bd += (ev == dev::kEvBoundary);
@@ -315,6 +351,10 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
             carry_hit = sub;
         }
     }
+    if constexpr (Mode == kModeDeposit) {
+        // mark the unused tail of this thread's last chunk
+        for (; dep_pos < dep_end; ++dep_pos) a.dep[dep_pos * kDepositWords + 5] = __uint_as_float(kDepositEmpty);
+    }
     // Counters: one atomic per warp per counter.
     unsigned long long v[kNumCounters];
     v[kCntSteps] = c_steps;
@@ -333,6 +373,8 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
     v[kCntRouletteKilled] = c_kill;
     v[kCntSplit] = c_split;
     v[kCntSamples] = c_smp;
+    v[kCntDeposits] = c_dep;
+    v[kCntDepositsDropped] = c_dep_drop;
     __syncwarp();
     const int lane = threadIdx.x & 31;
 #pragma unroll
@@ -449,7 +491,7 @@ __global__ void step_query_kernel(const dev::Physics P, ElectronRecord* el, uint
         dev::Electron se{};
         int ev;
         bool hs;
-        status[i] = dev::step(P, e, &ev, &se, &hs);
+        status[i] = P.penn ? dev::step<true>(P, e, &ev, &se, &hs) : dev::step<false>(P, e, &ev, &se, &hs);
         event[i] = ev;
         has_se[i] = hs ? 1 : 0;
         to_record(e, el[i]);
@@ -557,31 +599,39 @@ static void fit_carveout(Kernel kernel, int block) {
     }
 }
 
-template <int Mode>
+template <int Mode, bool Penn>
 static cudaError_t launch_mode(const dev::Physics& P, const TransportArgs& a, int grid, int block, int variant,
                                cudaStream_t s) {
     if (block <= 0 || block > (variant == 7 ? 128 : 256)) return cudaErrorInvalidValue;
     const size_t sm = leaf_cache_bytes(block);
     switch (variant) {
-    case 2: fit_carveout(transport_kernel<2, Mode>, block); break;
-    case 4: fit_carveout(transport_kernel<4, Mode>, block); break;
-    case 7: fit_carveout(transport_kernel<7, Mode>, block); break;
-    default: fit_carveout(transport_kernel<3, Mode>, block); break;
+    case 2: fit_carveout(transport_kernel<2, Mode, Penn>, block); break;
+    case 4: fit_carveout(transport_kernel<4, Mode, Penn>, block); break;
+    case 7: fit_carveout(transport_kernel<7, Mode, Penn>, block); break;
+    default: fit_carveout(transport_kernel<3, Mode, Penn>, block); break;
     }
     switch (variant) {
-    case 2: transport_kernel<2, Mode><<<grid, block, sm, s>>>(P, a); break;
-    case 4: transport_kernel<4, Mode><<<grid, block, sm, s>>>(P, a); break;
-    case 7: transport_kernel<7, Mode><<<grid, block, sm, s>>>(P, a); break;
-    default: transport_kernel<3, Mode><<<grid, block, sm, s>>>(P, a); break;
+    case 2: transport_kernel<2, Mode, Penn><<<grid, block, sm, s>>>(P, a); break;
+    case 4: transport_kernel<4, Mode, Penn><<<grid, block, sm, s>>>(P, a); break;
+    case 7: transport_kernel<7, Mode, Penn><<<grid, block, sm, s>>>(P, a); break;
+    default: transport_kernel<3, Mode, Penn><<<grid, block, sm, s>>>(P, a); break;
     }
     return cudaGetLastError();
 }
 
+template <bool Penn>
+static cudaError_t launch_model(const dev::Physics& P, const TransportArgs& a, int grid, int block, int variant,
+                                cudaStream_t s, int mode) {
+    if (mode == kModeSample) return launch_mode<kModeSample, Penn>(P, a, grid, block, variant, s);
+    if (mode == kModeLearned) return launch_mode<kModeLearned, Penn>(P, a, grid, block, variant, s);
+    if (mode == kModeDeposit) return launch_mode<kModeDeposit, Penn>(P, a, grid, block, variant, s);
+    return launch_mode<kModePlain, Penn>(P, a, grid, block, variant, s);
+}
+
 cudaError_t launch_transport(const dev::Physics& P, const TransportArgs& a, int grid, int block, int variant,
                              cudaStream_t s, int mode) {
-    if (mode == kModeSample) return launch_mode<kModeSample>(P, a, grid, block, variant, s);
-    if (mode == kModeLearned) return launch_mode<kModeLearned>(P, a, grid, block, variant, s);
-    return launch_mode<kModePlain>(P, a, grid, block, variant, s);
+    return P.penn ? launch_model<true>(P, a, grid, block, variant, s, mode)
+                  : launch_model<false>(P, a, grid, block, variant, s, mode);
 }
 
 template <int Mode>
@@ -590,10 +640,11 @@ static int max_blocks_mode(int block, int variant) {
     cudaError_t e;
     const size_t sm = leaf_cache_bytes(block);
     switch (variant) {
-    case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<2, Mode>, block, sm); break;
-    case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<4, Mode>, block, sm); break;
-    case 7: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<7, Mode>, block, sm); break;
-    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<3, Mode>, block, sm); break;
+    // both models share launch bounds and shared memory, hence occupancy
+    case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<2, Mode, false>, block, sm); break;
+    case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<4, Mode, false>, block, sm); break;
+    case 7: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<7, Mode, false>, block, sm); break;
+    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<3, Mode, false>, block, sm); break;
     }
     if (e != cudaSuccess) return 1;
     return n > 0 ? n : 1;
@@ -602,6 +653,7 @@ static int max_blocks_mode(int block, int variant) {
 int transport_max_blocks_per_sm(int block, int variant, int mode) {
     if (mode == kModeSample) return max_blocks_mode<kModeSample>(block, variant);
     if (mode == kModeLearned) return max_blocks_mode<kModeLearned>(block, variant);
+    if (mode == kModeDeposit) return max_blocks_mode<kModeDeposit>(block, variant);
     return max_blocks_mode<kModePlain>(block, variant);
 }
 

@@ -668,7 +668,10 @@ __device__ __forceinline__ bool ends_at_init(const Physics& P, const Electron& e
 // inelastic/elastic free paths, z the ICDF probability (or the boundary
 // transmission draw), w the scattering azimuth; block 1 the remaining four
 // inelastic draws.  The mechanisms' log(E) is the init pass's log(E): the
-// energy has not changed in between, so the value is the same.
+// energy has not changed in between, so the value is the same.  kPenn
+// selects the inelastic model at compile time (P.penn must agree), as the
+// reference's physics_config.h does.
+template <bool kPenn>
 __device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, Electron* se, bool* has_se,
                                     LeafCache cache = LeafCache{nullptr, 0}) {
     *event = kEvNone;
@@ -724,7 +727,7 @@ __device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, E
                 *event = kEvElastic;
             } else {
                 const uint4 r1 = draw(P.seed, e, 1);
-                if (P.penn)
+                if constexpr (kPenn)
                     *has_se = penn_finish(P, m, e, tv, logE, nd, n, r1, se);
                 else
                     *has_se = inelastic_finish(m, e, tv, nd, n, u01(r1.x), u01(r1.y), u01(r1.z), u01(r1.w), se);
