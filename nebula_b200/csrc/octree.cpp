@@ -1,11 +1,16 @@
 // Octree builder with the reference's linearized layout; see octree.h.
 #include "octree.h"
 
+#include <algorithm>
+#include <array>
+#include <atomic>
 #include <cmath>
+#include <cstring>
 #include <fstream>
-#include <queue>
 #include <sstream>
 #include <stdexcept>
+#include <thread>
+#include <unordered_map>
 
 namespace nbx {
 
@@ -16,23 +21,12 @@ constexpr int kSplitCount = 16;  // octree_builder.h:158
 inline Vec3 add(Vec3 a, Vec3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
 inline Vec3 sub(Vec3 a, Vec3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
 inline Vec3 scale(float s, Vec3 a) { return {s * a.x, s * a.y, s * a.z}; }
-inline bool eq(Vec3 a, Vec3 b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
 inline float fmin_ref(float a, float b) { return (b < a) ? b : a; }   // std::min
 inline float fmax_ref(float a, float b) { return (a < b) ? b : a; }   // std::max
 
 Vec3 vert(const Triangle& t, int i) {
     if (i == 0) return t.r0;
     return add(t.r0, i == 1 ? t.e1 : t.e2);
-}
-
-// triangle::perfect_overlap (source/core/triangle.inl:94-111): same vertex
-// set in any cyclic or reversed order, materials ignored.
-bool perfect_overlap(const Triangle& a, const Triangle& b) {
-    const Vec3 a0 = vert(a, 0), a1 = vert(a, 1), a2 = vert(a, 2);
-    const Vec3 b0 = vert(b, 0), b1 = vert(b, 1), b2 = vert(b, 2);
-    return (eq(a0, b0) && eq(a1, b1) && eq(a2, b2)) || (eq(a0, b1) && eq(a1, b2) && eq(a2, b0)) ||
-           (eq(a0, b2) && eq(a1, b0) && eq(a2, b1)) || (eq(a0, b0) && eq(a1, b2) && eq(a2, b1)) ||
-           (eq(a0, b1) && eq(a1, b0) && eq(a2, b2)) || (eq(a0, b2) && eq(a1, b1) && eq(a2, b0));
 }
 
 // Separating-axis triangle/box overlap test of T. Akenine-Moeller ("Fast 3D
@@ -144,62 +138,158 @@ bool overlap(const Triangle& t, Vec3 c, Vec3 h) {
     return tri_box_overlap(center, half, tv);
 }
 
-struct Builder {
-    struct Node {
-        int32_t first_child = -1;     // -1: leaf
-        std::vector<uint32_t> tris;
-    };
-    const std::vector<Triangle>& all;
-    std::vector<Node> nodes;
-    uint64_t duplicates = 0;
-    int max_depth = 0;
+// Children of a cell (octree_builder.cpp: octree_node octants).
+void octant(int o, Vec3 c, Vec3 h, Vec3* oc, Vec3* oh) {
+    *oh = scale(0.5f, h);
+    oc->x = c.x + float(((o & 1) << 1) - 1) * oh->x;
+    oc->y = c.y + float((o & 2) - 1) * oh->y;
+    oc->z = c.z + float(((o & 4) >> 1) - 1) * oh->z;
+}
 
-    explicit Builder(const std::vector<Triangle>& t) : all(t) {}
-
-    static void octant(int o, Vec3 c, Vec3 h, Vec3* oc, Vec3* oh) {
-        *oh = scale(0.5f, h);
-        oc->x = c.x + float(((o & 1) << 1) - 1) * oh->x;
-        oc->y = c.y + float((o & 2) - 1) * oh->y;
-        oc->z = c.z + float(((o & 4) >> 1) - 1) * oh->z;
+// Runs fn(task) for task in [0, n) on all host cores.
+template <typename Fn>
+void parallel_for(size_t n, Fn fn) {
+    const size_t hw = std::max<unsigned>(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::min(hw, n);
+    if (nt <= 1) {
+        for (size_t i = 0; i < n; ++i) fn(i);
+        return;
     }
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> th;
+    th.reserve(nt);
+    for (size_t t = 0; t < nt; ++t)
+        th.emplace_back([&] {
+            for (size_t i; (i = next.fetch_add(1)) < n;) fn(i);
+        });
+    for (auto& t : th) t.join();
+}
 
-    bool insert(int32_t node, uint32_t ti, Vec3 c, Vec3 h, int depth) {
-        const Triangle& t = all[ti];
-        if (!overlap(t, c, h)) return false;
-        if (depth > max_depth) max_depth = depth;
-        if (nodes[node].first_child < 0) {
-            for (uint32_t j : nodes[node].tris) {
-                if (perfect_overlap(t, all[j])) {
-                    ++duplicates;
-                    return false;
-                }
-            }
-            nodes[node].tris.push_back(ti);
-            if (int(nodes[node].tris.size()) > kSplitCount && depth < kMaxDepth) split(node, c, h, depth);
-        } else {
-            const int32_t fc = nodes[node].first_child;
-            for (int o = 0; o < 8; ++o) {
-                Vec3 oc, oh;
-                octant(o, c, h, &oc, &oh);
-                insert(fc + o, ti, oc, oh, depth + 1);
-            }
-        }
-        return true;
-    }
-
-    void split(int32_t node, Vec3 c, Vec3 h, int depth) {
-        const int32_t fc = int32_t(nodes.size());
-        nodes.resize(nodes.size() + 8);
-        nodes[node].first_child = fc;
-        const std::vector<uint32_t> tris = nodes[node].tris;
-        for (int o = 0; o < 8; ++o) {
-            Vec3 oc, oh;
-            octant(o, c, h, &oc, &oh);
-            for (uint32_t ti : tris) insert(fc + o, ti, oc, oh, depth + 1);
-        }
-        std::vector<uint32_t>().swap(nodes[node].tris);
+// Perfect-overlap class key (triangle::perfect_overlap, core/triangle.inl:
+// 94-111): the three vertices compared with ==, in any order.  -0 is folded
+// into +0 (they compare equal); a vertex with a NaN never equals anything.
+struct TriKey {
+    uint32_t w[9];
+    bool operator==(const TriKey& o) const { return std::memcmp(w, o.w, sizeof w) == 0; }
+};
+struct TriKeyHash {
+    size_t operator()(const TriKey& k) const {
+        uint64_t h = 1469598103934665603ull;
+        for (uint32_t x : k.w) h = (h ^ x) * 1099511628211ull;
+        return size_t(h);
     }
 };
+bool tri_key(const Triangle& t, TriKey* k) {
+    std::array<std::array<uint32_t, 3>, 3> v;
+    for (int i = 0; i < 3; ++i) {
+        const Vec3 p = vert(t, i);
+        const float c[3] = {p.x, p.y, p.z};
+        for (int j = 0; j < 3; ++j) {
+            if (std::isnan(c[j])) return false;
+            const float f = c[j] == 0.0f ? 0.0f : c[j];
+            std::memcpy(&v[i][j], &f, 4);
+        }
+    }
+    std::sort(v.begin(), v.end());
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) k->w[3 * i + j] = v[i][j];
+    return true;
+}
+
+// Top-down, level-synchronous construction of the tree the reference's
+// incremental octree_root::insert produces (octree_builder.cpp:93-169):
+//  * a triangle that perfectly overlaps an earlier one has the same geometry,
+//    so it reaches exactly the cells of the earlier one and is rejected in
+//    every leaf it reaches: dropping it up front changes no cell;
+//  * a cell is split as soon as its leaf list exceeds 16 distinct triangles
+//    below depth 21, and the set reaching a cell only grows, so the final
+//    tree splits exactly the cells whose final distinct count exceeds 16;
+//  * each list keeps insertion (= input) order, as splitting redistributes a
+//    leaf's list in order and later triangles are appended.
+// Cells are created level by level with children in octant order, which is
+// the breadth-first order of the linearized layout.  Each level's overlap
+// tests run in parallel over (cell, chunk of its list) tasks whose outputs
+// are concatenated in chunk order.
+struct Cell {
+    Vec3 c, h;
+    int depth;
+    int32_t first_child = -1;   // -1: leaf
+    std::vector<uint32_t> tris;
+};
+
+std::vector<Cell> build_cells(const std::vector<Triangle>& all, const std::vector<uint32_t>& ids, Vec3 c, Vec3 h,
+                              int* max_depth) {
+    std::vector<Cell> cells;
+    cells.push_back(Cell{c, h, 0, 1, {}});   // the root is always split
+    for (int o = 0; o < 8; ++o) {
+        Cell ch;
+        octant(o, c, h, &ch.c, &ch.h);
+        ch.depth = 1;
+        cells.push_back(std::move(ch));
+    }
+    // level 1 lists from the whole (deduplicated) triangle set
+    struct Task {
+        size_t parent;   // cell whose children receive the output
+        size_t lo, hi;   // range of the parent's list (or of `ids` for the root)
+        std::array<std::vector<uint32_t>, 8> out;
+    };
+    constexpr size_t kChunk = 4096;
+    auto run_level = [&](std::vector<Task>& tasks, auto source) {
+        parallel_for(tasks.size(), [&](size_t i) {
+            Task& t = tasks[i];
+            const Cell& p = cells[t.parent];
+            const std::vector<uint32_t>& src = source(t.parent);
+            Vec3 oc[8], oh[8];
+            for (int o = 0; o < 8; ++o) octant(o, p.c, p.h, &oc[o], &oh[o]);
+            for (size_t k = t.lo; k < t.hi; ++k) {
+                const uint32_t ti = src[k];
+                for (int o = 0; o < 8; ++o)
+                    if (overlap(all[ti], oc[o], oh[o])) t.out[o].push_back(ti);
+            }
+        });
+        // concatenate per child in chunk order
+        for (Task& t : tasks) {
+            const int32_t fc = cells[t.parent].first_child;
+            for (int o = 0; o < 8; ++o) {
+                auto& dst = cells[size_t(fc) + o].tris;
+                dst.insert(dst.end(), t.out[o].begin(), t.out[o].end());
+                std::vector<uint32_t>().swap(t.out[o]);
+            }
+        }
+    };
+    {
+        std::vector<Task> tasks;
+        for (size_t lo = 0; lo < ids.size(); lo += kChunk) tasks.push_back(Task{0, lo, std::min(ids.size(), lo + kChunk), {}});
+        run_level(tasks, [&](size_t) -> const std::vector<uint32_t>& { return ids; });
+    }
+    size_t level_begin = 1, level_end = cells.size();
+    while (level_begin < level_end) {
+        std::vector<Task> tasks;
+        for (size_t n = level_begin; n < level_end; ++n) {
+            Cell& cell = cells[n];
+            if (!cell.tris.empty() && cell.depth > *max_depth) *max_depth = cell.depth;
+            if (int(cell.tris.size()) > kSplitCount && cell.depth < kMaxDepth) {
+                cell.first_child = int32_t(cells.size());
+                const Vec3 pc = cell.c, ph = cell.h;
+                const int d = cell.depth + 1;
+                const size_t m = cell.tris.size();
+                for (int o = 0; o < 8; ++o) {
+                    Cell ch;
+                    octant(o, pc, ph, &ch.c, &ch.h);
+                    ch.depth = d;
+                    cells.push_back(std::move(ch));   // invalidates `cell`
+                }
+                for (size_t lo = 0; lo < m; lo += kChunk) tasks.push_back(Task{n, lo, std::min(m, lo + kChunk), {}});
+            }
+        }
+        run_level(tasks, [&](size_t parent) -> const std::vector<uint32_t>& { return cells[parent].tris; });
+        for (size_t n = level_begin; n < level_end; ++n)
+            if (cells[n].first_child >= 0) std::vector<uint32_t>().swap(cells[n].tris);
+        level_begin = level_end;
+        level_end = cells.size();
+    }
+    return cells;
+}
 }  // namespace
 
 Triangle make_triangle(Vec3 a, Vec3 b, Vec3 c, int mat_in, int mat_out) {
@@ -237,65 +327,64 @@ LinearOctree build_octree(const std::vector<Triangle>& input) {
     // Insert (octree_root::insert): triangles outside the root are skipped and
     // the kept ones are renumbered in insertion order.
     std::vector<Triangle> kept;
-    kept.reserve(input.size());
-    for (const Triangle& t : input)
-        if (overlap(t, out.center, out.halfsize)) kept.push_back(t);
-    Builder b(kept);
-    b.nodes.resize(9);
-    b.nodes[0].first_child = 1;
-    for (uint32_t ti = 0; ti < kept.size(); ++ti) {
-        for (int o = 0; o < 8; ++o) {
-            Vec3 oc, oh;
-            Builder::octant(o, out.center, out.halfsize, &oc, &oh);
-            b.insert(1 + o, ti, oc, oh, 1);
-        }
-    }
-    out.duplicates_dropped = b.duplicates;
-    out.max_depth = b.max_depth;
-
-    // Breadth-first (Morton) order of nodes.
-    std::vector<int32_t> order;
-    order.reserve(b.nodes.size());
     {
-        std::queue<int32_t> q;
-        q.push(0);
-        while (!q.empty()) {
-            const int32_t n = q.front();
-            q.pop();
-            order.push_back(n);
-            if (b.nodes[n].first_child >= 0)
-                for (int o = 0; o < 8; ++o) q.push(b.nodes[n].first_child + o);
+        std::vector<uint8_t> keep(input.size());
+        parallel_for((input.size() + 4095) / 4096, [&](size_t c) {
+            const size_t hi = std::min(input.size(), (c + 1) * 4096);
+            for (size_t i = c * 4096; i < hi; ++i) keep[i] = overlap(input[i], out.center, out.halfsize) ? 1 : 0;
+        });
+        kept.reserve(input.size());
+        for (size_t i = 0; i < input.size(); ++i)
+            if (keep[i]) kept.push_back(input[i]);
+    }
+    // Perfect-overlap duplicates (rejected in every leaf they reach).
+    std::vector<uint32_t> ids;
+    ids.reserve(kept.size());
+    {
+        std::unordered_map<TriKey, uint32_t, TriKeyHash> seen;
+        seen.reserve(kept.size() * 2);
+        for (uint32_t i = 0; i < kept.size(); ++i) {
+            TriKey k;
+            if (tri_key(kept[i], &k) && !seen.emplace(k, i).second) {
+                ++out.duplicates_dropped;
+                continue;
+            }
+            ids.push_back(i);
         }
     }
-    // Triangles in first-visit order over the leaves.
+    int max_depth = 0;
+    const std::vector<Cell> cells = build_cells(kept, ids, out.center, out.halfsize, &max_depth);
+    out.max_depth = max_depth;
+
+    // Triangles in first-visit order over the leaves (cells are breadth-first).
     std::vector<int32_t> tri_map(kept.size(), -1);
-    out.triangles.reserve(kept.size());
-    for (int32_t n : order) {
-        if (b.nodes[n].first_child >= 0) continue;
-        for (uint32_t ti : b.nodes[n].tris) {
+    out.triangles.reserve(ids.size());
+    for (const Cell& cell : cells) {
+        if (cell.first_child >= 0) continue;
+        for (uint32_t ti : cell.tris) {
             if (tri_map[ti] >= 0) continue;
             tri_map[ti] = int32_t(out.triangles.size());
             out.triangles.push_back(kept[ti]);
         }
     }
     // Node table: 8 child slots for inner nodes, -1-terminated lists for leaves.
-    std::vector<int64_t> start(b.nodes.size(), -1);
-    for (int32_t n : order) {
+    std::vector<int64_t> start(cells.size(), -1);
+    for (size_t n = 0; n < cells.size(); ++n) {
         start[n] = int64_t(out.octree_data.size());
-        if (b.nodes[n].first_child < 0) {
-            for (uint32_t ti : b.nodes[n].tris) out.octree_data.push_back(tri_map[ti]);
+        if (cells[n].first_child < 0) {
+            for (uint32_t ti : cells[n].tris) out.octree_data.push_back(tri_map[ti]);
             out.octree_data.push_back(-1);
         } else {
             for (int o = 0; o < 8; ++o) out.octree_data.push_back(0);
         }
         if (out.octree_data.size() > size_t(INT32_MAX)) throw std::runtime_error("Octree is too large.");
     }
-    for (int32_t n : order) {
-        if (b.nodes[n].first_child < 0) continue;
+    for (size_t n = 0; n < cells.size(); ++n) {
+        if (cells[n].first_child < 0) continue;
         for (int o = 0; o < 8; ++o) {
-            const int32_t c = b.nodes[n].first_child + o;
+            const size_t c = size_t(cells[n].first_child) + o;
             int32_t v = int32_t(start[c]);
-            if (b.nodes[c].first_child < 0) v = -v;
+            if (cells[c].first_child < 0) v = -v;
             out.octree_data[size_t(start[n]) + o] = v;
         }
     }
