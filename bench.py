@@ -42,6 +42,25 @@ PER_PIXEL = 100
 ENERGY = 500.0
 WORKLOAD = "grating 256x256 px x 100 primaries @ 500 eV (6,553,600 primaries), 5,136 triangles, Si-like Kieft tables"
 
+# Scans the bench can run: the grating line scan (the headline workload) and
+# the rough-slab scan with mixed beam energies.
+WORKLOADS = {
+    "grating": dict(nx=256, ny=256, per_pixel=100, energy=500.0, energies=None, spacing=1.0,
+                    origin=(-128.0, -128.0), z_start=75.0, desc=WORKLOAD),
+    "rough": dict(nx=512, ny=512, per_pixel=20, energy=1000.0, energies=[300.0, 1000.0, 3000.0, 5000.0],
+                  spacing=1000.0 / 512, origin=(-500.0, -500.0), z_start=25.0,
+                  desc="rough slab: 512x512 Gaussian height field (RMS 3 nm, correlation 10 nm) over 1 um, "
+                       "526,334 triangles; 512x512 px x 20 primaries (5,242,880) at E uniform over "
+                       "{300, 1000, 3000, 5000} eV, Si-like Kieft tables"),
+}
+
+
+def configure(args):
+    """Point the module's scan constants at the chosen workload."""
+    global NX, NY, PER_PIXEL, ENERGY, WORKLOAD
+    w = WORKLOADS[args.workload]
+    NX, NY, PER_PIXEL, ENERGY, WORKLOAD = w["nx"], w["ny"], w["per_pixel"], w["energy"], w["desc"]
+
 
 def workload_name(args):
     if args.inelastic == "penn":
@@ -89,13 +108,15 @@ def barrier(dist):
         dist.barrier()
 
 
-def make_workload(tmp, rank=0, rows=None):
+def make_workload(tmp, rank=0, rows=None, workload="grating"):
     from nebula_b200 import formats, generators as g
+    w = WORKLOADS[workload]
     mat = g.make_material(os.path.join(tmp, "si.mat"))
-    tris = g.grating_geometry()
-    tri_path = os.path.join(tmp, "grating.tri")
+    tris = g.grating_geometry() if workload == "grating" else g.rough_geometry(512)
+    tri_path = os.path.join(tmp, workload + ".tri")
     formats.write_tri(tri_path, tris)
-    recs = g.scan_beam(NX, NY, PER_PIXEL, ENERGY, seed=1000 + rank, rows=rows)
+    recs = g.scan_beam(w["nx"], w["ny"], w["per_pixel"], w["energy"], spacing=w["spacing"], origin=w["origin"],
+                       z_start=w["z_start"], seed=1000 + rank, energies=w["energies"], rows=rows)
     return mat, tris, tri_path, recs
 
 
@@ -200,8 +221,8 @@ def cpu_baseline(tri_path, mat_path, recs, tmp, rows=16, penn=False):
     _, st, secs = oracle.ref_run(tri_path, pri, [mat_path], threads=cores, count_events=True, penn=penn)
     ev = st["n_intersect"] + st["n_elastic"] + st["n_inelastic"]
     return {"value": ev / secs, "unit": "events/s", "cores": cores, "kind": "reference",
-            "sample": "%d pixel rows x 256 px x 100 primaries = %d primaries (%d events) in %.2f s"
-                      % (rows, len(sub), ev, secs),
+            "sample": "%d pixel rows x %d px x %d primaries = %d primaries (%d events) in %.2f s"
+                      % (rows, NX, PER_PIXEL, len(sub), ev, secs),
             "primaries_per_s": st["n_primaries"] / secs}
 
 
@@ -216,7 +237,7 @@ def run_reference(args):
             print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref reference library not built"}))
             return 0
         from nebula_b200 import formats
-        mat, tris, tri_path, recs = make_workload(tmp)
+        mat, tris, tri_path, recs = make_workload(tmp, workload=args.workload)
         rows = 4
         sub = recs[recs["py"] < rows]
         pri = os.path.join(tmp, "ref_step.pri")
@@ -302,7 +323,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="nbx", choices=["nbx", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--rows", type=int, default=NY, help="pixel rows of the scan (profiling runs use fewer)")
+    ap.add_argument("--workload", default="grating", choices=sorted(WORKLOADS),
+                    help="grating line scan (headline) or rough slab with mixed energies")
+    ap.add_argument("--rows", type=int, default=0, help="pixel rows of the scan (0: all; profiling runs use fewer)")
     ap.add_argument("--variant", type=int, default=0, help="transport variant 2/3/4/7 (0: autotune)")
     ap.add_argument("--block", type=int, default=0, help="threads per block with --variant (0: 128)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-roulette FOM comparison")
@@ -311,6 +334,9 @@ def main():
     ap.add_argument("--inelastic", default="kieft", choices=["kieft", "penn"],
                     help="inelastic model: Kieft & Bosch (the headline workload) or full Penn (the reference's stock build)")
     args = ap.parse_args()
+    configure(args)
+    if args.rows <= 0:
+        args.rows = NY
     if args.impl == "reference":
         return run_reference(args)
 
@@ -319,7 +345,8 @@ def main():
     import nebula_b200 as nb
 
     tmp = tempfile.mkdtemp(prefix="nbx_bench_")
-    mat, tris, tri_path, recs = make_workload(tmp, rank, rows=None if args.rows >= NY else range(args.rows))
+    mat, tris, tri_path, recs = make_workload(tmp, rank, rows=None if args.rows >= NY else range(args.rows),
+                                              workload=args.workload)
     ctx = nb.setup(tris, [mat], device=local, seed=0x78C7E39B + rank, inelastic=args.inelastic)
     n = len(recs)
     prim = np.zeros((n, 7), np.float32)
@@ -414,7 +441,8 @@ def main():
     h2d = n * 7 * 4 + n * 4
     d2h = NX * NY * 5 * 8
 
-    learned = None if args.no_learned else learned_fom(args, tris, mat, local, rank, prim, tags, mean_se, var_primary,
+    # the network's surface map and training scan are set up for the grating
+    learned = None if (args.no_learned or args.workload != "grating") else learned_fom(args, tris, mat, local, rank, prim, tags, mean_se, var_primary,
                                                        fom)
 
     line = None
@@ -424,7 +452,7 @@ def main():
         achieved = events * b_event / (sum(dev_ms) / 1000.0) / 1e9
         traffic = None
         tp = os.path.join(ROOT, "profiles", "transport_kernel_traffic.json")
-        if os.path.exists(tp) and args.inelastic == "kieft":   # captured on the Kieft workload
+        if os.path.exists(tp) and args.inelastic == "kieft" and args.workload == "grating":   # captured there
             with open(tp) as f:
                 traffic = json.load(f).get("dram_bytes_per_launch")
         cpu = None if args.no_cpu_baseline else cpu_baseline(tri_path, mat, recs, tmp, penn=args.inelastic == "penn")
