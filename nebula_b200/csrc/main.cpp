@@ -106,6 +106,64 @@ int die(nbx_ctx* ctx, int rc, const char* what) {
     return 1;
 }
 
+// Counts of the reference loader's warnings (io/load_pri_file.cpp:120-176).
+struct PriWarnings {
+    const nbx_octree* oct;
+    float max_energy;
+    uint64_t outside = 0, low = 0, high = 0, dir0 = 0;
+    void add(const nbx_record* pri, uint64_t n) {
+        const float eps = 10 * 1.1920928955078125e-07f;
+        for (uint64_t i = 0; i < n; ++i) {
+            const nbx_record& r = pri[i];
+            bool inside = true;
+            for (int k = 0; k < 3; ++k)
+                inside = inside && r.pos[k] > oct->center[k] - oct->halfsize[k] &&
+                         r.pos[k] < oct->center[k] + oct->halfsize[k];
+            outside += !inside;
+            low += !(r.E > eps);
+            high += r.E > max_energy;
+            dir0 += !(std::fabs(r.dir[0]) > eps || std::fabs(r.dir[1]) > eps || std::fabs(r.dir[2]) > eps);
+        }
+    }
+    void print() const {
+        if (outside) std::fprintf(stderr, "WARNING: %llu primary electrons starting outside geometry.\n", (unsigned long long)outside);
+        if (low) std::fprintf(stderr, "WARNING: %llu primary electrons starting with low kinetic energy.\n", (unsigned long long)low);
+        if (high)
+            std::fprintf(stderr, "WARNING: %llu primary electrons starting with kinetic energy higher than what is "
+                                 "available in the material files. Limit is %g keV.\n", (unsigned long long)high, max_energy / 1000);
+        if (dir0) std::fprintf(stderr, "WARNING: %llu primary electrons start with unphysical direction vector.\n", (unsigned long long)dir0);
+    }
+};
+
+// Primaries either read whole (for sorting) or streamed from the file in
+// batches; batch(first, n) returns records first .. first + n - 1.
+struct PriSource {
+    nbx_record* all = nullptr;
+    uint64_t count = 0;
+    FILE* f = nullptr;
+    std::vector<nbx_record> buf;
+    bool open(const std::string& path, bool whole) {
+        if (whole) return nbx_load_pri(path.c_str(), &all, &count) == NBX_OK && count > 0;
+        f = std::fopen(path.c_str(), "rb");
+        if (!f) return false;
+        if (std::fseek(f, 0, SEEK_END) != 0) return false;
+        const long long size = std::ftell(f);
+        std::fseek(f, 0, SEEK_SET);
+        if (size <= 0 || size % 36 != 0) return false;   // "Unexpected end of primaries file"
+        count = uint64_t(size) / 36;
+        return true;
+    }
+    const nbx_record* batch(uint64_t first, uint64_t n) {
+        if (all) return all + first;
+        buf.resize(n);
+        return std::fread(buf.data(), 36, n, f) == n ? buf.data() : nullptr;
+    }
+    ~PriSource() {
+        if (all) nbx_free(all);
+        if (f) std::fclose(f);
+    }
+};
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -199,38 +257,25 @@ int main(int argc, char** argv) {
     }
     timer.stop("Loading materials");
 
-    // Primaries (gpu_main.cu:352-380, io/load_pri_file.cpp:134-246)
+    // Primaries (gpu_main.cu:352-380, io/load_pri_file.cpp:72-229).  Without
+    // --sort-primaries the file is streamed batch by batch (a 7.5 GB scan
+    // never sits in host memory); the reference's warnings are counted as the
+    // batches go by and printed once the last batch is read.  Sorting needs
+    // every primary, so --sort-primaries loads the whole file first.
     std::fprintf(stderr, "Loading primary electrons...\n");
     timer.start();
-    nbx_record* pri = nullptr;
-    uint64_t n_pri = 0;
-    rc = nbx_load_pri(p.positional[1].c_str(), &pri, &n_pri);
-    if (rc != NBX_OK || n_pri == 0) {
+    PriWarnings warn{oct, max_energy};
+    PriSource src;
+    if (!src.open(p.positional[1], sort_primaries)) {
         std::fprintf(stderr, "Error: could not load primary electrons!\n");
         p.usage(std::cerr);
         return 1;
     }
-    {
-        const float eps = 10 * 1.1920928955078125e-07f;
-        uint64_t outside = 0, low = 0, high = 0, dir0 = 0;
-        for (uint64_t i = 0; i < n_pri; ++i) {
-            const nbx_record& r = pri[i];
-            bool inside = true;
-            for (int k = 0; k < 3; ++k)
-                inside = inside && r.pos[k] > oct->center[k] - oct->halfsize[k] && r.pos[k] < oct->center[k] + oct->halfsize[k];
-            outside += !inside;
-            low += !(r.E > eps);
-            high += r.E > max_energy;
-            dir0 += !(std::fabs(r.dir[0]) > eps || std::fabs(r.dir[1]) > eps || std::fabs(r.dir[2]) > eps);
-        }
-        if (outside) std::fprintf(stderr, "WARNING: %llu primary electrons starting outside geometry.\n", (unsigned long long)outside);
-        if (low) std::fprintf(stderr, "WARNING: %llu primary electrons starting with low kinetic energy.\n", (unsigned long long)low);
-        if (high)
-            std::fprintf(stderr, "WARNING: %llu primary electrons starting with kinetic energy higher than what is "
-                                 "available in the material files. Limit is %g keV.\n", (unsigned long long)high, max_energy / 1000);
-        if (dir0) std::fprintf(stderr, "WARNING: %llu primary electrons start with unphysical direction vector.\n", (unsigned long long)dir0);
-    }
+    const uint64_t n_pri = src.count;
     if (sort_primaries) {
+        nbx_record* pri = src.all;
+        warn.add(pri, n_pri);
+        warn.print();
         // Morton order of the start positions (io/load_pri_file.cpp:186-229)
         float vmin[3], vmax[3];
         for (int k = 0; k < 3; ++k) vmin[k] = vmax[k] = pri[0].pos[k];
@@ -310,12 +355,18 @@ int main(int argc, char** argv) {
     uint64_t done = 0;
     while (done < n_pri) {
         const uint64_t n = std::min(batch, n_pri - done);
+        const nbx_record* pri = src.batch(done, n);
+        if (!pri) {
+            std::fprintf(stderr, "Error: could not read primary electrons!\n");
+            return die(ctx, NBX_ERR_FORMAT, "primaries");
+        }
+        if (!sort_primaries) warn.add(pri, n);
         part.resize(n);
         tags.resize(n);
         for (uint64_t i = 0; i < n; ++i) {
-            std::memcpy(part[i].pos, pri[done + i].pos, 12);
-            std::memcpy(part[i].dir, pri[done + i].dir, 12);
-            part[i].E = pri[done + i].E;
+            std::memcpy(part[i].pos, pri[i].pos, 12);
+            std::memcpy(part[i].dir, pri[i].dir, 12);
+            part[i].E = pri[i].E;
             tags[i] = uint32_t(done + i);
         }
         uint64_t acc = 0;
@@ -330,8 +381,8 @@ int main(int argc, char** argv) {
                 std::memcpy(out[i].pos, det[i].pos, 12);
                 std::memcpy(out[i].dir, det[i].dir, 12);
                 out[i].E = det[i].E;
-                out[i].px = pri[det[i].tag].px;
-                out[i].py = pri[det[i].tag].py;
+                out[i].px = pri[det[i].tag - done].px;
+                out[i].py = pri[det[i].tag - done].py;
             }
             std::fwrite(out.data(), sizeof(nbx_record), got, detect_out);
         }
@@ -346,7 +397,8 @@ int main(int argc, char** argv) {
                 dep_out.resize(got);
                 for (uint64_t i = 0; i < got; ++i) {
                     const nbx_deposit& d = dep[i];
-                    dep_out[i] = {d.pos[0], d.pos[1], d.pos[2], d.E, d.dE, pri[d.tag].px, pri[d.tag].py};
+                    const nbx_record& r = pri[d.tag - done];
+                    dep_out[i] = {d.pos[0], d.pos[1], d.pos[2], d.E, d.dE, r.px, r.py};
                 }
                 std::fwrite(dep_out.data(), sizeof(DepositRecord), got, deposit_out);
             }
@@ -366,6 +418,10 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, " \rProgress %.2f%%", 100.0 * double(done) / double(n_pri));
     }
     std::fflush(stdout);
+    if (!sort_primaries) {
+        std::fprintf(stderr, "\n");
+        warn.print();
+    }
     if (energy_deposit) {
         if (detect_out != stdout) std::fclose(detect_out);
         if (deposit_out != stdout) std::fclose(deposit_out);
@@ -382,6 +438,5 @@ int main(int argc, char** argv) {
     nbx_destroy(ctx);
     for (auto* m : mats) nbx_material_free(m);
     nbx_octree_free(oct);
-    nbx_free(pri);
     return 0;
 }
