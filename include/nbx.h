@@ -268,8 +268,13 @@ int nbx_flush_detected(nbx_ctx* ctx, nbx_detected* out, uint64_t cap, uint64_t* 
 /* Detections per primary tag below / at-or-above 50 eV. */
 int nbx_get_tag_counts(nbx_ctx* ctx, uint64_t first_tag, uint64_t n, uint32_t* se, uint32_t* bse);
 /* Per-pixel FP64 yields: pixel_of_tag maps tags to [0, n_pixels); out has
- * n_pixels x 5 doubles {primaries, sum_se, sum_se^2, sum_bse, sum_bse^2}. */
+ * n_pixels x 5 doubles {primaries, sum_se, sum_se^2, sum_bse, sum_bse^2}.
+ * pixel_of_tag = NULL uses the map last given to nbx_set_pixel_map (n_tags
+ * must not exceed its length). */
 int nbx_pixel_yields(nbx_ctx* ctx, const uint32_t* pixel_of_tag, uint64_t n_tags, uint64_t n_pixels, double* out);
+/* Keep a tag -> pixel map on the device for later nbx_pixel_yields calls
+ * (a scan that repeats does not re-send it every time). */
+int nbx_set_pixel_map(nbx_ctx* ctx, const uint32_t* pixel_of_tag, uint64_t n_tags);
 /* Detected-energy histogram: n_bins bins of bin_width eV from 0. */
 int nbx_get_spectrum(nbx_ctx* ctx, uint64_t* counts, uint32_t n_bins, float* bin_width);
 int nbx_reset_tallies(nbx_ctx* ctx);
@@ -278,8 +283,9 @@ int nbx_reset_tallies(nbx_ctx* ctx);
  * 32-thread blocks over the whole capacity, drivers/gpu/gpu_driver.inl:64):
  * runs the given sample once per transport variant (2, 3, 4 resident
  * 256-thread blocks per SM, 7 resident 128-thread blocks) and block size
- * (256, 128), keeps the fastest, and resets the tallies.  Random streams of
- * later pushes are unaffected. */
+ * (256, 128) -- twice on the same random streams, timing the second pass --
+ * keeps the fastest, and resets the tallies.  Random streams of later pushes
+ * are unaffected. */
 int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n,
                  int32_t* blocks_per_sm, int32_t* block_size);
 

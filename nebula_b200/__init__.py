@@ -137,6 +137,7 @@ def lib():
         "nbx_flush_deposits": (C.c_int, [_vp, _vp, C.c_uint64, C.POINTER(C.c_uint64)]),
         "nbx_get_tag_counts": (C.c_int, [_vp, C.c_uint64, C.c_uint64, _vp, _vp]),
         "nbx_pixel_yields": (C.c_int, [_vp, _vp, C.c_uint64, C.c_uint64, _vp]),
+        "nbx_set_pixel_map": (C.c_int, [_vp, _vp, C.c_uint64]),
         "nbx_get_spectrum": (C.c_int, [_vp, _vp, C.c_uint32, C.POINTER(C.c_float)]),
         "nbx_reset_tallies": (C.c_int, [_vp]),
         "nbx_ray_query": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_uint64, _vp, _vp]),
@@ -285,6 +286,7 @@ class Context:
         cfg.inelastic_model = INELASTIC_MODELS.get(inelastic, inelastic)
         cfg.record_deposits, cfg.deposit_capacity = int(record_deposits), deposit_capacity
         self.h = _vp()
+        self._pixel_map_len = 0
         _check(L.nbx_create(C.byref(self.h), C.byref(cfg)))
         self.L = L
         self._keep = []
@@ -372,10 +374,22 @@ class Context:
         self._ck(self.L.nbx_get_tag_counts(self.h, first, n, _ptr(se), _ptr(bse)))
         return se, bse
 
-    def pixel_yields(self, pixel_of_tag: np.ndarray, n_pixels: int) -> np.ndarray:
+    def set_pixel_map(self, pixel_of_tag: np.ndarray):
         m = np.ascontiguousarray(pixel_of_tag, np.uint32)
-        out = np.zeros((n_pixels, 5), np.float64)
-        self._ck(self.L.nbx_pixel_yields(self.h, _ptr(m), len(m), n_pixels, _ptr(out)))
+        self._ck(self.L.nbx_set_pixel_map(self.h, _ptr(m), len(m)))
+        self._pixel_map_len = len(m)
+
+    def pixel_yields(self, pixel_of_tag, n_pixels: int, out=None) -> np.ndarray:
+        """Per-pixel sums; pixel_of_tag=None uses the map of set_pixel_map.
+        `out` (n_pixels x 5 float64, e.g. in pinned memory) is filled in place."""
+        if out is None:
+            out = np.zeros((n_pixels, 5), np.float64)
+        if pixel_of_tag is None:
+            self._ck(self.L.nbx_pixel_yields(self.h, None, self._pixel_map_len, n_pixels, _ptr(out)))
+        else:
+            m = np.ascontiguousarray(pixel_of_tag, np.uint32)
+            self._ck(self.L.nbx_pixel_yields(self.h, _ptr(m), len(m), n_pixels, _ptr(out)))
+            self._pixel_map_len = 0
         return out
 
     def spectrum(self, n_bins=20000):

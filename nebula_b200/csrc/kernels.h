@@ -78,6 +78,9 @@ struct TransportArgs {
     float* dep;
     unsigned long long* dep_cursor;   // records handed out (chunks of kDepositChunk)
     unsigned long long dep_capacity;  // records the buffer holds
+    // parked-ancestor stacks, 3 * kLocalStack float4 per launched thread
+    // (nullptr: a local-memory array)
+    float4* stack_mem;
 };
 
 // Deposit records: x, y, z, E_before, E_before - E_after, tag; unused slots of

@@ -137,7 +137,9 @@ struct nbx_ctx {
     DevBuf<uint32_t> sample_count;
     uint64_t sample_cap = 0;
     DevBuf<float> se_w, bse_w;
+    DevBuf<float4> stack_mem;     // transport parked-ancestor stacks (grow-only)
     DevBuf<uint32_t> yield_map;   // nbx_pixel_yields work buffers (grow-only)
+    uint64_t pixel_map_len = 0;    // tags covered by a map from nbx_set_pixel_map
     DevBuf<double> yield_out;
     uint64_t rec_cap = 0;
     // stats
@@ -704,6 +706,9 @@ int nbx_run(nbx_ctx* ctx) {
         }
         const int bpsm = nbx::transport_max_blocks_per_sm(ctx->block, ctx->variant, mode);
         const int grid = ctx->sms * bpsm;
+        // parked-ancestor stacks of the launched threads (grow-only)
+        ctx->stack_mem.ensure(uint64_t(grid) * uint64_t(ctx->block) * 3 * nbx::kLocalStack);
+        a.stack_mem = ctx->stack_mem.p;
 
         ck(cudaEventRecord(ctx->ev0, ctx->stream), "event");
         int g = 0;
@@ -831,15 +836,32 @@ int nbx_get_tag_counts(nbx_ctx* ctx, uint64_t first, uint64_t n, uint32_t* se, u
     });
 }
 
-int nbx_pixel_yields(nbx_ctx* ctx, const uint32_t* pixel_of_tag, uint64_t n_tags, uint64_t n_pixels, double* out) {
-    if (!ctx || !pixel_of_tag || !out) return NBX_ERR_ARG;
-    if (n_tags > ctx->n_tags) return fail(ctx, NBX_ERR_ARG, "n_tags beyond the tallied range");
+int nbx_set_pixel_map(nbx_ctx* ctx, const uint32_t* pixel_of_tag, uint64_t n_tags) {
+    if (!ctx || (n_tags && !pixel_of_tag)) return NBX_ERR_ARG;
     return guarded(ctx, [&] {
         ctx->yield_map.ensure(std::max<uint64_t>(n_tags, 1));
+        ck(cudaMemcpyAsync(ctx->yield_map.p, pixel_of_tag, 4 * n_tags, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+        ck(cudaStreamSynchronize(ctx->stream), "sync");
+        ctx->pixel_map_len = n_tags;
+        return NBX_OK;
+    });
+}
+
+int nbx_pixel_yields(nbx_ctx* ctx, const uint32_t* pixel_of_tag, uint64_t n_tags, uint64_t n_pixels, double* out) {
+    if (!ctx || !out) return NBX_ERR_ARG;
+    if (n_tags > ctx->n_tags) return fail(ctx, NBX_ERR_ARG, "n_tags beyond the tallied range");
+    if (!pixel_of_tag && n_tags > ctx->pixel_map_len)
+        return fail(ctx, NBX_ERR_STATE, "no stored pixel map covering n_tags (nbx_set_pixel_map)");
+    return guarded(ctx, [&] {
+        if (pixel_of_tag) {
+            ctx->yield_map.ensure(std::max<uint64_t>(n_tags, 1));
+            ctx->pixel_map_len = 0;   // the stored map is overwritten
+        }
         ctx->yield_out.ensure(std::max<uint64_t>(5 * n_pixels, 1));
         uint32_t* map = ctx->yield_map.p;
         double* res = ctx->yield_out.p;
-        ck(cudaMemcpyAsync(map, pixel_of_tag, 4 * n_tags, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+        if (pixel_of_tag)
+            ck(cudaMemcpyAsync(map, pixel_of_tag, 4 * n_tags, cudaMemcpyHostToDevice, ctx->stream), "H2D");
         ck(cudaMemsetAsync(res, 0, 8 * 5 * n_pixels, ctx->stream), "memset");
         ck(nbx::launch_pixel_yields(ctx->se_count.p, ctx->bse_count.p, map, n_tags, n_pixels, res, ctx->stream),
            "pixel yields");
@@ -1049,9 +1071,14 @@ int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* ta
             ctx->variant = v;
             ctx->block = b;
             ctx->bpsm = nbx::transport_max_blocks_per_sm(b, v);
-            int rc = nbx_push(ctx, particles, tags, n, nullptr);
-            if (rc == NBX_OK) rc = nbx_run(ctx);
-            if (rc != NBX_OK) return rc;
+            // Twice on the same random streams: the first pass also pays the
+            // kernel's one-time module load, the second is the timing kept.
+            for (int rep = 0; rep < 2; ++rep) {
+                ctx->uid_next = uid_save;
+                int rc = nbx_push(ctx, particles, tags, n, nullptr);
+                if (rc == NBX_OK) rc = nbx_run(ctx);
+                if (rc != NBX_OK) return rc;
+            }
             if (ctx->last_run_ms < best) {
                 best = ctx->last_run_ms;
                 best_v = v;

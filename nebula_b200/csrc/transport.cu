@@ -78,6 +78,48 @@ struct Extra {
     uint32_t flags;   // bit 0: sub-cascade produced a detected SE; bit 1: already split
 };
 
+// Parked ancestors of a thread's cascade, in global memory laid out per
+// thread (kLocalStack entries of three float4: (pos, E), (dir, material),
+// (uid, step, last triangle)).  A local-memory array interleaves threads word
+// by word, so lanes parked at different depths scatter each of an entry's 13
+// words into its own sector; here an entry is 48 contiguous bytes (two
+// sectors, three 16-byte accesses).  The tag is not stored: every electron of
+// a thread's cascade carries its primary's tag.  base == nullptr: use the
+// local array instead (callers without a stack buffer).
+struct ParkedStack {
+    float4* base;
+    __device__ __forceinline__ void put(int i, const dev::Electron& e, dev::Electron* local) const {
+        if (base) {
+            float4* p = base + 3 * i;
+            p[0] = make_float4(e.px, e.py, e.pz, e.E);
+            p[1] = make_float4(e.dx, e.dy, e.dz, __int_as_float(e.mat));
+            p[2] = make_float4(__uint_as_float(uint32_t(e.uid)), __uint_as_float(uint32_t(e.uid >> 32)),
+                               __uint_as_float(e.step), __int_as_float(e.last_tri));
+        } else {
+            local[i] = e;
+        }
+    }
+    __device__ __forceinline__ void get(int i, dev::Electron& e, const dev::Electron* local) const {
+        if (base) {
+            const float4* p = base + 3 * i;
+            const float4 a = p[0], b = p[1], c = p[2];
+            e.px = a.x;
+            e.py = a.y;
+            e.pz = a.z;
+            e.E = a.w;
+            e.dx = b.x;
+            e.dy = b.y;
+            e.dz = b.z;
+            e.mat = __float_as_int(b.w);
+            e.uid = uint64_t(__float_as_uint(c.x)) | (uint64_t(__float_as_uint(c.y)) << 32);
+            e.step = __float_as_uint(c.z);
+            e.last_tri = __float_as_int(c.w);
+        } else {
+            e = local[i];
+        }
+    }
+};
+
 __device__ __forceinline__ uint32_t mix32(uint64_t x) {
     x ^= x >> 33;
     x *= 0xFF51AFD7ED558CCDull;
@@ -118,6 +160,8 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
     // parent is parked here and the secondary is simulated at once, so the
     // stack only ever holds the current electron's ancestors.
     dev::Electron stack[kLocalStack];
+    const ParkedStack ps{a.stack_mem ? a.stack_mem + (size_t(blockIdx.x) * blockDim.x + threadIdx.x) * 3 * kLocalStack
+                                     : nullptr};
     Extra ex{1.0f, -1, 0u};
     Extra exs[kExtra ? kLocalStack : 1];
     int sp = 0;
@@ -136,7 +180,7 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
     for (;;) {
         if (!alive && !drained) {
             if (sp > 0) {
-                e = stack[--sp];
+                ps.get(--sp, e, stack);
                 if constexpr (kExtra) {
                     ex = exs[sp];
                     ex.flags |= carry_hit;
@@ -210,8 +254,9 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                             }
                         } else if (pr > a.split_threshold && ex.w > 2.0f * target && sp < kLocalStack) {
                             ex.w *= 0.5f;
-                            stack[sp] = e;
-                            stack[sp].uid = dev::secondary_uid(e.uid ^ 0x5DEECE66Dull, e.step);
+                            dev::Electron twin = e;
+                            twin.uid = dev::secondary_uid(e.uid ^ 0x5DEECE66Dull, e.step);
+                            ps.put(sp, twin, stack);
                             exs[sp] = ex;
                             ++sp;
                             ++c_split;
@@ -285,7 +330,7 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                 ++c_steps;
                 ++c_term;
             } else if (sp < kLocalStack) {
-                stack[sp] = e;
+                ps.put(sp, e, stack);
                 if constexpr (kExtra) exs[sp] = ex;
                 ++sp;
                 e = se;

@@ -355,3 +355,26 @@ def test_run_conservation_and_edge_cases(inputs, oracle_built):
     assert se[0] == 0 and bse[0] == 0
     assert bse[2] == 1               # 1 keV straight up: detected as BSE-range energy
     ctx.close()
+
+
+def test_pixel_yields_match_tag_counts(inputs):
+    """Per-pixel FP64 sums against the per-tag counts, with the map passed
+    per call and with the stored map of nbx_set_pixel_map."""
+    recs = g.scan_beam(8, 8, 50, 500.0, origin=(-4.0, -4.0), z_start=5.0, seed=8)
+    n = len(recs)
+    ctx = nb.setup(inputs["cube"], [inputs["si"]], device=0, seed=4)
+    s, se, bse = _run_gpu(ctx, recs)
+    pix = (recs["py"] * 8 + recs["px"]).astype(np.uint32)
+    a = ctx.pixel_yields(pix, 64)
+    ctx.set_pixel_map(pix)
+    b = ctx.pixel_yields(None, 64)
+    assert np.array_equal(a, b)
+    ref = np.zeros((64, 5))
+    np.add.at(ref[:, 0], pix, 1.0)
+    np.add.at(ref[:, 1], pix, se)
+    np.add.at(ref[:, 2], pix, se * se)
+    np.add.at(ref[:, 3], pix, bse)
+    np.add.at(ref[:, 4], pix, bse * bse)
+    assert np.array_equal(a, ref)
+    assert a[:, 0].sum() == n
+    ctx.close()
