@@ -4,7 +4,8 @@
 // operation by operation; the translation unit is compiled with
 // -fmad=false and IEEE division/square root, so octree ray queries and table
 // lookups are bit-identical to the reference CPU path.  Transcendentals are
-// CUDA's accurate (non-intrinsic) logf/expf/expm1f/sincospif.
+// CUDA's accurate logf/expf/expm1f/sincospif, except the free-path sampling
+// of step() (hardware approximations, see there).
 #pragma once
 
 #include <cstdint>
@@ -683,22 +684,28 @@ __device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, E
     float logE = 0;
     if (e.mat >= 0) {
         const Material& m = P.mat[e.mat];
-        logE = logf(e.E);
+        // The free-path sampling uses the hardware log2/exp2 approximations
+        // (__logf / __expf: a few ulp, 2^-21 absolute for log near 1): the
+        // paths only enter the statistics, and the table lookups that follow
+        // are exact functions of the log E they are given.  A path that the
+        // approximation would make slightly negative (U within 2^-21 of 1) is
+        // taken as 0.
+        logE = __logf(e.E);
         dist = __int_as_float(0x7f800000);
         // Mean free path exp(-log imfp) rather than 1 / exp(log imfp): the
         // same exponential sampling (scatter_list.h:106-132, random.h
         // exponential) without a division per mechanism.
         {
-            const float mfp = expf(-table1d_get(m.in_imfp, logE));
-            const float path = -mfp * logf(u01(r0.x));
+            const float mfp = __expf(-table1d_get(m.in_imfp, logE));
+            const float path = fmaxf(-mfp * __logf(u01(r0.x)), 0.0f);
             if (path < dist) {
                 type = 1;
                 dist = path;
             }
         }
         {
-            const float mfp = expf(-table1d_get(m.el_imfp, logE));
-            const float path = -mfp * logf(u01(r0.y));
+            const float mfp = __expf(-table1d_get(m.el_imfp, logE));
+            const float path = fmaxf(-mfp * __logf(u01(r0.y)), 0.0f);
             if (path < dist) {
                 type = 2;
                 dist = path;
