@@ -268,13 +268,26 @@ int nbx_flush_detected(nbx_ctx* ctx, nbx_detected* out, uint64_t cap, uint64_t* 
 /* Detections per primary tag below / at-or-above 50 eV. */
 int nbx_get_tag_counts(nbx_ctx* ctx, uint64_t first_tag, uint64_t n, uint32_t* se, uint32_t* bse);
 /* Per-pixel FP64 yields: pixel_of_tag maps tags to [0, n_pixels); out has
- * n_pixels x 5 doubles {primaries, sum_se, sum_se^2, sum_bse, sum_bse^2}.
+ * n_pixels x 5 doubles {primaries, sum_se, sum_se^2, sum_bse, sum_bse^2},
+ * over per-primary counts (weighted counts when the context is in learned
+ * mode, so sum_se^2 is the sum of squared weights per primary).
  * pixel_of_tag = NULL uses the map last given to nbx_set_pixel_map (n_tags
  * must not exceed its length). */
 int nbx_pixel_yields(nbx_ctx* ctx, const uint32_t* pixel_of_tag, uint64_t n_tags, uint64_t n_pixels, double* out);
 /* Keep a tag -> pixel map on the device for later nbx_pixel_yields calls
- * (a scan that repeats does not re-send it every time). */
+ * (a scan that repeats does not re-send it every time) and for the per-pixel
+ * spectra. */
 int nbx_set_pixel_map(nbx_ctx* ctx, const uint32_t* pixel_of_tag, uint64_t n_tags);
+/* Per-pixel exit spectra, tallied on the device during runs (no reference
+ * counterpart; the reference writes every detected electron and bins on the
+ * host): n_bins bins of bin_width eV from 0 for each of n_pixels pixels,
+ * through the map of nbx_set_pixel_map (detections of tags outside it, and
+ * energies past the last bin, are not binned).  Counts in plain mode, weights
+ * in learned mode.  n_pixels = 0 turns them off.  nbx_reset_tallies clears
+ * them. */
+int nbx_enable_pixel_spectra(nbx_ctx* ctx, uint64_t n_pixels, int32_t n_bins, float bin_width);
+/* Copy out n_pixels x n_bins floats, pixel-major. */
+int nbx_get_pixel_spectra(nbx_ctx* ctx, float* out);
 /* Detected-energy histogram: n_bins bins of bin_width eV from 0. */
 int nbx_get_spectrum(nbx_ctx* ctx, uint64_t* counts, uint32_t n_bins, float* bin_width);
 int nbx_reset_tallies(nbx_ctx* ctx);

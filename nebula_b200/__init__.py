@@ -138,6 +138,8 @@ def lib():
         "nbx_get_tag_counts": (C.c_int, [_vp, C.c_uint64, C.c_uint64, _vp, _vp]),
         "nbx_pixel_yields": (C.c_int, [_vp, _vp, C.c_uint64, C.c_uint64, _vp]),
         "nbx_set_pixel_map": (C.c_int, [_vp, _vp, C.c_uint64]),
+        "nbx_enable_pixel_spectra": (C.c_int, [_vp, C.c_uint64, C.c_int32, C.c_float]),
+        "nbx_get_pixel_spectra": (C.c_int, [_vp, _vp]),
         "nbx_get_spectrum": (C.c_int, [_vp, _vp, C.c_uint32, C.POINTER(C.c_float)]),
         "nbx_reset_tallies": (C.c_int, [_vp]),
         "nbx_ray_query": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_uint64, _vp, _vp]),
@@ -378,6 +380,15 @@ class Context:
         m = np.ascontiguousarray(pixel_of_tag, np.uint32)
         self._ck(self.L.nbx_set_pixel_map(self.h, _ptr(m), len(m)))
         self._pixel_map_len = len(m)
+
+    def enable_pixel_spectra(self, n_pixels, n_bins=200, bin_width=0.5):
+        self._ck(self.L.nbx_enable_pixel_spectra(self.h, n_pixels, n_bins, bin_width))
+        self._spec_shape = (n_pixels, n_bins)
+
+    def pixel_spectra(self) -> np.ndarray:
+        out = np.zeros(self._spec_shape, np.float32)
+        self._ck(self.L.nbx_get_pixel_spectra(self.h, _ptr(out)))
+        return out
 
     def pixel_yields(self, pixel_of_tag, n_pixels: int, out=None) -> np.ndarray:
         """Per-pixel sums; pixel_of_tag=None uses the map of set_pixel_map.

@@ -81,6 +81,14 @@ struct TransportArgs {
     // parked-ancestor stacks, 3 * kLocalStack float4 per launched thread
     // (nullptr: a local-memory array)
     float4* stack_mem;
+    // per-pixel exit spectra (nullptr: off): pix_spec[pixel * pix_bins + bin]
+    // counts (weights in learned mode) of detections, pixel = pixel_of_tag[tag]
+    float* pix_spec;
+    const uint32_t* pixel_of_tag;   // n_map entries
+    uint64_t n_map;
+    uint64_t n_pixels;
+    int pix_bins;
+    float pix_inv_width;
 };
 
 // Deposit records: x, y, z, E_before, E_before - E_after, tag; unused slots of
@@ -125,8 +133,10 @@ cudaError_t launch_philox(const uint32_t* ctr, const uint32_t* key, uint64_t n, 
 // electrons: 56-byte nbx_electron records
 cudaError_t launch_step_query(const dev::Physics& P, void* electrons, uint64_t n, int32_t* status, int32_t* event,
                               void* secondaries, int32_t* has_se, cudaStream_t s);
-cudaError_t launch_pixel_yields(const uint32_t* se, const uint32_t* bse, const uint32_t* pixel_of_tag,
-                                uint64_t n_tags, uint64_t n_pixels, double* out, cudaStream_t s);
+// se_w / bse_w: per-tag weights (learned mode) or nullptr for the counts.
+cudaError_t launch_pixel_yields(const uint32_t* se, const uint32_t* bse, const float* se_w, const float* bse_w,
+                                const uint32_t* pixel_of_tag, uint64_t n_tags, uint64_t n_pixels, double* out,
+                                cudaStream_t s);
 // Allocation-free transport on the file-scope scratch of transport.cu
 // (see nbx_run_noalloc).  Returns 0 or an NBX_ERR_* code with *err set.
 constexpr uint32_t kNoAllocMaxPrimaries = 65536;

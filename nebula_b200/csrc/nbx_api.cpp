@@ -140,6 +140,10 @@ struct nbx_ctx {
     DevBuf<float4> stack_mem;     // transport parked-ancestor stacks (grow-only)
     DevBuf<uint32_t> yield_map;   // nbx_pixel_yields work buffers (grow-only)
     uint64_t pixel_map_len = 0;    // tags covered by a map from nbx_set_pixel_map
+    DevBuf<float> pix_spec;        // per-pixel exit spectra (nbx_enable_pixel_spectra)
+    uint64_t spec_pixels = 0;
+    int spec_bins = 0;
+    float spec_width = 0;
     DevBuf<double> yield_out;
     uint64_t rec_cap = 0;
     // stats
@@ -676,6 +680,14 @@ int nbx_run(nbx_ctx* ctx) {
         a.rec_count = ctx->rec_count.p;
         a.rec_capacity = uint32_t(std::min<uint64_t>(ctx->rec_cap, 0xFFFFFFF0ull));
         a.hist = ctx->hist.p;
+        if (ctx->spec_pixels) {
+            a.pix_spec = ctx->pix_spec.p;
+            a.pixel_of_tag = ctx->yield_map.p;
+            a.n_map = ctx->pixel_map_len;
+            a.n_pixels = ctx->spec_pixels;
+            a.pix_bins = ctx->spec_bins;
+            a.pix_inv_width = 1.0f / ctx->spec_width;
+        }
         a.n_bins = kHistBins;
         a.inv_bin_width = 1.0f / kHistWidth;
         a.smap = ctx->smap;
@@ -836,6 +848,32 @@ int nbx_get_tag_counts(nbx_ctx* ctx, uint64_t first, uint64_t n, uint32_t* se, u
     });
 }
 
+int nbx_enable_pixel_spectra(nbx_ctx* ctx, uint64_t n_pixels, int32_t n_bins, float bin_width) {
+    if (!ctx || n_bins < 0 || (n_pixels && (n_bins == 0 || !(bin_width > 0)))) return NBX_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->pix_spec.release();
+        ctx->spec_pixels = 0;
+        if (n_pixels == 0) return NBX_OK;
+        ctx->pix_spec.alloc(n_pixels * uint64_t(n_bins));
+        ck(cudaMemset(ctx->pix_spec.p, 0, sizeof(float) * n_pixels * uint64_t(n_bins)), "memset");
+        ctx->spec_pixels = n_pixels;
+        ctx->spec_bins = n_bins;
+        ctx->spec_width = bin_width;
+        return NBX_OK;
+    });
+}
+
+int nbx_get_pixel_spectra(nbx_ctx* ctx, float* out) {
+    if (!ctx || !out) return NBX_ERR_ARG;
+    if (!ctx->spec_pixels) return fail(ctx, NBX_ERR_STATE, "per-pixel spectra not enabled");
+    return guarded(ctx, [&] {
+        ck(cudaMemcpyAsync(out, ctx->pix_spec.p, sizeof(float) * ctx->spec_pixels * uint64_t(ctx->spec_bins),
+                           cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        ck(cudaStreamSynchronize(ctx->stream), "sync");
+        return NBX_OK;
+    });
+}
+
 int nbx_set_pixel_map(nbx_ctx* ctx, const uint32_t* pixel_of_tag, uint64_t n_tags) {
     if (!ctx || (n_tags && !pixel_of_tag)) return NBX_ERR_ARG;
     return guarded(ctx, [&] {
@@ -863,7 +901,9 @@ int nbx_pixel_yields(nbx_ctx* ctx, const uint32_t* pixel_of_tag, uint64_t n_tags
         if (pixel_of_tag)
             ck(cudaMemcpyAsync(map, pixel_of_tag, 4 * n_tags, cudaMemcpyHostToDevice, ctx->stream), "H2D");
         ck(cudaMemsetAsync(res, 0, 8 * 5 * n_pixels, ctx->stream), "memset");
-        ck(nbx::launch_pixel_yields(ctx->se_count.p, ctx->bse_count.p, map, n_tags, n_pixels, res, ctx->stream),
+        const bool weighted = ctx->mode == nbx::kModeLearned;
+        ck(nbx::launch_pixel_yields(ctx->se_count.p, ctx->bse_count.p, weighted ? ctx->se_w.p : nullptr,
+                                    weighted ? ctx->bse_w.p : nullptr, map, n_tags, n_pixels, res, ctx->stream),
            "pixel yields");
         ck(cudaMemcpyAsync(out, res, 8 * 5 * n_pixels, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
         ck(cudaStreamSynchronize(ctx->stream), "sync");
@@ -888,6 +928,9 @@ int nbx_reset_tallies(nbx_ctx* ctx) {
         ck(cudaMemsetAsync(ctx->counters.p, 0, 8 * nbx::kNumCounters, ctx->stream), "memset");
         ck(cudaMemsetAsync(ctx->hist.p, 0, 8ull * kHistBins, ctx->stream), "memset");
         ck(cudaMemsetAsync(ctx->rec_count.p, 0, 4, ctx->stream), "memset");
+        if (ctx->spec_pixels)
+            ck(cudaMemsetAsync(ctx->pix_spec.p, 0, sizeof(float) * ctx->spec_pixels * uint64_t(ctx->spec_bins),
+                               ctx->stream), "memset");
         if (ctx->n_tags) {
             ck(cudaMemsetAsync(ctx->se_count.p, 0, 4 * ctx->n_tags, ctx->stream), "memset");
             ck(cudaMemsetAsync(ctx->bse_count.p, 0, 4 * ctx->n_tags, ctx->stream), "memset");

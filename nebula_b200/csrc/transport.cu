@@ -380,6 +380,16 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                 bin = bin < 0 ? 0 : (bin >= a.n_bins ? a.n_bins - 1 : bin);
                 atomicAdd(a.hist + bin, 1ull);
             }
+            if (a.pix_spec && e.tag < a.n_map) {
+                // per-pixel exit spectrum; energies past the last bin are not binned
+                const uint32_t px = a.pixel_of_tag[e.tag];
+                const int bin = dev::floor_to_int(e.E * a.pix_inv_width);
+                if (px < a.n_pixels && bin >= 0 && bin < a.pix_bins) {
+                    float wt = 1.0f;
+                    if constexpr (Mode == kModeLearned) wt = ex.w;
+                    atomicAdd(a.pix_spec + size_t(px) * a.pix_bins + bin, wt);
+                }
+            }
             if (a.rec_a) {
                 const uint32_t slot = atomicAdd(a.rec_count, 1u);
                 if (slot < a.rec_capacity) {
@@ -544,13 +554,15 @@ __global__ void step_query_kernel(const dev::Physics P, ElectronRecord* el, uint
     }
 }
 
-__global__ void pixel_yields_kernel(const uint32_t* se, const uint32_t* bse, const uint32_t* pixel_of_tag,
-                                    uint64_t n_tags, uint64_t n_pixels, double* out) {
+// se_w / bse_w (learned mode): per-tag weighted detections used instead of
+// the counts, so the sums are of per-primary weighted yields and their squares.
+__global__ void pixel_yields_kernel(const uint32_t* se, const uint32_t* bse, const float* se_w, const float* bse_w,
+                                    const uint32_t* pixel_of_tag, uint64_t n_tags, uint64_t n_pixels, double* out) {
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n_tags;
          i += uint64_t(gridDim.x) * blockDim.x) {
         const uint32_t p = pixel_of_tag[i];
         if (p >= n_pixels) continue;
-        const double s = se[i], b = bse[i];
+        const double s = se_w ? double(se_w[i]) : double(se[i]), b = bse_w ? double(bse_w[i]) : double(bse[i]);
         double* o = out + 5 * size_t(p);
         atomicAdd(o + 0, 1.0);
         if (s != 0) {
@@ -796,10 +808,12 @@ cudaError_t launch_step_query(const dev::Physics& P, void* electrons, uint64_t n
     return cudaGetLastError();
 }
 
-cudaError_t launch_pixel_yields(const uint32_t* se, const uint32_t* bse, const uint32_t* pixel_of_tag,
-                                uint64_t n_tags, uint64_t n_pixels, double* out, cudaStream_t s) {
+cudaError_t launch_pixel_yields(const uint32_t* se, const uint32_t* bse, const float* se_w, const float* bse_w,
+                                const uint32_t* pixel_of_tag, uint64_t n_tags, uint64_t n_pixels, double* out,
+                                cudaStream_t s) {
     if (n_tags == 0) return cudaSuccess;
-    pixel_yields_kernel<<<grid_for(n_tags, 256), 256, 0, s>>>(se, bse, pixel_of_tag, n_tags, n_pixels, out);
+    pixel_yields_kernel<<<grid_for(n_tags, 256), 256, 0, s>>>(se, bse, se_w, bse_w, pixel_of_tag, n_tags, n_pixels,
+                                                              out);
     return cudaGetLastError();
 }
 

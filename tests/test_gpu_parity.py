@@ -378,3 +378,50 @@ def test_pixel_yields_match_tag_counts(inputs):
     assert np.array_equal(a, ref)
     assert a[:, 0].sum() == n
     ctx.close()
+
+
+def test_pixel_spectra_match_detected_records(inputs):
+    """Per-pixel exit spectra tallied on the device against the detected
+    records binned on the host (through the same tag -> pixel map)."""
+    recs = g.scan_beam(8, 8, 50, 500.0, origin=(-4.0, -4.0), z_start=5.0, seed=9)
+    n = len(recs)
+    pix = (recs["py"] * 8 + recs["px"]).astype(np.uint32)
+    ctx = nb.setup(inputs["cube"], [inputs["si"]], device=0, seed=14, record_detected=True)
+    ctx.set_tag_range(n)
+    ctx.set_pixel_map(pix)
+    ctx.enable_pixel_spectra(64, 200, 0.5)
+    _run_gpu(ctx, recs)
+    spec = ctx.pixel_spectra()
+    det = ctx.flush_detected()
+    assert len(det) > 0
+    ref = np.zeros((64, 200), np.float64)
+    bins = np.floor(det["E"] / np.float32(0.5)).astype(np.int64)
+    keep = (bins >= 0) & (bins < 200)
+    np.add.at(ref, (pix[det["tag"][keep]], bins[keep]), 1.0)
+    assert np.array_equal(spec.astype(np.float64), ref)
+    ctx.reset_tallies()
+    assert ctx.pixel_spectra().sum() == 0
+    ctx.close()
+
+
+def test_learned_pixel_yields_are_weighted(inputs):
+    """In learned mode the pixel sums run over per-primary weighted counts;
+    with the roulette switched off every weight is 1 and they equal the
+    plain counts."""
+    recs = g.scan_beam(8, 8, 30, 500.0, origin=(-4.0, -4.0), z_start=5.0, seed=10)
+    pix = (recs["py"] * 8 + recs["px"]).astype(np.uint32)
+    ctx = nb.setup(inputs["cube"], [inputs["si"]], device=0, seed=15)
+    ctx.build_surface_map([-50, -50, -40], [50, 50, 20], 1.0, 20.0)
+    ctx.mlp_set_params(nb.mlp_init_params(0))
+    ctx.set_mode("learned", rr_threshold=0.0, split_threshold=2.0, rr_period=4)
+    _run_gpu(ctx, recs)
+    w = ctx.pixel_yields(pix, 64)
+    se, bse = ctx.tag_counts(0, len(recs))
+    ref = np.zeros((64, 5))
+    np.add.at(ref[:, 0], pix, 1.0)
+    np.add.at(ref[:, 1], pix, se.astype(float))
+    np.add.at(ref[:, 2], pix, se.astype(float) ** 2)
+    np.add.at(ref[:, 3], pix, bse.astype(float))
+    np.add.at(ref[:, 4], pix, bse.astype(float) ** 2)
+    assert np.allclose(w, ref)
+    ctx.close()
