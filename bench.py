@@ -42,16 +42,28 @@ PER_PIXEL = 100
 ENERGY = 500.0
 WORKLOAD = "grating 256x256 px x 100 primaries @ 500 eV (6,553,600 primaries), 5,136 triangles, Si-like Kieft tables"
 
-# Scans the bench can run: the grating line scan (the headline workload) and
-# the rough-slab scan with mixed beam energies.
+# Scans the bench can run: the grating line scan (the headline workload),
+# the rough-slab scan with mixed beam energies and the multi-material
+# contact-hole array.  `rows` is the default pixel-row subset of one step,
+# `cpu_sample` / `ref_sample` the primaries (evenly strided over the step's
+# scan) of the CPU-baseline run and of each reference-arm step.
 WORKLOADS = {
     "grating": dict(nx=256, ny=256, per_pixel=100, energy=500.0, energies=None, spacing=1.0,
-                    origin=(-128.0, -128.0), z_start=75.0, desc=WORKLOAD),
+                    origin=(-128.0, -128.0), z_start=75.0, materials=("si",), rows=256,
+                    cpu_sample=409600, ref_sample=102400, desc=WORKLOAD),
     "rough": dict(nx=512, ny=512, per_pixel=20, energy=1000.0, energies=[300.0, 1000.0, 3000.0, 5000.0],
-                  spacing=1000.0 / 512, origin=(-500.0, -500.0), z_start=25.0,
+                  spacing=1000.0 / 512, origin=(-500.0, -500.0), z_start=25.0, materials=("si",), rows=512,
+                  cpu_sample=163840, ref_sample=40960,
                   desc="rough slab: 512x512 Gaussian height field (RMS 3 nm, correlation 10 nm) over 1 um, "
                        "526,334 triangles; 512x512 px x 20 primaries (5,242,880) at E uniform over "
                        "{300, 1000, 3000, 5000} eV, Si-like Kieft tables"),
+    "holes": dict(nx=1024, ny=1024, per_pixel=200, energy=1000.0, energies=None, spacing=2.5,
+                  origin=(-1278.75, -1278.75), z_start=10.0, materials=("sio2", "w", "si"), rows=64,
+                  tune_row=8, cpu_sample=204800, ref_sample=102400,
+                  desc="contact holes: 32x32 holes (40 nm diameter, 100 nm deep, +-2 nm edge roughness) in a "
+                       "SiO2-like film over W-like plugs on a Si-like substrate, 2,359,316 triangles over "
+                       "2.56 um; 1024x1024 px at 2.5 nm x 200 primaries at 1 keV, one step = %d pixel rows "
+                       "(%d primaries); SiO2/W/Si-like Kieft tables"),
 }
 
 
@@ -59,7 +71,11 @@ def configure(args):
     """Point the module's scan constants at the chosen workload."""
     global NX, NY, PER_PIXEL, ENERGY, WORKLOAD
     w = WORKLOADS[args.workload]
-    NX, NY, PER_PIXEL, ENERGY, WORKLOAD = w["nx"], w["ny"], w["per_pixel"], w["energy"], w["desc"]
+    NX, NY, PER_PIXEL, ENERGY = w["nx"], w["ny"], w["per_pixel"], w["energy"]
+    if args.rows <= 0:
+        args.rows = w["rows"]
+    args.rows = min(args.rows, NY)
+    WORKLOAD = w["desc"] % (args.rows, args.rows * NX * PER_PIXEL) if "%d" in w["desc"] else w["desc"]
 
 
 def workload_name(args):
@@ -109,15 +125,26 @@ def barrier(dist):
 
 
 def make_workload(tmp, rank=0, rows=None, workload="grating"):
+    """Material files (in geometry order), triangles, .tri path and the
+    scan's primaries (pixel rows `rows`, all if None)."""
     from nebula_b200 import formats, generators as g
     w = WORKLOADS[workload]
-    mat = g.make_material(os.path.join(tmp, "si.mat"))
-    tris = g.grating_geometry() if workload == "grating" else g.rough_geometry(512)
+    mats = [g.make_material(os.path.join(tmp, k + ".mat"), kind=k) for k in w["materials"]]
+    tris = {"grating": g.grating_geometry, "rough": lambda: g.rough_geometry(512),
+            "holes": g.contact_hole_geometry}[workload]()
     tri_path = os.path.join(tmp, workload + ".tri")
     formats.write_tri(tri_path, tris)
     recs = g.scan_beam(w["nx"], w["ny"], w["per_pixel"], w["energy"], spacing=w["spacing"], origin=w["origin"],
                        z_start=w["z_start"], seed=1000 + rank, energies=w["energies"], rows=rows)
-    return mat, tris, tri_path, recs
+    return mats, tris, tri_path, recs
+
+
+def strided_sample(recs, count):
+    """`count` primaries evenly strided over the scan (every pixel row of
+    the step is represented)."""
+    if count >= len(recs):
+        return recs
+    return recs[np.linspace(0, len(recs) - 1, count).astype(np.int64)]
 
 
 class ClockSampler:
@@ -178,7 +205,7 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def algorithmic_bytes_per_event(tris, mat_path, recs, seed, penn=False):
+def algorithmic_bytes_per_event(tris, mat_paths, recs, seed, penn=False):
     """Section-8(d) algorithmic bytes per event, counted by the instrumented
     CPU restatement on a fixed sample of the workload.  An inelastic event
     reads a 2-D ICDF (16 B) and a rounddown value (4 B) under Kieft, and the
@@ -186,15 +213,15 @@ def algorithmic_bytes_per_event(tris, mat_path, recs, seed, penn=False):
     full Penn."""
     import oracle
     pg = oracle.PortGeometry(tris)
-    rm = oracle.RefMaterial(mat_path, penn=penn)
-    pms, arr = oracle.port_materials([rm])
-    sample = recs[:: max(1, len(recs) // 2000)][:2000]
+    rms = [oracle.RefMaterial(p, penn=penn) for p in mat_paths]
+    pms, arr = oracle.port_materials(rms)
+    sample = strided_sample(recs, 2000)
     prim = np.zeros((len(sample), 7), np.float32)
     prim[:, 0:3] = sample["pos"]
     prim[:, 3:6] = sample["dir"]
     prim[:, 6] = sample["E"]
     c, _, _, _, gc = oracle.port_run(pg, arr, prim, np.arange(len(sample), dtype=np.uint32), seed,
-                                     max_energy=rm.max_energy, penn=penn)
+                                     max_energy=min(m.max_energy for m in rms), penn=penn)
     ev = c["n_elastic"] + c["n_inelastic"] + c["n_boundary"]
     b_state = 88.0
     b_inel = 52.0 if penn else 20.0
@@ -206,23 +233,23 @@ def algorithmic_bytes_per_event(tris, mat_path, recs, seed, penn=False):
                                          "sample_primaries": len(sample), "sample_events": ev}
 
 
-def cpu_baseline(tri_path, mat_path, recs, tmp, rows=16, penn=False):
+def cpu_baseline(tri_path, mat_paths, recs, tmp, count, penn=False):
     """The reference's own CPU path (oracle/_ref, cpu_mt_main-style driver;
-    the stock full Penn build with `penn`) on the first `rows` pixel rows of
-    the scan, all host cores."""
+    the stock full Penn build with `penn`) on `count` primaries evenly
+    strided over the step's scan, all host cores."""
     import oracle
     from nebula_b200 import formats
     if not oracle.have_ref(penn):
         return None
-    sub = recs[recs["py"] < rows]
+    sub = strided_sample(recs, count)
     pri = os.path.join(tmp, "cpu_sample.pri")
     formats.write_pri(pri, sub)
     cores = os.cpu_count() or 1
-    _, st, secs = oracle.ref_run(tri_path, pri, [mat_path], threads=cores, count_events=True, penn=penn)
+    _, st, secs = oracle.ref_run(tri_path, pri, mat_paths, threads=cores, count_events=True, penn=penn)
     ev = st["n_intersect"] + st["n_elastic"] + st["n_inelastic"]
     return {"value": ev / secs, "unit": "events/s", "cores": cores, "kind": "reference",
-            "sample": "%d pixel rows x %d px x %d primaries = %d primaries (%d events) in %.2f s"
-                      % (rows, NX, PER_PIXEL, len(sub), ev, secs),
+            "sample": "%d primaries evenly strided over the step's scan (%d events) in %.2f s"
+                      % (len(sub), ev, secs),
             "primaries_per_s": st["n_primaries"] / secs}
 
 
@@ -237,15 +264,14 @@ def run_reference(args):
             print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref reference library not built"}))
             return 0
         from nebula_b200 import formats
-        mat, tris, tri_path, recs = make_workload(tmp, workload=args.workload)
-        rows = 4
-        sub = recs[recs["py"] < rows]
+        mats, tris, tri_path, recs = make_workload(tmp, rows=range(args.rows), workload=args.workload)
+        sub = strided_sample(recs, WORKLOADS[args.workload]["ref_sample"])
         pri = os.path.join(tmp, "ref_step.pri")
         formats.write_pri(pri, sub)
         cores = os.cpu_count() or 1
         total_ev, total_s, total_p = 0, 0.0, 0
         for i in range(args.warmup + args.steps):
-            _, st, secs = oracle.ref_run(tri_path, pri, [mat], seed=0x78C7E39B + i, threads=cores, count_events=True,
+            _, st, secs = oracle.ref_run(tri_path, pri, mats, seed=0x78C7E39B + i, threads=cores, count_events=True,
                                          penn=penn)
             if i >= args.warmup:
                 total_ev += st["n_intersect"] + st["n_elastic"] + st["n_inelastic"]
@@ -257,7 +283,7 @@ def run_reference(args):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic", "primaries_per_s": total_p / total_s,
                 "config": {"workload": workload_name(args), "inelastic": args.inelastic,
-                           "step_sample": "%d pixel rows (%d primaries) per step" % (rows, len(sub))},
+                           "step_sample": "%d primaries per step, evenly strided over the scan" % len(sub)},
                 "cpu_baseline": {"value": v, "unit": "events/s", "cores": cores, "kind": "reference",
                                  "sample": "%d primaries per step, %d steps" % (len(sub), args.steps)},
                 "e2e": {"value": v, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -325,7 +351,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="grating", choices=sorted(WORKLOADS),
                     help="grating line scan (headline) or rough slab with mixed energies")
-    ap.add_argument("--rows", type=int, default=0, help="pixel rows of the scan (0: all; profiling runs use fewer)")
+    ap.add_argument("--rows", type=int, default=0,
+                    help="pixel rows of one step (0: the workload's default, all rows but for the contact holes)")
     ap.add_argument("--variant", type=int, default=0, help="transport variant 2/3/4/7 (0: autotune)")
     ap.add_argument("--block", type=int, default=0, help="threads per block with --variant (0: 128)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-roulette FOM comparison")
@@ -335,8 +362,6 @@ def main():
                     help="inelastic model: Kieft & Bosch (the headline workload) or full Penn (the reference's stock build)")
     args = ap.parse_args()
     configure(args)
-    if args.rows <= 0:
-        args.rows = NY
     if args.impl == "reference":
         return run_reference(args)
 
@@ -345,9 +370,8 @@ def main():
     import nebula_b200 as nb
 
     tmp = tempfile.mkdtemp(prefix="nbx_bench_")
-    mat, tris, tri_path, recs = make_workload(tmp, rank, rows=None if args.rows >= NY else range(args.rows),
-                                              workload=args.workload)
-    ctx = nb.setup(tris, [mat], device=local, seed=0x78C7E39B + rank, inelastic=args.inelastic)
+    mats, tris, tri_path, recs = make_workload(tmp, rank, rows=range(args.rows), workload=args.workload)
+    ctx = nb.setup(tris, mats, device=local, seed=0x78C7E39B + rank, inelastic=args.inelastic)
     n = len(recs)
     prim = np.zeros((n, 7), np.float32)
     prim[:, 0:3] = recs["pos"]
@@ -370,12 +394,15 @@ def main():
     # Autotune the transport launch shape on a 16-row sample of the scan.
     if args.variant:
         ctx.close()
-        ctx = nb.setup(tris, [mat], device=local, seed=0x78C7E39B + rank, blocks_per_sm=args.variant,
+        ctx = nb.setup(tris, mats, device=local, seed=0x78C7E39B + rank, blocks_per_sm=args.variant,
                        block_size=args.block or 128, inelastic=args.inelastic)
         ctx.set_tag_range(n)
         tuned = (args.variant, args.block or 128)
     else:
-        sample = np.arange(min(n, 16 * NX * PER_PIXEL))   # records are row-major: the first 16 rows
+        # records are row-major: 16 pixel rows from `tune_row` (the contact
+        # holes' first band of holes; the grating and the slab are uniform)
+        r0 = min(WORKLOADS[args.workload].get("tune_row", 0), max(0, args.rows - 16))
+        sample = np.arange(r0 * NX * PER_PIXEL, min(n, (r0 + 16) * NX * PER_PIXEL))
         tuned = ctx.autotune(prim[sample], tags[sample])
 
     def one_step():
@@ -423,11 +450,12 @@ def main():
     # End-to-end through the C ABI from pinned host buffers.  The scan's
     # tag -> pixel map is given once, like the geometry (setup, untimed).
     ctx.set_pixel_map(pixel_of_tag)
+    n_pix = args.rows * NX
     try:
         import torch
-        pin_y = torch.empty((NX * NY, 5), dtype=torch.float64, pin_memory=True).numpy()
+        pin_y = torch.empty((n_pix, 5), dtype=torch.float64, pin_memory=True).numpy()
     except Exception:
-        pin_y = np.empty((NX * NY, 5), np.float64)
+        pin_y = np.empty((n_pix, 5), np.float64)
     e2e_s = []
     parts = {"push_ms": 0.0, "run_ms": 0.0, "yields_ms": 0.0}
     for _ in range(args.steps):
@@ -437,7 +465,7 @@ def main():
         t1 = time.perf_counter()
         ctx.run()
         t2 = time.perf_counter()
-        out = ctx.pixel_yields(None, NX * NY, out=pin_y)
+        out = ctx.pixel_yields(None, n_pix, out=pin_y)
         t3 = time.perf_counter()
         e2e_s.append(t3 - t0)
         parts["push_ms"] += 1000 * (t1 - t0) / args.steps
@@ -446,23 +474,25 @@ def main():
     t_e2e = allreduce_max(dist, sum(e2e_s))
     e2e_val = ev_all / t_e2e
     h2d = n * 7 * 4 + n * 4
-    d2h = NX * NY * 5 * 8
+    d2h = n_pix * 5 * 8
 
     # the network's surface map and training scan are set up for the grating
-    learned = None if (args.no_learned or args.workload != "grating") else learned_fom(args, tris, mat, local, rank, prim, tags, mean_se, var_primary,
-                                                       fom)
+    learned = None if (args.no_learned or args.workload != "grating") else \
+        learned_fom(args, tris, mats[0], local, rank, prim, tags, mean_se, var_primary, fom)
 
     line = None
     if rank == 0:
         peak, peak_kind = measured_peaks()
-        b_event, b_parts = algorithmic_bytes_per_event(tris, mat, recs, 0x78C7E39B, penn=args.inelastic == "penn")
+        b_event, b_parts = algorithmic_bytes_per_event(tris, mats, recs, 0x78C7E39B, penn=args.inelastic == "penn")
         achieved = events * b_event / (sum(dev_ms) / 1000.0) / 1e9
         traffic = None
         tp = os.path.join(ROOT, "profiles", "transport_kernel_traffic.json")
         if os.path.exists(tp) and args.inelastic == "kieft" and args.workload == "grating":   # captured there
             with open(tp) as f:
                 traffic = json.load(f).get("dram_bytes_per_launch")
-        cpu = None if args.no_cpu_baseline else cpu_baseline(tri_path, mat, recs, tmp, penn=args.inelastic == "penn")
+        cpu = None if args.no_cpu_baseline else cpu_baseline(tri_path, mats, recs, tmp,
+                                                              WORKLOADS[args.workload]["cpu_sample"],
+                                                              penn=args.inelastic == "penn")
         line = {
             "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,

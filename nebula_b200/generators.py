@@ -379,6 +379,130 @@ def rough_geometry(n=512, size=1000.0, rms=3.0, corr=10.0, depth=1000.0, seed=0,
     return np.concatenate([top, b.array()])
 
 
+def _quads_to_tris(A, B, C, D, mat_in, mat_out):
+    """Triangles (A, B, C), (A, C, D) of quads given as (..., 3) corner arrays,
+    counter-clockwise seen from the mat_out side."""
+    A, B, C, D = (np.asarray(v, np.float64).reshape(-1, 3) for v in (A, B, C, D))
+    out = np.zeros(2 * len(A), formats.TRI_DTYPE)
+    out["mat_in"] = mat_in
+    out["mat_out"] = mat_out
+    out["v"][0::2] = np.stack([A, B, C], 1).astype(np.float32)
+    out["v"][1::2] = np.stack([A, C, D], 1).astype(np.float32)
+    return out
+
+
+def _fan(center, ring, mat_in, mat_out):
+    """Triangles (center, ring[j], ring[j+1]) for rings of shape (holes, n, 3),
+    counter-clockwise seen from the mat_out side when the ring runs so."""
+    n = ring.shape[1]
+    c = np.repeat(center[:, None, :], n, 1).reshape(-1, 3)
+    a = ring.reshape(-1, 3)
+    b = np.roll(ring, -1, axis=1).reshape(-1, 3)
+    out = np.zeros(len(a), formats.TRI_DTYPE)
+    out["mat_in"] = mat_in
+    out["mat_out"] = mat_out
+    out["v"] = np.stack([c, a, b], 1).astype(np.float32)
+    return out
+
+
+def contact_hole_geometry(n_holes=32, pitch=80.0, radius=20.0, depth=100.0, roughness=2.0, plug_depth=50.0,
+                          substrate=500.0, n_theta=48, n_rings=20, detector_z=20.0, seed=0,
+                          materials=(0, 1, 2)):
+    """Contact-hole array: an ``n_holes`` x ``n_holes`` grid of holes of
+    ``radius`` nm (edge roughness up to +-``roughness`` nm, a few seeded
+    Fourier modes in angle blended along the depth) through a ``depth`` nm
+    film (material ``materials[0]``, SiO2-like) down to plugs (``[1]``,
+    W-like, ``plug_depth`` nm) set in the substrate (``[2]``, Si-like).  With
+    the defaults about 2.4 M triangles over 2.56 um; a DETECTOR plane sits at
+    ``detector_z``.  The surface meshes are conforming: neighbouring cells
+    share the vertices of their common edges."""
+    film, plug, sub = materials
+    V = formats.VACUUM
+    rng = np.random.Generator(np.random.Philox(seed))
+    H = n_holes * n_holes
+    half = n_holes * pitch / 2.0
+    idx = np.arange(n_holes)
+    cx = (-half + (idx + 0.5) * pitch)
+    CX, CY = np.meshgrid(cx, cx, indexing="ij")
+    centers = np.stack([CX.ravel(), CY.ravel()], 1)                       # (H, 2)
+    # angles: multiples of 360/n_theta, including the square's corners
+    theta = 2 * np.pi * np.arange(n_theta) / n_theta
+    # edge roughness r(theta, z): modes k = 2..6, top and bottom profiles
+    # blended linearly in depth, scaled so the largest excursion is `roughness`
+    ks = np.arange(2, 7)
+
+    def profile():
+        a = rng.standard_normal((H, len(ks)))
+        b = rng.standard_normal((H, len(ks)))
+        p = (a[:, :, None] * np.cos(ks[None, :, None] * theta) + b[:, :, None] * np.sin(ks[None, :, None] * theta)).sum(1)
+        return p / np.abs(p).max(1, keepdims=True) * roughness
+
+    top_p, bot_p = profile(), profile()
+    zs = -depth * np.arange(n_rings + 1) / n_rings                        # 0 .. -depth
+    w = (np.arange(n_rings + 1) / n_rings)[None, :, None]
+    r = radius + (1 - w) * top_p[:, None, :] + w * bot_p[:, None, :]       # (H, rings+1, n_theta)
+    ring = np.stack([centers[:, None, None, 0] + r * np.cos(theta),
+                     centers[:, None, None, 1] + r * np.sin(theta),
+                     np.broadcast_to(zs[None, :, None], r.shape)], -1)   # (H, rings+1, n_theta, 3)
+    parts = []
+    # hole walls (film | vacuum inside the hole): normals point to the axis
+    A = ring[:, :-1]
+    B = np.roll(ring[:, :-1], -1, axis=2)
+    Cc = np.roll(ring[:, 1:], -1, axis=2)
+    D = ring[:, 1:]
+    parts.append(_quads_to_tris(A, B, Cc, D, film, V))
+    # square-cell boundary points at the same angles: edge e (right, top,
+    # left, bottom) and offset hp * tan(m * step) along it, built from one
+    # table of tangents with explicit sign flips so that neighbouring cells
+    # compute bit-identical shared vertices
+    hp = pitch / 2.0
+    if n_theta % 8:
+        raise ValueError("n_theta must be a multiple of 8")
+    q = n_theta // 8
+    T = np.tan(np.arange(q + 1) * (2 * np.pi / n_theta))
+    T[q] = 1.0
+    sq = np.zeros((n_theta, 2))
+    for j in range(n_theta):
+        e = ((j + q) // (2 * q)) % 4
+        m = j - e * 2 * q
+        if m > q:
+            m -= n_theta
+        off = hp * (np.sign(m) * T[abs(m)])
+        sq[j] = ((hp, off), (-off, hp), (-hp, -off), (off, -hp))[e]
+    outer = centers[:, None, :] + sq[None, :, :]                          # (H, n_theta, 2)
+
+    def annulus(inner, z, mat_in, mat_out):
+        o = np.concatenate([outer, np.full(outer.shape[:2] + (1,), z)], -1)
+        return _quads_to_tris(inner, o, np.roll(o, -1, axis=1), np.roll(inner, -1, axis=1), mat_in, mat_out)
+
+    parts.append(annulus(ring[:, 0], 0.0, film, V))                       # film top (normal +z)
+    parts.append(annulus(ring[:, -1], -depth, sub, film))                 # film / substrate interface
+    bottom = ring[:, -1]
+    ctr_b = np.concatenate([centers, np.full((H, 1), -depth)], 1)
+    parts.append(_fan(ctr_b, bottom, plug, V))                            # hole floor: plug top
+    low = bottom.copy()
+    low[..., 2] = -depth - plug_depth
+    # plug walls (plug | substrate outside): normals point away from the axis
+    parts.append(_quads_to_tris(bottom, low, np.roll(low, -1, axis=1), np.roll(bottom, -1, axis=1), plug, sub))
+    ctr_l = np.concatenate([centers, np.full((H, 1), -depth - plug_depth)], 1)
+    parts.append(_fan(ctr_l, low[:, ::-1], plug, sub))                    # plug bottom (normal -z)
+    # outer box: film and substrate sides, substrate bottom
+    b = TriBuilder()
+    lo, hi = -half, half
+    zb = -depth - substrate
+    for z0, z1, m in ((-depth, 0.0, film), (zb, -depth, sub)):
+        b.quad((lo, lo, z0), (hi, lo, z0), (hi, lo, z1), (lo, lo, z1), m, V)   # -y
+        b.quad((hi, hi, z0), (lo, hi, z0), (lo, hi, z1), (hi, hi, z1), m, V)   # +y
+        b.quad((lo, hi, z0), (lo, lo, z0), (lo, lo, z1), (lo, hi, z1), m, V)   # -x
+        b.quad((hi, lo, z0), (hi, hi, z0), (hi, hi, z1), (hi, lo, z1), m, V)   # +x
+    b.quad((lo, lo, zb), (lo, hi, zb), (hi, hi, zb), (hi, lo, zb), sub, V)     # bottom (normal -z)
+    m = 50.0
+    b.quad((lo - m, lo - m, detector_z), (hi + m, lo - m, detector_z), (hi + m, hi + m, detector_z),
+           (lo - m, hi + m, detector_z), formats.DETECTOR, formats.DETECTOR)
+    parts.append(b.array())
+    return np.concatenate(parts)
+
+
 # ----------------------------------------------------------------------------
 # Primaries
 # ----------------------------------------------------------------------------

@@ -1,0 +1,97 @@
+"""The seeded geometry generators produce closed, consistently oriented
+meshes: a ray from any point of a known region leaves it through a triangle
+whose material on the ray's side is that region's material (the normal
+points to the `mat_out` side, geometry/trimesh conventions of the .tri
+format), and the contact-hole cells share their boundary vertices."""
+from collections import Counter
+
+import numpy as np
+
+from nebula_b200 import formats, generators as g
+
+
+def _first_hit(v, p, d):
+    v0, e1, e2 = v[:, 0], v[:, 1] - v[:, 0], v[:, 2] - v[:, 0]
+    pv = np.cross(d, e2)
+    det = (e1 * pv).sum(1)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        inv = 1.0 / det
+        tv = p - v0
+        u = (tv * pv).sum(1) * inv
+        qv = np.cross(tv, e1)
+        w = (qv @ d) * inv
+        t = (qv * e2).sum(1) * inv
+    hit = (np.abs(det) > 1e-12) & (u >= 0) & (w >= 0) & (u + w <= 1) & (t > 1e-9)
+    if not hit.any():
+        return -1
+    return int(np.argmin(np.where(hit, t, np.inf)))
+
+
+def _holes_region(p, n, pitch, radius, rough, depth, plug_depth, substrate):
+    """Material at point p of the contact-hole geometry, None within the
+    edge-roughness band of a hole wall."""
+    half = n * pitch / 2
+    x, y, z = p
+    if abs(x) > half or abs(y) > half or z > 0 or z < -depth - substrate:
+        return formats.VACUUM
+    cx = -half + pitch * (np.clip(np.floor((x + half) / pitch), 0, n - 1) + 0.5)
+    cy = -half + pitch * (np.clip(np.floor((y + half) / pitch), 0, n - 1) + 0.5)
+    r = np.hypot(x - cx, y - cy)
+    inside, outside = r < radius - rough - 0.5, r > radius + rough + 0.5
+    if z > -depth:
+        return formats.VACUUM if inside else (0 if outside else None)
+    if z > -depth - plug_depth:
+        return 1 if inside else (2 if outside else None)
+    return 2
+
+
+def test_contact_holes_closed_and_oriented():
+    n = 2
+    tris = g.contact_hole_geometry(n_holes=n, seed=3)
+    keep = tris["mat_in"] != formats.DETECTOR
+    t = tris[keep]
+    v = t["v"].reshape(-1, 3, 3).astype(np.float64)
+    nrm = np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0])
+    rng = np.random.default_rng(7)
+    checked = 0
+    for _ in range(1500):
+        p = rng.uniform([-100, -100, -640], [100, 100, 10])
+        reg = _holes_region(p, n, 80.0, 20.0, 2.0, 100.0, 50.0, 500.0)
+        if reg is None:
+            continue
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        k = _first_hit(v, p, d)
+        if k < 0:
+            assert reg == formats.VACUUM, p
+            continue
+        side = t["mat_in"][k] if d @ nrm[k] > 0 else t["mat_out"][k]
+        assert side == reg, (p, d, k)
+        checked += 1
+    assert checked > 800
+
+
+def test_contact_hole_cells_share_vertices():
+    """Inside the array every edge is shared by two triangles, or by four
+    on the rings where the hole wall, the hole floor, the film/substrate
+    interface and the plug wall meet; single edges lie only on the outer
+    box, where the box faces meet the cells' boundary points."""
+    n, n_theta = 2, 48
+    tris = g.contact_hole_geometry(n_holes=n, n_theta=n_theta, seed=1)
+    t = tris[tris["mat_in"] != formats.DETECTOR]
+    pts = t["v"].reshape(-1, 3)
+    _, vid = np.unique(pts, axis=0, return_inverse=True)
+    vid = vid.reshape(-1, 3)
+    edges = Counter()
+    for a, b, c in vid:
+        for e in ((a, b), (b, c), (c, a)):
+            edges[(min(e), max(e))] += 1
+    counts = Counter(edges.values())
+    assert set(counts) <= {1, 2, 4}
+    assert counts[4] == n * n * n_theta
+    uniq = np.unique(pts, axis=0)
+    half = n * 80.0 / 2
+    for (a, b), c in edges.items():
+        if c == 1:
+            for q in (uniq[a], uniq[b]):
+                assert abs(abs(q[0]) - half) < 1e-9 or abs(abs(q[1]) - half) < 1e-9

@@ -22,7 +22,7 @@ def _compare_octree(oracle, tris):
     return ho
 
 
-@pytest.mark.parametrize("name", ["cube", "grating", "rough"])
+@pytest.mark.parametrize("name", ["cube", "grating", "rough", "holes"])
 def test_octree_layout_identical(oracle_built, inputs, name):
     ho = _compare_octree(oracle_built, inputs[name])
     assert len(ho.octree_data) >= 8
