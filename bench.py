@@ -61,7 +61,7 @@ WORKLOADS = {
                   origin=(-1278.75, -1278.75), z_start=10.0, materials=("sio2", "w", "si"), rows=64,
                   tune_row=8, cpu_sample=204800, ref_sample=102400,
                   desc="contact holes: 32x32 holes (40 nm diameter, 100 nm deep, +-2 nm edge roughness) in a "
-                       "SiO2-like film over W-like plugs on a Si-like substrate, 2,359,316 triangles over "
+                       "SiO2-like film over W-like plugs on a Si-like substrate, 2,506,772 triangles over "
                        "2.56 um; 1024x1024 px at 2.5 nm x 200 primaries at 1 keV, one step = %d pixel rows "
                        "(%d primaries); SiO2/W/Si-like Kieft tables"),
 }

@@ -185,12 +185,42 @@ int guarded(nbx_ctx* ctx, F&& f) {
     }
 }
 
+// All device traffic of a context goes through its own stream, which is
+// created non-blocking and so does not wait for the legacy default stream: a
+// plain cudaMemcpy from pageable host memory, a cudaMemset or a
+// device-to-device cudaMemcpy can return before the bytes land, and a kernel
+// queued on the context's stream would not wait for them.  These helpers
+// queue the copy on the context's stream and wait for it.
+static void to_device(nbx_ctx* ctx, void* dst, const void* src, size_t bytes, const char* what) {
+    if (!bytes) return;
+    ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream), what);
+    ck(cudaStreamSynchronize(ctx->stream), what);
+}
+
+static void to_host(nbx_ctx* ctx, void* dst, const void* src, size_t bytes, const char* what) {
+    if (!bytes) return;
+    ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream), what);
+    ck(cudaStreamSynchronize(ctx->stream), what);
+}
+
+static void on_device(nbx_ctx* ctx, void* dst, const void* src, size_t bytes, const char* what) {
+    if (!bytes) return;
+    ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, ctx->stream), what);
+    ck(cudaStreamSynchronize(ctx->stream), what);
+}
+
+static void zero(nbx_ctx* ctx, void* dst, size_t bytes, const char* what) {
+    if (!bytes) return;
+    ck(cudaMemsetAsync(dst, 0, bytes, ctx->stream), what);
+    ck(cudaStreamSynchronize(ctx->stream), what);
+}
+
 nbx::dev::Table1D upload1d(nbx_ctx* ctx, const nbx_table1d& t) {
     if (t.n < 2 || !t.data) throw ApiError(NBX_ERR_ARG, "1D table needs at least 2 points");
     auto* b = new DevBuf<float>();
     ctx->tables.push_back(b);
     b->alloc(size_t(t.n));
-    ck(cudaMemcpy(b->p, t.data, sizeof(float) * t.n, cudaMemcpyHostToDevice), "table upload");
+    to_device(ctx, b->p, t.data, sizeof(float) * t.n, "table upload");
     return nbx::dev::Table1D{b->p, t.n, t.x_min, t.x_step};
 }
 
@@ -200,7 +230,7 @@ nbx::dev::Table2D upload2d(nbx_ctx* ctx, const nbx_table2d& t) {
     ctx->tables.push_back(b);
     const size_t n = size_t(t.width) * size_t(t.height);
     b->alloc(n);
-    ck(cudaMemcpy(b->p, t.data, sizeof(float) * n, cudaMemcpyHostToDevice), "table upload");
+    to_device(ctx, b->p, t.data, sizeof(float) * n, "table upload");
     return nbx::dev::Table2D{b->p, t.width, t.height, t.x_min, t.x_step, t.y_min, t.y_step};
 }
 
@@ -211,7 +241,7 @@ nbx::dev::Table3D upload3d(nbx_ctx* ctx, const nbx_table3d& t) {
     ctx->tables.push_back(b);
     const size_t n = size_t(t.width) * size_t(t.height) * size_t(t.depth);
     b->alloc(n);
-    ck(cudaMemcpy(b->p, t.data, sizeof(float) * n, cudaMemcpyHostToDevice), "table upload");
+    to_device(ctx, b->p, t.data, sizeof(float) * n, "table upload");
     return nbx::dev::Table3D{b->p, t.width, t.height, t.depth, t.x_min, t.x_step, t.y_min, t.y_step, t.z_min, t.z_step};
 }
 
@@ -462,12 +492,12 @@ int nbx_create(nbx_ctx** out, const nbx_config* cfg) {
         ck(cudaEventCreate(&ctx->ev1), "event");
         ck(cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, c.device), "attribute");
         ctx->counters.alloc(nbx::kNumCounters);
-        ck(cudaMemset(ctx->counters.p, 0, sizeof(unsigned long long) * nbx::kNumCounters), "memset");
+        zero(ctx, ctx->counters.p, sizeof(unsigned long long) * nbx::kNumCounters, "memset");
         ctx->hist.alloc(kHistBins);
-        ck(cudaMemset(ctx->hist.p, 0, sizeof(unsigned long long) * kHistBins), "memset");
+        zero(ctx, ctx->hist.p, sizeof(unsigned long long) * kHistBins, "memset");
         ctx->ctl.alloc(2 * kMaxGenerations + 2);
         ctx->rec_count.alloc(1);
-        ck(cudaMemset(ctx->rec_count.p, 0, 4), "memset");
+        zero(ctx, ctx->rec_count.p, 4, "memset");
         ctx->block = c.block_size > 0 ? c.block_size : 256;
         if (ctx->block % 32 != 0 || ctx->block > 256) throw ApiError(NBX_ERR_ARG, "block_size must be a multiple of 32, <= 256");
         // Kernel variant = resident blocks per SM it was register-limited for:
@@ -480,7 +510,7 @@ int nbx_create(nbx_ctx** out, const nbx_config* cfg) {
             ctx->dep_cap = c.deposit_capacity ? c.deposit_capacity : (1ull << 27);
             ctx->dep.alloc(ctx->dep_cap * nbx::kDepositWords);
             ctx->dep_cursor.alloc(1);
-            ck(cudaMemset(ctx->dep_cursor.p, 0, sizeof(unsigned long long)), "memset");
+            zero(ctx, ctx->dep_cursor.p, sizeof(unsigned long long), "memset");
         }
         if (c.record_detected) {
             ctx->rec_cap = c.record_capacity ? c.record_capacity : (1ull << 24);
@@ -517,7 +547,7 @@ int nbx_set_geometry(nbx_ctx* ctx, const nbx_octree* o) {
     if (!ctx || !o || !o->octree_data || o->n_octree < 8 || !o->triangles) return NBX_ERR_ARG;
     return guarded(ctx, [&] {
         ctx->octree.alloc(o->n_octree);
-        ck(cudaMemcpy(ctx->octree.p, o->octree_data, sizeof(int32_t) * o->n_octree, cudaMemcpyHostToDevice), "octree");
+        to_device(ctx, ctx->octree.p, o->octree_data, sizeof(int32_t) * o->n_octree, "octree");
         std::vector<float4> t(3 * std::max<uint64_t>(o->n_triangles, 1));
         for (uint64_t i = 0; i < o->n_triangles; ++i) {
             const nbx_triangle& s = o->triangles[i];
@@ -531,7 +561,7 @@ int nbx_set_geometry(nbx_ctx* ctx, const nbx_octree* o) {
             t[3 * i + 2] = make_float4(s.e2[0], s.e2[1], s.e2[2], 0.0f);
         }
         ctx->tris.alloc(t.size());
-        ck(cudaMemcpy(ctx->tris.p, t.data(), sizeof(float4) * t.size(), cudaMemcpyHostToDevice), "triangles");
+        to_device(ctx, ctx->tris.p, t.data(), sizeof(float4) * t.size(), "triangles");
         ctx->tri_faces.alloc(std::max<uint64_t>(o->n_triangles, 1));
         ck(nbx::launch_triangle_faces(ctx->tris.p, ctx->tri_faces.p, int(o->n_triangles), ctx->stream), "faces");
         ck(cudaStreamSynchronize(ctx->stream), "faces");
@@ -754,7 +784,7 @@ int nbx_run(nbx_ctx* ctx) {
         ctx->generations = uint64_t(g);
         ctx->n_queued = 0;
         unsigned long long ovf = 0;
-        ck(cudaMemcpy(&ovf, ctx->counters.p + nbx::kCntOverflow, 8, cudaMemcpyDeviceToHost), "D2H");
+        to_host(ctx, &ovf, ctx->counters.p + nbx::kCntOverflow, 8, "D2H");
         if (ovf) throw ApiError(NBX_ERR_CAPACITY, "secondary queue overflow: electrons lost");
         return NBX_OK;
     });
@@ -770,7 +800,7 @@ int nbx_get_stats(nbx_ctx* ctx, nbx_stats* out) {
     if (!ctx || !out) return NBX_ERR_ARG;
     return guarded(ctx, [&] {
         unsigned long long c[nbx::kNumCounters];
-        ck(cudaMemcpy(c, ctx->counters.p, sizeof(c), cudaMemcpyDeviceToHost), "D2H");
+        to_host(ctx, c, ctx->counters.p, sizeof(c), "D2H");
         std::memset(out, 0, sizeof(*out));
         out->primaries_pushed = ctx->pushed;
         out->primaries_done = ctx->pushed - ctx->n_queued;
@@ -804,13 +834,13 @@ int nbx_flush_detected(nbx_ctx* ctx, nbx_detected* out, uint64_t cap, uint64_t* 
         *n = 0;
         if (!ctx->rec_a.p) return NBX_OK;
         uint32_t cnt = 0;
-        ck(cudaMemcpy(&cnt, ctx->rec_count.p, 4, cudaMemcpyDeviceToHost), "D2H");
+        to_host(ctx, &cnt, ctx->rec_count.p, 4, "D2H");
         const uint64_t have = std::min<uint64_t>(cnt, ctx->rec_cap);
         const uint64_t take = std::min<uint64_t>(have, cap);
         if (take) {
             std::vector<float4> a(take), b(take);
-            ck(cudaMemcpy(a.data(), ctx->rec_a.p, 16 * take, cudaMemcpyDeviceToHost), "D2H");
-            ck(cudaMemcpy(b.data(), ctx->rec_b.p, 16 * take, cudaMemcpyDeviceToHost), "D2H");
+            to_host(ctx, a.data(), ctx->rec_a.p, 16 * take, "D2H");
+            to_host(ctx, b.data(), ctx->rec_b.p, 16 * take, "D2H");
             for (uint64_t i = 0; i < take; ++i) {
                 out[i].pos[0] = a[i].x;
                 out[i].pos[1] = a[i].y;
@@ -825,12 +855,12 @@ int nbx_flush_detected(nbx_ctx* ctx, nbx_detected* out, uint64_t cap, uint64_t* 
         if (take < have) {
             // keep the remainder at the front
             const uint64_t rest = have - take;
-            ck(cudaMemcpy(ctx->rec_a.p, ctx->rec_a.p + take, 16 * rest, cudaMemcpyDeviceToDevice), "D2D");
-            ck(cudaMemcpy(ctx->rec_b.p, ctx->rec_b.p + take, 16 * rest, cudaMemcpyDeviceToDevice), "D2D");
+            on_device(ctx, ctx->rec_a.p, ctx->rec_a.p + take, 16 * rest, "D2D");
+            on_device(ctx, ctx->rec_b.p, ctx->rec_b.p + take, 16 * rest, "D2D");
             const uint32_t r = uint32_t(rest);
-            ck(cudaMemcpy(ctx->rec_count.p, &r, 4, cudaMemcpyHostToDevice), "H2D");
+            to_device(ctx, ctx->rec_count.p, &r, 4, "H2D");
         } else {
-            ck(cudaMemset(ctx->rec_count.p, 0, 4), "memset");
+            zero(ctx, ctx->rec_count.p, 4, "memset");
         }
         *n = take;
         return NBX_OK;
@@ -842,8 +872,8 @@ int nbx_get_tag_counts(nbx_ctx* ctx, uint64_t first, uint64_t n, uint32_t* se, u
     if (first + n > ctx->n_tags) return fail(ctx, NBX_ERR_ARG, "tag range beyond nbx_set_tag_range");
     return guarded(ctx, [&] {
         if (n == 0) return NBX_OK;
-        if (se) ck(cudaMemcpy(se, ctx->se_count.p + first, 4 * n, cudaMemcpyDeviceToHost), "D2H");
-        if (bse) ck(cudaMemcpy(bse, ctx->bse_count.p + first, 4 * n, cudaMemcpyDeviceToHost), "D2H");
+        if (se) to_host(ctx, se, ctx->se_count.p + first, 4 * n, "D2H");
+        if (bse) to_host(ctx, bse, ctx->bse_count.p + first, 4 * n, "D2H");
         return NBX_OK;
     });
 }
@@ -855,7 +885,7 @@ int nbx_enable_pixel_spectra(nbx_ctx* ctx, uint64_t n_pixels, int32_t n_bins, fl
         ctx->spec_pixels = 0;
         if (n_pixels == 0) return NBX_OK;
         ctx->pix_spec.alloc(n_pixels * uint64_t(n_bins));
-        ck(cudaMemset(ctx->pix_spec.p, 0, sizeof(float) * n_pixels * uint64_t(n_bins)), "memset");
+        zero(ctx, ctx->pix_spec.p, sizeof(float) * n_pixels * uint64_t(n_bins), "memset");
         ctx->spec_pixels = n_pixels;
         ctx->spec_bins = n_bins;
         ctx->spec_width = bin_width;
@@ -917,7 +947,7 @@ int nbx_get_spectrum(nbx_ctx* ctx, uint64_t* counts, uint32_t n_bins, float* bin
     if (!counts) return NBX_OK;
     return guarded(ctx, [&] {
         const uint32_t n = std::min<uint32_t>(n_bins, kHistBins);
-        ck(cudaMemcpy(counts, ctx->hist.p, 8ull * n, cudaMemcpyDeviceToHost), "D2H");
+        to_host(ctx, counts, ctx->hist.p, 8ull * n, "D2H");
         return NBX_OK;
     });
 }
@@ -1168,7 +1198,7 @@ int nbx_build_surface_map(nbx_ctx* ctx, const float lo[3], const float hi[3], fl
         if (cells > (1ull << 31)) throw ApiError(NBX_ERR_ARG, "surface map larger than 2^31 cells");
         // candidates: triangles whose box reaches the map box grown by d_max
         std::vector<float4> t(3 * size_t(ctx->phys.geo.n_tri));
-        ck(cudaMemcpy(t.data(), ctx->tris.p, sizeof(float4) * t.size(), cudaMemcpyDeviceToHost), "D2H");
+        to_host(ctx, t.data(), ctx->tris.p, sizeof(float4) * t.size(), "D2H");
         std::vector<int32_t> cand;
         for (int i = 0; i < ctx->phys.geo.n_tri; ++i) {
             const float4 r0 = t[3 * i], e1 = t[3 * i + 1], e2 = t[3 * i + 2];
@@ -1186,7 +1216,7 @@ int nbx_build_surface_map(nbx_ctx* ctx, const float lo[3], const float hi[3], fl
         DevBuf<int32_t> dcand;
         dcand.alloc(std::max<size_t>(cand.size(), 1));
         if (!cand.empty())
-            ck(cudaMemcpy(dcand.p, cand.data(), 4 * cand.size(), cudaMemcpyHostToDevice), "H2D");
+            to_device(ctx, dcand.p, cand.data(), 4 * cand.size(), "H2D");
         ck(nbx::launch_build_surface_map(ctx->tris.p, dcand.p, int(cand.size()), ctx->smap_cells.p, lo[0], lo[1], lo[2],
                                          cell, n[0], n[1], n[2], d_max, ctx->stream), "surface map");
         ck(cudaStreamSynchronize(ctx->stream), "surface map");
@@ -1209,8 +1239,8 @@ int nbx_set_sample_capacity(nbx_ctx* ctx, uint64_t capacity) {
         ctx->sample_feat.alloc(6 * capacity);
         ctx->sample_label.alloc(capacity);
         ctx->sample_count.alloc(1);
-        ck(cudaMemset(ctx->sample_count.p, 0, 4), "memset");
-        ck(cudaMemset(ctx->sample_label.p, 0, 4 * capacity), "memset");
+        zero(ctx, ctx->sample_count.p, 4, "memset");
+        zero(ctx, ctx->sample_label.p, 4 * capacity, "memset");
         ctx->sample_cap = capacity;
         return NBX_OK;
     });
@@ -1222,15 +1252,15 @@ int nbx_get_samples(nbx_ctx* ctx, float* features, float* labels, uint64_t cap, 
         *n = 0;
         if (!ctx->sample_cap) return NBX_OK;
         uint32_t cnt = 0;
-        ck(cudaMemcpy(&cnt, ctx->sample_count.p, 4, cudaMemcpyDeviceToHost), "D2H");
+        to_host(ctx, &cnt, ctx->sample_count.p, 4, "D2H");
         const uint64_t have = std::min<uint64_t>(cnt, ctx->sample_cap);
         const uint64_t take = std::min<uint64_t>(have, cap);
         if (take) {
-            ck(cudaMemcpy(features, ctx->sample_feat.p, 24 * take, cudaMemcpyDeviceToHost), "D2H");
-            ck(cudaMemcpy(labels, ctx->sample_label.p, 4 * take, cudaMemcpyDeviceToHost), "D2H");
+            to_host(ctx, features, ctx->sample_feat.p, 24 * take, "D2H");
+            to_host(ctx, labels, ctx->sample_label.p, 4 * take, "D2H");
         }
-        ck(cudaMemset(ctx->sample_count.p, 0, 4), "memset");
-        ck(cudaMemset(ctx->sample_label.p, 0, 4 * ctx->sample_cap), "memset");
+        zero(ctx, ctx->sample_count.p, 4, "memset");
+        zero(ctx, ctx->sample_label.p, 4 * ctx->sample_cap, "memset");
         *n = take;
         return NBX_OK;
     });
@@ -1241,8 +1271,8 @@ int nbx_get_tag_weights(nbx_ctx* ctx, uint64_t first, uint64_t n, float* se_w, f
     if (first + n > ctx->n_tags) return fail(ctx, NBX_ERR_ARG, "tag range beyond nbx_set_tag_range");
     return guarded(ctx, [&] {
         if (n == 0) return NBX_OK;
-        if (se_w) ck(cudaMemcpy(se_w, ctx->se_w.p + first, 4 * n, cudaMemcpyDeviceToHost), "D2H");
-        if (bse_w) ck(cudaMemcpy(bse_w, ctx->bse_w.p + first, 4 * n, cudaMemcpyDeviceToHost), "D2H");
+        if (se_w) to_host(ctx, se_w, ctx->se_w.p + first, 4 * n, "D2H");
+        if (bse_w) to_host(ctx, bse_w, ctx->bse_w.p + first, 4 * n, "D2H");
         return NBX_OK;
     });
 }
@@ -1273,9 +1303,9 @@ void mlp_alloc(nbx_ctx* ctx) {
     ctx->mlp_v.alloc(nbx::mlp::kParams);
     ctx->mlp_grad.alloc(nbx::mlp::kParams);
     ctx->mlp_loss.alloc(1);
-    ck(cudaMemset(ctx->mlp_params.p, 0, 4 * nbx::mlp::kParams), "memset");
-    ck(cudaMemset(ctx->mlp_m.p, 0, 4 * nbx::mlp::kParams), "memset");
-    ck(cudaMemset(ctx->mlp_v.p, 0, 4 * nbx::mlp::kParams), "memset");
+    zero(ctx, ctx->mlp_params.p, 4 * nbx::mlp::kParams, "memset");
+    zero(ctx, ctx->mlp_m.p, 4 * nbx::mlp::kParams, "memset");
+    zero(ctx, ctx->mlp_v.p, 4 * nbx::mlp::kParams, "memset");
 }
 void mlp_upload(nbx_ctx* ctx, const float* features, const float* labels, uint64_t n) {
     ctx->mlp_feat.ensure(std::max<uint64_t>(n, 1) * nbx::mlp::kFeatures);
@@ -1299,9 +1329,9 @@ int nbx_mlp_set_params(nbx_ctx* ctx, const float* params) {
             for (int i = 0; i < nbx::mlp::kHidden; ++i) p[nbx::mlp::kOffW3 + o * nbx::mlp::kHidden + i] = 0;
             p[nbx::mlp::kOffB3 + o] = 0;
         }
-        ck(cudaMemcpy(ctx->mlp_params.p, p.data(), 4 * nbx::mlp::kParams, cudaMemcpyHostToDevice), "H2D");
-        ck(cudaMemset(ctx->mlp_m.p, 0, 4 * nbx::mlp::kParams), "memset");
-        ck(cudaMemset(ctx->mlp_v.p, 0, 4 * nbx::mlp::kParams), "memset");
+        to_device(ctx, ctx->mlp_params.p, p.data(), 4 * nbx::mlp::kParams, "H2D");
+        zero(ctx, ctx->mlp_m.p, 4 * nbx::mlp::kParams, "memset");
+        zero(ctx, ctx->mlp_v.p, 4 * nbx::mlp::kParams, "memset");
         ctx->mlp_step = 0;
         ctx->mlp_ready = true;
         return NBX_OK;
@@ -1312,7 +1342,7 @@ int nbx_mlp_get_params(nbx_ctx* ctx, float* out) {
     if (!ctx || !out) return NBX_ERR_ARG;
     if (!ctx->mlp_ready) return fail(ctx, NBX_ERR_STATE, "network parameters not set");
     return guarded(ctx, [&] {
-        ck(cudaMemcpy(out, ctx->mlp_params.p, 4 * nbx::mlp::kParams, cudaMemcpyDeviceToHost), "D2H");
+        to_host(ctx, out, ctx->mlp_params.p, 4 * nbx::mlp::kParams, "D2H");
         return NBX_OK;
     });
 }

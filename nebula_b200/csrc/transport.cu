@@ -945,7 +945,8 @@ int run_transport_noalloc(const dev::Physics& P, int grid, int block, int varian
         }
     }
     unsigned long long c[kNumCounters];
-    if (cudaMemcpy(c, cnt, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) return fail("reading counters failed");
+    if (cudaMemcpyAsync(c, cnt, sizeof(c), cudaMemcpyDeviceToHost, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+        return fail("reading counters failed");
     if (counts) {
         counts[0] = c[kCntElastic];
         counts[1] = c[kCntInelastic];

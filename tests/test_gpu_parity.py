@@ -317,7 +317,7 @@ def test_whole_run_grating_rows_vs_reference(inputs, oracle_built, tmp_path):
 
 def test_whole_run_contact_holes_vs_reference(inputs, oracle_built, tmp_path):
     """Three materials (SiO2-like film, W-like plugs, Si-like substrate) on
-    the 3 x 3 contact-hole array (20,756 triangles): a 1 keV line scan
+    the 3 x 3 contact-hole array (22,052 triangles): a 1 keV line scan
     across the middle hole, 32 px x 400 primaries.  Per-pixel SE and BSE
     yields of the GPU path and the reference CPU path agree by chi-square,
     totals within 3 sigma, events per primary within 5 %."""
