@@ -356,6 +356,8 @@ def main():
     ap.add_argument("--variant", type=int, default=0, help="transport variant 2/3/4/7 (0: autotune)")
     ap.add_argument("--block", type=int, default=0, help="threads per block with --variant (0: 128)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-roulette FOM comparison")
+    ap.add_argument("--shared-pop", action="store_true",
+                    help="all transport blocks pop primaries from one cursor (default: per-SM ranges)")
     ap.add_argument("--rr-threshold", type=float, default=0.02)
     ap.add_argument("--rr-period", type=int, default=32)
     ap.add_argument("--inelastic", default="kieft", choices=["kieft", "penn"],
@@ -371,7 +373,8 @@ def main():
 
     tmp = tempfile.mkdtemp(prefix="nbx_bench_")
     mats, tris, tri_path, recs = make_workload(tmp, rank, rows=range(args.rows), workload=args.workload)
-    ctx = nb.setup(tris, mats, device=local, seed=0x78C7E39B + rank, inelastic=args.inelastic)
+    ctx = nb.setup(tris, mats, device=local, seed=0x78C7E39B + rank, inelastic=args.inelastic,
+                   shared_pop=args.shared_pop)
     n = len(recs)
     prim = np.zeros((n, 7), np.float32)
     prim[:, 0:3] = recs["pos"]
@@ -395,7 +398,7 @@ def main():
     if args.variant:
         ctx.close()
         ctx = nb.setup(tris, mats, device=local, seed=0x78C7E39B + rank, blocks_per_sm=args.variant,
-                       block_size=args.block or 128, inelastic=args.inelastic)
+                       block_size=args.block or 128, inelastic=args.inelastic, shared_pop=args.shared_pop)
         ctx.set_tag_range(n)
         tuned = (args.variant, args.block or 128)
     else:
@@ -500,7 +503,8 @@ def main():
             "config": {"workload": workload_name(args), "inelastic": args.inelastic,
                        "parallelism": "replicas x%d" % world,
                        "l2": "inputs larger than L2 (primary queue %.0f MB per step)" % (n * 48 / 1e6),
-                       "autotuned": {"blocks_per_sm_variant": tuned[0], "block_size": tuned[1]}},
+                       "autotuned": {"blocks_per_sm_variant": tuned[0], "block_size": tuned[1]},
+                       "pop": "shared cursor" if args.shared_pop else "per-SM ranges"},
             "primaries_per_s": prim_all / t_dev,
             "events_per_primary": events / (n * args.steps),
             "se_yield": mean_se, "bse_yield": float(bse.sum()) / (n * args.steps),

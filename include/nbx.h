@@ -185,6 +185,9 @@ typedef struct {
     int32_t inelastic_model;   /* NBX_INELASTIC_KIEFT (0, default) or NBX_INELASTIC_FULL_PENN */
     int32_t record_deposits;   /* keep energy-deposit records (plain mode; cpu_energydep.cpp) */
     uint64_t deposit_capacity; /* deposit records held on the device; 0 = 2^27 (3.2 GB) */
+    int32_t shared_pop;        /* 0: the transport blocks on each SM pop the primaries of that SM's
+                                  contiguous range of the queue first (neighbouring primaries share
+                                  the SM's caches; push them in scan order); 1: one shared cursor */
 } nbx_config;
 
 /* One energy deposit (drivers/cpu/energydeposit_cpu_driver.h:74-96,

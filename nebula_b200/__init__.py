@@ -73,7 +73,7 @@ class Config(C.Structure):
     _fields_ = [("device", C.c_int32), ("seed", C.c_uint32), ("energy_threshold", C.c_float),
                 ("capacity", C.c_uint64), ("record_detected", C.c_int32), ("record_capacity", C.c_uint64),
                 ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("inelastic_model", C.c_int32),
-                ("record_deposits", C.c_int32), ("deposit_capacity", C.c_uint64)]
+                ("record_deposits", C.c_int32), ("deposit_capacity", C.c_uint64), ("shared_pop", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -278,7 +278,7 @@ class Context:
 
     def __init__(self, device=0, seed=0x78C7E39B, energy_threshold=0.0, record_detected=False,
                  record_capacity=0, capacity=0, block_size=0, blocks_per_sm=0, inelastic="kieft",
-                 record_deposits=False, deposit_capacity=0):
+                 record_deposits=False, deposit_capacity=0, shared_pop=False):
         L = lib()
         cfg = Config()
         L.nbx_config_default(C.byref(cfg))
@@ -287,6 +287,7 @@ class Context:
         cfg.block_size, cfg.blocks_per_sm = block_size, blocks_per_sm
         cfg.inelastic_model = INELASTIC_MODELS.get(inelastic, inelastic)
         cfg.record_deposits, cfg.deposit_capacity = int(record_deposits), deposit_capacity
+        cfg.shared_pop = int(shared_pop)
         self.h = _vp()
         self._pixel_map_len = 0
         _check(L.nbx_create(C.byref(self.h), C.byref(cfg)))

@@ -46,6 +46,14 @@ struct TransportArgs {
     const uint32_t* n_in;       // number of entries pushed to `in` (may exceed in_capacity)
     uint32_t in_capacity;
     uint32_t* head;             // pop cursor into `in`
+    // Per-SM pop cursors (nullptr: every block pops from `head`).  The queue
+    // is cut into n_ranges contiguous ranges, range r = [n_in * r / n_ranges,
+    // n_in * (r + 1) / n_ranges).  The blocks on SM s pop from range
+    // s % n_ranges and, once it is handed out, from ranges s + 1, s + 2, ...
+    // in turn, so an SM's threads work on neighbouring entries of the queue
+    // (for a raster scan, neighbouring pixels) and share its L1.
+    uint32_t* range_cursor;
+    uint32_t n_ranges;
     uint32_t* out_tail;         // push cursor into `out`
     uint32_t out_capacity;
     uint32_t* se_count;         // per-tag detections below 50 eV

@@ -138,6 +138,7 @@ struct nbx_ctx {
     uint64_t sample_cap = 0;
     DevBuf<float> se_w, bse_w;
     DevBuf<float4> stack_mem;     // transport parked-ancestor stacks (grow-only)
+    DevBuf<uint32_t> range_cursor; // per-SM pop cursors of the primary generation (grow-only)
     DevBuf<uint32_t> yield_map;   // nbx_pixel_yields work buffers (grow-only)
     uint64_t pixel_map_len = 0;    // tags covered by a map from nbx_set_pixel_map
     DevBuf<float> pix_spec;        // per-pixel exit spectra (nbx_enable_pixel_spectra)
@@ -751,6 +752,14 @@ int nbx_run(nbx_ctx* ctx) {
         // parked-ancestor stacks of the launched threads (grow-only)
         ctx->stack_mem.ensure(uint64_t(grid) * uint64_t(ctx->block) * 3 * nbx::kLocalStack);
         a.stack_mem = ctx->stack_mem.p;
+        // The primaries are popped from per-SM ranges (neighbouring queue
+        // entries stay on one SM); the secondary generations, written in
+        // arbitrary order, from one shared cursor.
+        if (!ctx->cfg.shared_pop) {
+            ctx->range_cursor.ensure(uint64_t(ctx->sms));
+            ck(cudaMemsetAsync(ctx->range_cursor.p, 0, sizeof(uint32_t) * ctx->sms, ctx->stream), "memset");
+            a.n_ranges = uint32_t(ctx->sms);
+        }
 
         ck(cudaEventRecord(ctx->ev0, ctx->stream), "event");
         int g = 0;
@@ -763,6 +772,7 @@ int nbx_run(nbx_ctx* ctx) {
                 a.out = out->q();
                 a.n_in = g == 0 ? ctl + 2 * kMaxGenerations : ctl + kMaxGenerations + (g - 1);
                 a.head = ctl + g;
+                a.range_cursor = (g == 0 && !ctx->cfg.shared_pop) ? ctx->range_cursor.p : nullptr;
                 a.out_tail = ctl + kMaxGenerations + g;
                 a.out_capacity = cap;
                 a.in_capacity = uint32_t(std::min<uint64_t>(in->cap, 0xFFFFFFF0ull));

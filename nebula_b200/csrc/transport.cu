@@ -167,6 +167,7 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
     int sp = 0;
     int warp_iter = 0;
     bool alive = false, drained = false;
+    uint32_t probe = 0;   // ranges this thread has found used up (range_cursor)
     uint32_t carry_hit = 0;
     // Per-thread tallies in 32 bits (a thread would need 2^32 steps in one
     // launch to wrap); rare ones (dropped records, queue overflow) go straight
@@ -188,15 +189,40 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                 }
                 alive = true;
             } else {
-                uint32_t idx;
-                {
+                uint32_t idx = 0;
+                bool got = false;
+                if (a.range_cursor) {
+                    // this SM's range first, then the following ranges
+                    const uint32_t nb = a.n_ranges;
+                    uint32_t smid;
+                    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+                    while (probe < nb) {
+                        uint32_t v = smid % nb + probe;
+                        if (v >= nb) v -= nb;
+                        const cg::coalesced_group g = cg::coalesced_threads();
+                        const cg::coalesced_group part = cg::labeled_partition(g, int(v));
+                        uint32_t base = 0;
+                        if (part.thread_rank() == 0) base = atomicAdd(a.range_cursor + v, part.size());
+                        base = part.shfl(base, 0);
+                        const uint32_t lo = uint32_t(uint64_t(n_in) * v / nb);
+                        const uint32_t hi = uint32_t(uint64_t(n_in) * (v + 1) / nb);
+                        const uint32_t off = base + part.thread_rank();
+                        if (off < hi - lo) {
+                            idx = lo + off;
+                            got = true;
+                            break;
+                        }
+                        ++probe;
+                    }
+                } else {
                     cg::coalesced_group g = cg::coalesced_threads();
                     uint32_t base = 0;
                     if (g.thread_rank() == 0) base = atomicAdd(a.head, g.size());
                     base = g.shfl(base, 0);
                     idx = base + g.thread_rank();
+                    got = idx < n_in;
                 }
-                if (idx >= n_in) {
+                if (!got) {
                     drained = true;
                 } else {
                     load_electron(a.in, idx, e);
