@@ -42,24 +42,19 @@ PER_PIXEL = 100
 ENERGY = 500.0
 WORKLOAD = "grating 256x256 px x 100 primaries @ 500 eV (6,553,600 primaries), 5,136 triangles, Si-like Kieft tables"
 
-# Scans the bench can run: the grating line scan (the headline workload),
-# the rough-slab scan with mixed beam energies and the multi-material
-# contact-hole array.  `rows` is the default pixel-row subset of one step,
-# `cpu_sample` / `ref_sample` the primaries (evenly strided over the step's
-# scan) of the CPU-baseline run and of each reference-arm step.
+# Scans the bench can run (geometry, materials and raster scan in
+# nebula_b200.generators.SCANS): the grating line scan (the headline
+# workload), the rough-slab scan with mixed beam energies and the
+# multi-material contact-hole array.  `rows` is the default pixel-row subset
+# of one step, `cpu_sample` / `ref_sample` the primaries (evenly strided over
+# the step's scan) of the CPU-baseline run and of each reference-arm step.
 WORKLOADS = {
-    "grating": dict(nx=256, ny=256, per_pixel=100, energy=500.0, energies=None, spacing=1.0,
-                    origin=(-128.0, -128.0), z_start=75.0, materials=("si",), rows=256,
-                    cpu_sample=409600, ref_sample=102400, desc=WORKLOAD),
-    "rough": dict(nx=512, ny=512, per_pixel=20, energy=1000.0, energies=[300.0, 1000.0, 3000.0, 5000.0],
-                  spacing=1000.0 / 512, origin=(-500.0, -500.0), z_start=25.0, materials=("si",), rows=512,
-                  cpu_sample=163840, ref_sample=40960,
+    "grating": dict(rows=256, cpu_sample=409600, ref_sample=102400, desc=WORKLOAD),
+    "rough": dict(rows=512, cpu_sample=163840, ref_sample=40960,
                   desc="rough slab: 512x512 Gaussian height field (RMS 3 nm, correlation 10 nm) over 1 um, "
                        "526,334 triangles; 512x512 px x 20 primaries (5,242,880) at E uniform over "
                        "{300, 1000, 3000, 5000} eV, Si-like Kieft tables"),
-    "holes": dict(nx=1024, ny=1024, per_pixel=200, energy=1000.0, energies=None, spacing=2.5,
-                  origin=(-1278.75, -1278.75), z_start=10.0, materials=("sio2", "w", "si"), rows=64,
-                  tune_row=8, cpu_sample=204800, ref_sample=102400,
+    "holes": dict(rows=64, tune_row=8, cpu_sample=204800, ref_sample=102400,
                   desc="contact holes: 32x32 holes (40 nm diameter, 100 nm deep, +-2 nm edge roughness) in a "
                        "SiO2-like film over W-like plugs on a Si-like substrate, 2,506,772 triangles over "
                        "2.56 um; 1024x1024 px at 2.5 nm x 200 primaries at 1 keV, one step = %d pixel rows "
@@ -67,10 +62,16 @@ WORKLOADS = {
 }
 
 
+def workload(name):
+    """Bench settings of a workload merged with its scan definition."""
+    from nebula_b200 import generators as g
+    return dict(g.SCANS[name], **WORKLOADS[name])
+
+
 def configure(args):
     """Point the module's scan constants at the chosen workload."""
     global NX, NY, PER_PIXEL, ENERGY, WORKLOAD
-    w = WORKLOADS[args.workload]
+    w = workload(args.workload)
     NX, NY, PER_PIXEL, ENERGY = w["nx"], w["ny"], w["per_pixel"], w["energy"]
     if args.rows <= 0:
         args.rows = w["rows"]
@@ -128,10 +129,9 @@ def make_workload(tmp, rank=0, rows=None, workload="grating"):
     """Material files (in geometry order), triangles, .tri path and the
     scan's primaries (pixel rows `rows`, all if None)."""
     from nebula_b200 import formats, generators as g
-    w = WORKLOADS[workload]
+    w = g.SCANS[workload]
     mats = [g.make_material(os.path.join(tmp, k + ".mat"), kind=k) for k in w["materials"]]
-    tris = {"grating": g.grating_geometry, "rough": lambda: g.rough_geometry(512),
-            "holes": g.contact_hole_geometry}[workload]()
+    tris = w["geometry"]()
     tri_path = os.path.join(tmp, workload + ".tri")
     formats.write_tri(tri_path, tris)
     recs = g.scan_beam(w["nx"], w["ny"], w["per_pixel"], w["energy"], spacing=w["spacing"], origin=w["origin"],

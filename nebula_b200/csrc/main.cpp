@@ -20,6 +20,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "nbx.h"
@@ -171,7 +172,7 @@ int main(int argc, char** argv) {
                  NBX_VERSION_MINOR, NBX_VERSION_PATCH);
     Cli p;
     p.add("energy-threshold", "Lowest energy to simulate", "0");
-    p.add("capacity", "Electron capacity on the GPU", "1000000");
+    p.add("capacity", "Electron capacity on the GPU (primaries per device run)", "4000000");
     p.add("prescan-size", "Number of electrons to use for prescan", "1000");
     p.add("batch-factor", "Multiplication factor for electron batch size", "0.9");
     p.add("seed", "Random seed", std::to_string(0x78c7e39b));
@@ -343,64 +344,98 @@ int main(int argc, char** argv) {
     };
     static_assert(sizeof(DepositRecord) == 28, "deposit record layout");
     const uint64_t dep_capacity = uint64_t(1) << 27;   // nbx_config default
+
+    // Two-stage pipeline: while the device runs batch k, a helper thread
+    // writes the records of batch k - 1 and reads and converts batch k + 1
+    // (in the energy-deposit mode the next batch's size depends on batch k's
+    // deposits, so it is read after the run).  Tags are batch-relative.
+    struct Batch {
+        uint64_t first = 0, n = 0;
+        bool ok = false;
+        std::vector<nbx_record> pri;
+        std::vector<nbx_particle> part;
+        std::vector<uint32_t> tags;
+    };
+    auto prepare = [&](Batch& b, uint64_t first, uint64_t n) {
+        b.first = first;
+        b.n = n;
+        const nbx_record* pri = src.batch(first, n);
+        b.ok = pri != nullptr;
+        if (!b.ok) return;
+        b.pri.assign(pri, pri + n);
+        if (!sort_primaries) warn.add(pri, n);
+        b.part.resize(n);
+        b.tags.resize(n);
+        for (uint64_t i = 0; i < n; ++i) {
+            std::memcpy(b.part[i].pos, pri[i].pos, 12);
+            std::memcpy(b.part[i].dir, pri[i].dir, 12);
+            b.part[i].E = pri[i].E;
+            b.tags[i] = uint32_t(i);
+        }
+    };
+    std::vector<nbx_record> out, out_prev;
+    std::vector<DepositRecord> dep_out, dep_prev;
+    auto write_prev = [&] {
+        if (!out_prev.empty()) std::fwrite(out_prev.data(), sizeof(nbx_record), out_prev.size(), detect_out);
+        if (!dep_prev.empty()) std::fwrite(dep_prev.data(), sizeof(DepositRecord), dep_prev.size(), deposit_out);
+        out_prev.clear();
+        dep_prev.clear();
+    };
+    std::vector<nbx_detected> det(1u << 20);
     std::vector<nbx_deposit> dep(energy_deposit ? (1u << 20) : 0);
-    std::vector<DepositRecord> dep_out;
     timer.start();
     uint64_t batch = std::max<uint64_t>(capacity, 1);
     if (energy_deposit) batch = std::min<uint64_t>(batch, std::max<uint32_t>(prescan, 1));
-    std::vector<nbx_particle> part;
-    std::vector<uint32_t> tags;
-    std::vector<nbx_detected> det(1u << 20);
-    std::vector<nbx_record> out;
+    Batch cur, next;
+    prepare(cur, 0, std::min(batch, n_pri));
     uint64_t done = 0;
     while (done < n_pri) {
-        const uint64_t n = std::min(batch, n_pri - done);
-        const nbx_record* pri = src.batch(done, n);
-        if (!pri) {
+        if (!cur.ok) {
             std::fprintf(stderr, "Error: could not read primary electrons!\n");
             return die(ctx, NBX_ERR_FORMAT, "primaries");
         }
-        if (!sort_primaries) warn.add(pri, n);
-        part.resize(n);
-        tags.resize(n);
-        for (uint64_t i = 0; i < n; ++i) {
-            std::memcpy(part[i].pos, pri[i].pos, 12);
-            std::memcpy(part[i].dir, pri[i].dir, 12);
-            part[i].E = pri[i].E;
-            tags[i] = uint32_t(done + i);
-        }
+        const uint64_t n = cur.n;
+        const uint64_t next_first = done + n;
+        const bool ahead = !energy_deposit && next_first < n_pri;
         uint64_t acc = 0;
-        if ((rc = nbx_push(ctx, part.data(), tags.data(), n, &acc)) != NBX_OK) return die(ctx, rc, "push");
-        if ((rc = nbx_run(ctx)) != NBX_OK) return die(ctx, rc, "run");
+        if ((rc = nbx_push(ctx, cur.part.data(), cur.tags.data(), n, &acc)) != NBX_OK) return die(ctx, rc, "push");
+        std::thread helper([&] {
+            write_prev();
+            if (ahead) prepare(next, next_first, std::min(batch, n_pri - next_first));
+        });
+        rc = nbx_run(ctx);
+        helper.join();
+        if (rc != NBX_OK) return die(ctx, rc, "run");
+        out.clear();
         for (;;) {
             uint64_t got = 0;
             if ((rc = nbx_flush_detected(ctx, det.data(), det.size(), &got)) != NBX_OK) return die(ctx, rc, "flush");
             if (got == 0) break;
-            out.resize(got);
+            const size_t base = out.size();
+            out.resize(base + got);
             for (uint64_t i = 0; i < got; ++i) {
-                std::memcpy(out[i].pos, det[i].pos, 12);
-                std::memcpy(out[i].dir, det[i].dir, 12);
-                out[i].E = det[i].E;
-                out[i].px = pri[det[i].tag - done].px;
-                out[i].py = pri[det[i].tag - done].py;
+                nbx_record& o = out[base + i];
+                std::memcpy(o.pos, det[i].pos, 12);
+                std::memcpy(o.dir, det[i].dir, 12);
+                o.E = det[i].E;
+                o.px = cur.pri[det[i].tag].px;
+                o.py = cur.pri[det[i].tag].py;
             }
-            std::fwrite(out.data(), sizeof(nbx_record), got, detect_out);
         }
+        dep_out.clear();
         if (energy_deposit) {
-            uint64_t n_dep = 0;
             for (;;) {
                 uint64_t got = 0;
                 if ((rc = nbx_flush_deposits(ctx, dep.data(), dep.size(), &got)) != NBX_OK)
                     return die(ctx, rc, "flush deposits");
                 if (got == 0) break;
-                n_dep += got;
-                dep_out.resize(got);
+                const size_t base = dep_out.size();
+                dep_out.resize(base + got);
                 for (uint64_t i = 0; i < got; ++i) {
                     const nbx_deposit& d = dep[i];
-                    const nbx_record& r = pri[d.tag - done];
-                    dep_out[i] = {d.pos[0], d.pos[1], d.pos[2], d.E, d.dE, r.px, r.py};
+                    const nbx_record& r = cur.pri[d.tag];
+                    dep_out[base + i] = {d.pos[0], d.pos[1], d.pos[2], d.E, d.dE, r.px, r.py};
                 }
-                std::fwrite(dep_out.data(), sizeof(DepositRecord), got, deposit_out);
             }
             nbx_stats st;
             nbx_get_stats(ctx, &st);
@@ -410,13 +445,18 @@ int main(int argc, char** argv) {
                 return die(ctx, NBX_ERR_CAPACITY, "deposit buffer");
             }
             // size the next batches from the deposits per primary seen so far
-            const double per_primary = double(n_dep) / double(n);
+            const double per_primary = double(dep_out.size()) / double(n);
             const double fit = batch_factor * double(dep_capacity) / std::max(per_primary, 1.0);
             batch = std::max<uint64_t>(1, std::min<uint64_t>(std::max<uint64_t>(capacity, 1), uint64_t(fit)));
+            if (next_first < n_pri) prepare(next, next_first, std::min(batch, n_pri - next_first));
         }
-        done += n;
+        std::swap(out, out_prev);
+        std::swap(dep_out, dep_prev);
+        std::swap(cur, next);
+        done = next_first;
         std::fprintf(stderr, " \rProgress %.2f%%", 100.0 * double(done) / double(n_pri));
     }
+    write_prev();
     std::fflush(stdout);
     if (!sort_primaries) {
         std::fprintf(stderr, "\n");

@@ -553,3 +553,70 @@ def scan_beam(nx, ny, per_pixel, energy, spacing=1.0, origin=(-128.0, -128.0), z
     else:
         E = np.asarray(energies, np.float64)[rng.integers(0, len(energies), n)]
     return formats.make_records(pos, dirs, E, px, py)
+
+
+def write_scan_pri(path, nx, ny, per_pixel, energy, rows_per_block=16, seed=0, **scan_kw):
+    """Write a raster scan (``scan_beam`` arguments) to a ``.pri`` file,
+    ``rows_per_block`` pixel rows at a time, so that a full-size scan (the
+    1024 x 1024 x 200 contact-hole scan is 7.5 GB) never sits in memory.
+    Block k draws from the Philox stream keyed by (seed, k).  Returns the
+    number of primaries written."""
+    n = 0
+    with open(path, "wb") as f:
+        for k, r0 in enumerate(range(0, ny, rows_per_block)):
+            recs = scan_beam(nx, ny, per_pixel, energy, seed=[seed, k],
+                             rows=range(r0, min(ny, r0 + rows_per_block)), **scan_kw)
+            recs.tofile(f)
+            n += len(recs)
+    return n
+
+
+# The scans of the benchmark workloads (BASELINE configs 2, 3 and 5): geometry,
+# materials in geometry order, and the raster scan.
+SCANS = {
+    "grating": dict(geometry=lambda: grating_geometry(), materials=("si",), nx=256, ny=256, per_pixel=100,
+                    energy=500.0, energies=None, spacing=1.0, origin=(-128.0, -128.0), z_start=75.0),
+    "rough": dict(geometry=lambda: rough_geometry(512), materials=("si",), nx=512, ny=512, per_pixel=20,
+                  energy=1000.0, energies=[300.0, 1000.0, 3000.0, 5000.0], spacing=1000.0 / 512,
+                  origin=(-500.0, -500.0), z_start=25.0),
+    "holes": dict(geometry=lambda: contact_hole_geometry(), materials=("sio2", "w", "si"), nx=1024, ny=1024,
+                  per_pixel=200, energy=1000.0, energies=None, spacing=2.5, origin=(-1278.75, -1278.75),
+                  z_start=10.0),
+}
+
+
+def write_workload(name, outdir, rows=None, seed=0):
+    """Write one benchmark workload as reference-format inputs: ``<name>.tri``,
+    one ``<kind>.mat`` per material and ``<name>.pri`` (the first ``rows``
+    pixel rows of the scan, all if None).  Returns the paths, ready for
+    ``nebula_b200 <tri> <pri> <mat>...``."""
+    import os
+    w = SCANS[name]
+    os.makedirs(outdir, exist_ok=True)
+    tri = os.path.join(outdir, name + ".tri")
+    formats.write_tri(tri, w["geometry"]())
+    mats = [make_material(os.path.join(outdir, k + ".mat"), kind=k) for k in w["materials"]]
+    pri = os.path.join(outdir, name + ".pri")
+    write_scan_pri(pri, w["nx"], w["ny"] if rows is None else min(rows, w["ny"]), w["per_pixel"], w["energy"],
+                   seed=seed, energies=w["energies"], spacing=w["spacing"], origin=w["origin"],
+                   z_start=w["z_start"])
+    return {"tri": tri, "pri": pri, "mats": mats}
+
+
+def main(argv=None):
+    """python -m nebula_b200.generators {grating,rough,holes} OUTDIR [--rows N] [--seed S]"""
+    import argparse
+    ap = argparse.ArgumentParser(prog="python -m nebula_b200.generators",
+                                 description="write a benchmark workload as .tri/.mat/.pri inputs")
+    ap.add_argument("workload", choices=sorted(SCANS))
+    ap.add_argument("outdir")
+    ap.add_argument("--rows", type=int, default=None, help="first N pixel rows of the scan (default: all)")
+    ap.add_argument("--seed", type=int, default=0)
+    args = ap.parse_args(argv)
+    out = write_workload(args.workload, args.outdir, rows=args.rows, seed=args.seed)
+    print(" ".join([out["tri"], out["pri"]] + out["mats"]))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

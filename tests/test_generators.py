@@ -95,3 +95,25 @@ def test_contact_hole_cells_share_vertices():
         if c == 1:
             for q in (uniq[a], uniq[b]):
                 assert abs(abs(q[0]) - half) < 1e-9 or abs(abs(q[1]) - half) < 1e-9
+
+
+def test_streamed_scan_matches_blocks(tmp_path):
+    """write_scan_pri streams the scan block by block: the file holds every
+    pixel's primaries, in row-major order, and equals the concatenation of
+    the per-block scans."""
+    p = str(tmp_path / "s.pri")
+    n = g.write_scan_pri(p, 24, 21, 3, 800.0, rows_per_block=8, seed=5, spacing=2.0, origin=(-24.0, -21.0))
+    r = formats.read_pri(p)
+    assert n == len(r) == 24 * 21 * 3
+    assert np.array_equal(r["py"], np.repeat(np.arange(21), 24 * 3))
+    blocks = [g.scan_beam(24, 21, 3, 800.0, seed=[5, k], rows=range(8 * k, min(21, 8 * k + 8)), spacing=2.0,
+                          origin=(-24.0, -21.0)) for k in range(3)]
+    assert np.array_equal(np.concatenate(blocks).view(np.uint8), r.view(np.uint8))
+
+
+def test_workload_writer(tmp_path):
+    out = g.write_workload("grating", str(tmp_path), rows=2)
+    assert len(out["mats"]) == 1
+    r = formats.read_pri(out["pri"])
+    assert len(r) == 2 * 256 * 100 and set(np.unique(r["py"])) == {0, 1}
+    assert len(formats.read_tri(out["tri"])) == len(g.grating_geometry())
