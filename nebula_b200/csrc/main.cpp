@@ -16,6 +16,7 @@
 #include <cstring>
 #include <iostream>
 #include <map>
+#include <mutex>
 #include <numeric>
 #include <sstream>
 #include <stdexcept>
@@ -178,6 +179,7 @@ int main(int argc, char** argv) {
     p.add("seed", "Random seed", std::to_string(0x78c7e39b));
     p.add("sort-primaries", "Sort primary electrons before simulation", "0");
     p.add("device", "CUDA device ordinal", "0");
+    p.add("streams", "Device contexts working on batches at once (one with --energy-deposit)", "2");
     p.add("inelastic", "Inelastic model: kieft (Kieft & Bosch) or penn (full Penn, the reference's stock build)",
           "kieft");
     p.add("energy-deposit", "Also write energy deposits, as the reference's nebula_cpu_energydep", "0");
@@ -197,11 +199,12 @@ int main(int argc, char** argv) {
     const uint32_t seed = p.get<uint32_t>("seed");
     const bool sort_primaries = p.get<bool>("sort-primaries");
     const int device = p.get<int>("device");
+    const int streams = p.get<int>("streams");
     const std::string inelastic = p.get<std::string>("inelastic");
     const bool energy_deposit = p.get<bool>("energy-deposit");
     const std::string detect_filename = p.get<std::string>("detect-filename");
     const std::string deposit_filename = p.get<std::string>("deposit-filename");
-    if (p.positional.size() < 3 || capacity == 0 || prescan == 0 || batch_factor <= 0 ||
+    if (p.positional.size() < 3 || capacity == 0 || prescan == 0 || batch_factor <= 0 || streams < 1 || streams > 8 ||
         (inelastic != "kieft" && inelastic != "penn")) {
         p.usage(std::cerr);
         return 1;
@@ -313,12 +316,19 @@ int main(int argc, char** argv) {
     cfg.record_detected = 1;
     cfg.record_capacity = 1ull << 24;
     cfg.record_deposits = energy_deposit ? 1 : 0;
-    nbx_ctx* ctx = nullptr;
-    rc = nbx_create(&ctx, &cfg);
-    if (rc != NBX_OK) return die(nullptr, rc, "nbx_create");
-    if ((rc = nbx_set_geometry(ctx, oct)) != NBX_OK) return die(ctx, rc, "set_geometry");
-    for (auto* m : mats)
-        if ((rc = nbx_add_material(ctx, m)) != NBX_OK) return die(ctx, rc, "add_material");
+    // Several contexts on the one device: while one drains the last long
+    // cascades of its batch, the next batch's kernel fills the freed SMs.
+    const int n_ctx = energy_deposit ? 1 : streams;
+    std::vector<nbx_ctx*> ctxs;
+    for (int k = 0; k < n_ctx; ++k) {
+        nbx_ctx* c = nullptr;
+        rc = nbx_create(&c, &cfg);
+        if (rc != NBX_OK) return die(nullptr, rc, "nbx_create");
+        ctxs.push_back(c);
+        if ((rc = nbx_set_geometry(c, oct)) != NBX_OK) return die(c, rc, "set_geometry");
+        for (auto* m : mats)
+            if ((rc = nbx_add_material(c, m)) != NBX_OK) return die(c, rc, "add_material");
+    }
     std::fprintf(stderr, "\nLoaded %llu triangles.\nLoaded %llu primaries.\nLoaded %zu materials.\n\n",
                  (unsigned long long)oct->n_triangles, (unsigned long long)n_pri, mats.size());
 
@@ -345,118 +355,132 @@ int main(int argc, char** argv) {
     static_assert(sizeof(DepositRecord) == 28, "deposit record layout");
     const uint64_t dep_capacity = uint64_t(1) << 27;   // nbx_config default
 
-    // Two-stage pipeline: while the device runs batch k, a helper thread
-    // writes the records of batch k - 1 and reads and converts batch k + 1
-    // (in the energy-deposit mode the next batch's size depends on batch k's
-    // deposits, so it is read after the run).  Tags are batch-relative.
+    // Worker threads, one per context, take the next batch from the file
+    // (in order, under a lock), run it and write its records (under a second
+    // lock).  A batch's primaries keep their global index as the uid of their
+    // random streams, so the records do not depend on the number of workers
+    // or on which worker ran a batch; only their order in the output does, as
+    // with the reference's worker threads.  Tags are batch-relative.
     struct Batch {
         uint64_t first = 0, n = 0;
-        bool ok = false;
         std::vector<nbx_record> pri;
         std::vector<nbx_particle> part;
         std::vector<uint32_t> tags;
     };
-    auto prepare = [&](Batch& b, uint64_t first, uint64_t n) {
-        b.first = first;
-        b.n = n;
-        const nbx_record* pri = src.batch(first, n);
-        b.ok = pri != nullptr;
-        if (!b.ok) return;
-        b.pri.assign(pri, pri + n);
-        if (!sort_primaries) warn.add(pri, n);
-        b.part.resize(n);
-        b.tags.resize(n);
-        for (uint64_t i = 0; i < n; ++i) {
-            std::memcpy(b.part[i].pos, pri[i].pos, 12);
-            std::memcpy(b.part[i].dir, pri[i].dir, 12);
-            b.part[i].E = pri[i].E;
-            b.tags[i] = uint32_t(i);
-        }
-    };
-    std::vector<nbx_record> out, out_prev;
-    std::vector<DepositRecord> dep_out, dep_prev;
-    auto write_prev = [&] {
-        if (!out_prev.empty()) std::fwrite(out_prev.data(), sizeof(nbx_record), out_prev.size(), detect_out);
-        if (!dep_prev.empty()) std::fwrite(dep_prev.data(), sizeof(DepositRecord), dep_prev.size(), deposit_out);
-        out_prev.clear();
-        dep_prev.clear();
-    };
-    std::vector<nbx_detected> det(1u << 20);
-    std::vector<nbx_deposit> dep(energy_deposit ? (1u << 20) : 0);
-    timer.start();
+    std::mutex in_mu, out_mu;
+    uint64_t next_first = 0, done = 0;
     uint64_t batch = std::max<uint64_t>(capacity, 1);
     if (energy_deposit) batch = std::min<uint64_t>(batch, std::max<uint32_t>(prescan, 1));
-    Batch cur, next;
-    prepare(cur, 0, std::min(batch, n_pri));
-    uint64_t done = 0;
-    while (done < n_pri) {
-        if (!cur.ok) {
-            std::fprintf(stderr, "Error: could not read primary electrons!\n");
-            return die(ctx, NBX_ERR_FORMAT, "primaries");
+    int failed_rc = NBX_OK;
+    std::string failed_what;
+    nbx_ctx* failed_ctx = nullptr;
+    auto fail_with = [&](nbx_ctx* c, int code, const char* what) {
+        std::lock_guard<std::mutex> lk(in_mu);
+        if (failed_rc == NBX_OK) {
+            failed_rc = code;
+            failed_what = what;
+            failed_ctx = c;
         }
-        const uint64_t n = cur.n;
-        const uint64_t next_first = done + n;
-        const bool ahead = !energy_deposit && next_first < n_pri;
-        uint64_t acc = 0;
-        if ((rc = nbx_push(ctx, cur.part.data(), cur.tags.data(), n, &acc)) != NBX_OK) return die(ctx, rc, "push");
-        std::thread helper([&] {
-            write_prev();
-            if (ahead) prepare(next, next_first, std::min(batch, n_pri - next_first));
-        });
-        rc = nbx_run(ctx);
-        helper.join();
-        if (rc != NBX_OK) return die(ctx, rc, "run");
-        out.clear();
+    };
+    auto worker = [&](nbx_ctx* c) {
+        Batch b;
+        std::vector<nbx_detected> det(1u << 20);
+        std::vector<nbx_deposit> dep(energy_deposit ? (1u << 20) : 0);
+        std::vector<nbx_record> out;
+        std::vector<DepositRecord> dep_out;
         for (;;) {
-            uint64_t got = 0;
-            if ((rc = nbx_flush_detected(ctx, det.data(), det.size(), &got)) != NBX_OK) return die(ctx, rc, "flush");
-            if (got == 0) break;
-            const size_t base = out.size();
-            out.resize(base + got);
-            for (uint64_t i = 0; i < got; ++i) {
-                nbx_record& o = out[base + i];
-                std::memcpy(o.pos, det[i].pos, 12);
-                std::memcpy(o.dir, det[i].dir, 12);
-                o.E = det[i].E;
-                o.px = cur.pri[det[i].tag].px;
-                o.py = cur.pri[det[i].tag].py;
+            {
+                std::lock_guard<std::mutex> lk(in_mu);
+                if (failed_rc != NBX_OK || next_first >= n_pri) return;
+                b.first = next_first;
+                b.n = std::min(batch, n_pri - next_first);
+                next_first += b.n;
+                const nbx_record* pri = src.batch(b.first, b.n);
+                if (!pri) {
+                    failed_rc = NBX_ERR_FORMAT;
+                    failed_what = "primaries";
+                    std::fprintf(stderr, "Error: could not read primary electrons!\n");
+                    return;
+                }
+                b.pri.assign(pri, pri + b.n);
+                if (!sort_primaries) warn.add(pri, b.n);
             }
-        }
-        dep_out.clear();
-        if (energy_deposit) {
+            b.part.resize(b.n);
+            b.tags.resize(b.n);
+            for (uint64_t i = 0; i < b.n; ++i) {
+                std::memcpy(b.part[i].pos, b.pri[i].pos, 12);
+                std::memcpy(b.part[i].dir, b.pri[i].dir, 12);
+                b.part[i].E = b.pri[i].E;
+                b.tags[i] = uint32_t(i);
+            }
+            int r;
+            uint64_t acc = 0;
+            if ((r = nbx_set_uid_base(c, b.first)) != NBX_OK) return fail_with(c, r, "uid base");
+            if ((r = nbx_push(c, b.part.data(), b.tags.data(), b.n, &acc)) != NBX_OK) return fail_with(c, r, "push");
+            if ((r = nbx_run(c)) != NBX_OK) return fail_with(c, r, "run");
+            out.clear();
             for (;;) {
                 uint64_t got = 0;
-                if ((rc = nbx_flush_deposits(ctx, dep.data(), dep.size(), &got)) != NBX_OK)
-                    return die(ctx, rc, "flush deposits");
+                if ((r = nbx_flush_detected(c, det.data(), det.size(), &got)) != NBX_OK) return fail_with(c, r, "flush");
                 if (got == 0) break;
-                const size_t base = dep_out.size();
-                dep_out.resize(base + got);
+                const size_t base = out.size();
+                out.resize(base + got);
                 for (uint64_t i = 0; i < got; ++i) {
-                    const nbx_deposit& d = dep[i];
-                    const nbx_record& r = cur.pri[d.tag];
-                    dep_out[base + i] = {d.pos[0], d.pos[1], d.pos[2], d.E, d.dE, r.px, r.py};
+                    nbx_record& o = out[base + i];
+                    std::memcpy(o.pos, det[i].pos, 12);
+                    std::memcpy(o.dir, det[i].dir, 12);
+                    o.E = det[i].E;
+                    o.px = b.pri[det[i].tag].px;
+                    o.py = b.pri[det[i].tag].py;
                 }
             }
-            nbx_stats st;
-            nbx_get_stats(ctx, &st);
-            if (st.deposits_dropped) {
-                std::fprintf(stderr, "\nError: %llu energy deposits did not fit the device buffer; lower --batch-factor\n",
-                             (unsigned long long)st.deposits_dropped);
-                return die(ctx, NBX_ERR_CAPACITY, "deposit buffer");
+            dep_out.clear();
+            if (energy_deposit) {
+                for (;;) {
+                    uint64_t got = 0;
+                    if ((r = nbx_flush_deposits(c, dep.data(), dep.size(), &got)) != NBX_OK)
+                        return fail_with(c, r, "flush deposits");
+                    if (got == 0) break;
+                    const size_t base = dep_out.size();
+                    dep_out.resize(base + got);
+                    for (uint64_t i = 0; i < got; ++i) {
+                        const nbx_deposit& d = dep[i];
+                        const nbx_record& rec = b.pri[d.tag];
+                        dep_out[base + i] = {d.pos[0], d.pos[1], d.pos[2], d.E, d.dE, rec.px, rec.py};
+                    }
+                }
+                nbx_stats st;
+                nbx_get_stats(c, &st);
+                if (st.deposits_dropped) {
+                    std::fprintf(stderr, "\nError: %llu energy deposits did not fit the device buffer; lower --batch-factor\n",
+                                 (unsigned long long)st.deposits_dropped);
+                    return fail_with(c, NBX_ERR_CAPACITY, "deposit buffer");
+                }
+                // size the next batches from the deposits per primary seen so
+                // far (one context in this mode, so batches run in turn)
+                const double per_primary = double(dep_out.size()) / double(b.n);
+                const double fit = batch_factor * double(dep_capacity) / std::max(per_primary, 1.0);
+                std::lock_guard<std::mutex> lk(in_mu);
+                batch = std::max<uint64_t>(1, std::min<uint64_t>(std::max<uint64_t>(capacity, 1), uint64_t(fit)));
             }
-            // size the next batches from the deposits per primary seen so far
-            const double per_primary = double(dep_out.size()) / double(n);
-            const double fit = batch_factor * double(dep_capacity) / std::max(per_primary, 1.0);
-            batch = std::max<uint64_t>(1, std::min<uint64_t>(std::max<uint64_t>(capacity, 1), uint64_t(fit)));
-            if (next_first < n_pri) prepare(next, next_first, std::min(batch, n_pri - next_first));
+            std::lock_guard<std::mutex> lk(out_mu);
+            if (!out.empty()) std::fwrite(out.data(), sizeof(nbx_record), out.size(), detect_out);
+            if (!dep_out.empty()) std::fwrite(dep_out.data(), sizeof(DepositRecord), dep_out.size(), deposit_out);
+            done += b.n;
+            std::fprintf(stderr, " \rProgress %.2f%%", 100.0 * double(done) / double(n_pri));
         }
-        std::swap(out, out_prev);
-        std::swap(dep_out, dep_prev);
-        std::swap(cur, next);
-        done = next_first;
-        std::fprintf(stderr, " \rProgress %.2f%%", 100.0 * double(done) / double(n_pri));
+    };
+    timer.start();
+    {
+        std::vector<std::thread> threads;
+        for (nbx_ctx* c : ctxs) threads.emplace_back(worker, c);
+        for (auto& t : threads) t.join();
     }
-    write_prev();
+    if (failed_rc != NBX_OK) {
+        const int r = die(failed_ctx, failed_rc, failed_what.c_str());
+        for (nbx_ctx* c : ctxs) nbx_destroy(c);
+        return r;
+    }
     std::fflush(stdout);
     if (!sort_primaries) {
         std::fprintf(stderr, "\n");
@@ -467,15 +491,23 @@ int main(int argc, char** argv) {
         if (deposit_out != stdout) std::fclose(deposit_out);
     }
     timer.stop("Simulation");
-    nbx_stats st;
-    nbx_get_stats(ctx, &st);
+    nbx_stats st{};
+    for (nbx_ctx* c : ctxs) {
+        nbx_stats one;
+        nbx_get_stats(c, &one);
+        st.events_elastic += one.events_elastic;
+        st.events_inelastic += one.events_inelastic;
+        st.events_boundary += one.events_boundary;
+        st.detected += one.detected;
+        st.records_dropped += one.records_dropped;
+    }
     std::fprintf(stderr, "\n\nSimulation successful!\n  events: %llu elastic, %llu inelastic, %llu boundary; %llu detected",
                  (unsigned long long)st.events_elastic, (unsigned long long)st.events_inelastic,
                  (unsigned long long)st.events_boundary, (unsigned long long)st.detected);
     if (st.records_dropped) std::fprintf(stderr, " (%llu records dropped)", (unsigned long long)st.records_dropped);
     std::fprintf(stderr, "\n\n");
     timer.print();
-    nbx_destroy(ctx);
+    for (nbx_ctx* c : ctxs) nbx_destroy(c);
     for (auto* m : mats) nbx_material_free(m);
     nbx_octree_free(oct);
     return 0;

@@ -2,9 +2,10 @@
 nebula_cpu_mt: same inputs (.tri, .pri, .mat), 36-byte detected records on
 stdout.
 
-* Primaries are streamed from the .pri file in --capacity batches; every
-  primary keeps its own random stream, so the detected records do not depend
-  on the batch size (byte-identical record sets).
+* Primaries are streamed from the .pri file in --capacity batches, run by
+  --streams device contexts at once; every primary keeps its own random
+  stream, so the detected records depend on neither (byte-identical record
+  sets).
 * Against the reference's own cpu_mt_main program (oracle/_ref, Kieft and
   stock full Penn builds): SE/BSE yields per primary within 3 sigma.
 * --sort-primaries reorders the primaries (Morton order) and still reports
@@ -44,10 +45,12 @@ def _sorted_bytes(recs):
 
 
 def test_batches_do_not_change_results(inputs, tmp_path):
+    """One batch on one context against 4 batches spread over 3 contexts
+    working at once: byte-identical record sets."""
     pri = str(tmp_path / "p.pri")
     formats.write_pri(pri, _beam(2500))
-    one = _cli(["--capacity", "5000", inputs["cube_tri"], pri, inputs["si"]])
-    many = _cli(["--capacity", "700", inputs["cube_tri"], pri, inputs["si"]])
+    one = _cli(["--capacity", "5000", "--streams", "1", inputs["cube_tri"], pri, inputs["si"]])
+    many = _cli(["--capacity", "700", "--streams", "3", inputs["cube_tri"], pri, inputs["si"]])
     assert len(one) > 500
     assert np.array_equal(_sorted_bytes(one), _sorted_bytes(many))
 
