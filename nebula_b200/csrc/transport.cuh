@@ -214,6 +214,10 @@ __device__ __forceinline__ bool in_domain(const Geometry& g, V3 p) {
            (p.z > g.cz - g.hz) && (p.z < g.cz + g.hz);
 }
 
+// The octant offset (bit - 0.5) of geometry/octree.inl:65-67,79-81, as a
+// select: exactly +-0.5, without an integer-to-float conversion.
+__device__ __forceinline__ float half_step(unsigned bit) { return bit ? 0.5f : -0.5f; }
+
 // Per-thread memo of the last octree leaf a descent reached, kept in shared
 // memory as 13 words strided by the block size: location code (2 words), raw
 // leaf value, the leaf's AABB centre and scale (ax, ay, az, aw) exactly as the
@@ -267,9 +271,9 @@ __device__ __forceinline__ float propagate(const Geometry& g, V3 start, V3 dir, 
                 if (octant & 1) lox = ax; else hix = ax;
                 if (octant & 2) loy = ay; else hiy = ay;
                 if (octant & 4) loz = az; else hiz = az;
-                ax += aw * g.hx * (float(octant & 1) - 0.5f);
-                ay += aw * g.hy * (float((octant & 2) >> 1) - 0.5f);
-                az += aw * g.hz * (float((octant & 4) >> 2) - 0.5f);
+                ax += aw * g.hx * half_step(octant & 1);
+                ay += aw * g.hy * half_step(octant & 2);
+                az += aw * g.hz * half_step(octant & 4);
                 aw *= 0.5f;
             }
             while (index >= 0) {
@@ -282,9 +286,9 @@ __device__ __forceinline__ float propagate(const Geometry& g, V3 start, V3 dir, 
                 if (octant & 1) lox = ax; else hix = ax;
                 if (octant & 2) loy = ay; else hiy = ay;
                 if (octant & 4) loz = az; else hiz = az;
-                ax += aw * g.hx * (float(octant & 1) - 0.5f);
-                ay += aw * g.hy * (float((octant & 2) >> 1) - 0.5f);
-                az += aw * g.hz * (float((octant & 4) >> 2) - 0.5f);
+                ax += aw * g.hx * half_step(octant & 1);
+                ay += aw * g.hy * half_step(octant & 2);
+                az += aw * g.hz * half_step(octant & 4);
                 aw *= 0.5f;
             }
             if (cache.base) {

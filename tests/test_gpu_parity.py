@@ -315,12 +315,17 @@ def test_whole_run_grating_rows_vs_reference(inputs, oracle_built, tmp_path):
     ctx.close()
 
 
-def test_whole_run_contact_holes_vs_reference(inputs, oracle_built, tmp_path):
+@pytest.mark.parametrize("model", ["kieft", "penn"])
+def test_whole_run_contact_holes_vs_reference(inputs, oracle_built, tmp_path, model):
     """Three materials (SiO2-like film, W-like plugs, Si-like substrate) on
     the 3 x 3 contact-hole array (22,052 triangles): a 1 keV line scan
-    across the middle hole, 32 px x 400 primaries.  Per-pixel SE and BSE
-    yields of the GPU path and the reference CPU path agree by chi-square,
+    across the middle hole, 32 px x 400 primaries, Kieft and full Penn
+    inelastic models.  Per-pixel SE and BSE yields of the GPU path and the
+    reference CPU path (its Kieft or stock build) agree by chi-square,
     totals within 3 sigma, events per primary within 5 %."""
+    penn = model == "penn"
+    if penn and not oracle.have_ref(penn=True):
+        pytest.skip("reference full Penn build unavailable")
     per_px, nx = 400, 32
     recs = g.scan_beam(nx, 1, per_px, 1000.0, spacing=2.5, origin=(-38.75, 0.0), z_start=10.0, seed=9)
     n = len(recs)
@@ -330,9 +335,9 @@ def test_whole_run_contact_holes_vs_reference(inputs, oracle_built, tmp_path):
     pri = str(tmp_path / "holes.pri")
     formats.write_pri(pri, tagged)
     mats = [inputs["sio2"], inputs["w"], inputs["si"]]
-    ref_recs, st, _ = oracle.ref_run(inputs["holes_tri"], pri, mats, seed=23, count_events=True)
+    ref_recs, st, _ = oracle.ref_run(inputs["holes_tri"], pri, mats, seed=23, count_events=True, penn=penn)
     rse, rbse = _per_primary_from_records(ref_recs, n)
-    ctx = nb.setup(inputs["holes"], mats, device=0, seed=29)
+    ctx = nb.setup(inputs["holes"], mats, device=0, seed=29, inelastic=model)
     s, se, bse = _run_gpu(ctx, recs)
     pix = np.arange(n) // per_px
     for mine, ref in ((se, rse), (bse, rbse)):

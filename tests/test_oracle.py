@@ -189,12 +189,17 @@ def test_penn_whole_run_statistics(oracle_built, inputs, tmp_path):
     assert abs(ev_o - ev_r) / ev_r < 0.05
 
 
-def test_multi_material_contact_holes_statistics(oracle_built, inputs, tmp_path):
+@pytest.mark.parametrize("penn", [False, True])
+def test_multi_material_contact_holes_statistics(oracle_built, inputs, tmp_path, penn):
     """Three materials (SiO2-like film, W-like plugs, Si-like substrate) on
     the 3 x 3 contact-hole array: a 1 keV line scan across the middle hole
     (32 px x 250 primaries), the C restatement against the reference's CPU
-    path.  Per-pixel SE and BSE yields agree by chi-square (sigma from the
-    per-primary variances), totals within 3 sigma, events within 5 %."""
+    path, with the Kieft and with the full Penn inelastic model (the stock
+    reference build).  Per-pixel SE and BSE yields agree by chi-square (sigma
+    from the per-primary variances), totals within 3 sigma, events within
+    5 %."""
+    if penn and not oracle_built.have_ref(penn=True):
+        pytest.skip("reference full Penn build unavailable")
     per_px, nx = 250, 32
     recs = g.scan_beam(nx, 1, per_px, 1000.0, spacing=2.5, origin=(-38.75, 0.0), z_start=10.0, seed=9)
     n = len(recs)
@@ -204,16 +209,16 @@ def test_multi_material_contact_holes_statistics(oracle_built, inputs, tmp_path)
     pri = str(tmp_path / "holes.pri")
     formats.write_pri(pri, tagged)
     mats = [inputs["sio2"], inputs["w"], inputs["si"]]
-    ref_recs, st, _ = oracle_built.ref_run(inputs["holes_tri"], pri, mats, seed=17, count_events=True)
+    ref_recs, st, _ = oracle_built.ref_run(inputs["holes_tri"], pri, mats, seed=17, count_events=True, penn=penn)
     pg = oracle_built.PortGeometry(inputs["holes"])
-    rms = [oracle_built.RefMaterial(m) for m in mats]
+    rms = [oracle_built.RefMaterial(m, penn=penn) for m in mats]
     pms, arr = oracle_built.port_materials(rms)
     prim = np.zeros((n, 7), np.float32)
     prim[:, 0:3] = recs["pos"]
     prim[:, 3:6] = recs["dir"]
     prim[:, 6] = recs["E"]
     c, se, bse, _, _ = oracle_built.port_run(pg, arr, prim, np.arange(n, dtype=np.uint32), 19,
-                                             max_energy=min(m.max_energy for m in rms))
+                                             max_energy=min(m.max_energy for m in rms), penn=penn)
     px = ref_recs["px"].astype(np.int64)
     se_r = np.bincount(px[ref_recs["E"] < 50], minlength=n).astype(float)
     bse_r = np.bincount(px[ref_recs["E"] >= 50], minlength=n).astype(float)
