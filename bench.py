@@ -402,10 +402,13 @@ def main():
         ctx.set_tag_range(n)
         tuned = (args.variant, args.block or 128)
     else:
-        # records are row-major: 16 pixel rows from `tune_row` (the contact
-        # holes' first band of holes; the grating and the slab are uniform)
-        r0 = min(WORKLOADS[args.workload].get("tune_row", 0), max(0, args.rows - 16))
-        sample = np.arange(r0 * NX * PER_PIXEL, min(n, (r0 + 16) * NX * PER_PIXEL))
+        # records are row-major: at least 16 pixel rows and about 1.6 M
+        # primaries (short runs rank the launch shapes by their tails) from
+        # `tune_row` (the contact holes' first band of holes; the grating and
+        # the slab are uniform)
+        tune_rows = min(args.rows, max(16, -(-1600000 // (NX * PER_PIXEL))))
+        r0 = min(WORKLOADS[args.workload].get("tune_row", 0), max(0, args.rows - tune_rows))
+        sample = np.arange(r0 * NX * PER_PIXEL, min(n, (r0 + tune_rows) * NX * PER_PIXEL))
         tuned = ctx.autotune(prim[sample], tags[sample])
 
     def one_step():
