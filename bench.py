@@ -491,11 +491,14 @@ def main():
         peak, peak_kind = measured_peaks()
         b_event, b_parts = algorithmic_bytes_per_event(tris, mats, recs, 0x78C7E39B, penn=args.inelastic == "penn")
         achieved = events * b_event / (sum(dev_ms) / 1000.0) / 1e9
+        # DRAM bytes per launch: the ncu capture's bytes per event (Kieft
+        # model, this workload) times the events of one step, whose first
+        # generation's launch carries the whole scan
         traffic = None
-        tp = os.path.join(ROOT, "profiles", "transport_kernel_traffic.json")
-        if os.path.exists(tp) and args.inelastic == "kieft" and args.workload == "grating":   # captured there
+        tp = os.path.join(ROOT, "profiles", "transport_kernel_traffic_%s.json" % args.workload)
+        if os.path.exists(tp) and args.inelastic == "kieft":
             with open(tp) as f:
-                traffic = json.load(f).get("dram_bytes_per_launch")
+                traffic = json.load(f)["dram_bytes_per_event"] * events / args.steps
         cpu = None if args.no_cpu_baseline else cpu_baseline(tri_path, mats, recs, tmp,
                                                               WORKLOADS[args.workload]["cpu_sample"],
                                                               penn=args.inelastic == "penn")
