@@ -19,6 +19,8 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import shutil
+import sys
 
 import numpy as np
 
@@ -43,6 +45,15 @@ def build(reference_dir="/root/reference/source"):
     subprocess.run(["make", "-s", "-C", HERE, "port"], check=True)
     if os.path.isdir(reference_dir):
         subprocess.run(["make", "-s", "-C", HERE, "ref", "REF=" + reference_dir], check=True)
+        # the reference's GPU program, when nvcc is present
+        if shutil.which(os.environ.get("NVCC", "nvcc")) or os.path.exists("/usr/local/cuda/bin/nvcc"):
+            env = dict(os.environ)
+            if not shutil.which(env.get("NVCC", "nvcc")):
+                env["NVCC"] = "/usr/local/cuda/bin/nvcc"
+            # optional: the GPU-to-GPU comparison only; a failed build leaves it out
+            r = subprocess.run(["make", "-s", "-C", HERE, "gpu", "REF=" + reference_dir], check=False, env=env)
+            if r.returncode != 0:
+                print("oracle: the reference's GPU program did not build; it is left out", file=sys.stderr)
 
 
 def have_ref(penn=False):
