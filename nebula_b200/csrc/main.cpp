@@ -24,6 +24,10 @@
 #include <thread>
 #include <vector>
 
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include "nbx.h"
 
 namespace {
@@ -127,6 +131,12 @@ struct PriWarnings {
             dir0 += !(std::fabs(r.dir[0]) > eps || std::fabs(r.dir[1]) > eps || std::fabs(r.dir[2]) > eps);
         }
     }
+    void merge(const PriWarnings& o) {
+        outside += o.outside;
+        low += o.low;
+        high += o.high;
+        dir0 += o.dir0;
+    }
     void print() const {
         if (outside) std::fprintf(stderr, "WARNING: %llu primary electrons starting outside geometry.\n", (unsigned long long)outside);
         if (low) std::fprintf(stderr, "WARNING: %llu primary electrons starting with low kinetic energy.\n", (unsigned long long)low);
@@ -138,31 +148,42 @@ struct PriWarnings {
 };
 
 // Primaries either read whole (for sorting) or streamed from the file in
-// batches; batch(first, n) returns records first .. first + n - 1.
+// batches; read(first, n, out) copies records first .. first + n - 1 with a
+// positional read, so batches can be read by several threads at once.
 struct PriSource {
     nbx_record* all = nullptr;
     uint64_t count = 0;
-    FILE* f = nullptr;
-    std::vector<nbx_record> buf;
+    int fd = -1;
     bool open(const std::string& path, bool whole) {
         if (whole) return nbx_load_pri(path.c_str(), &all, &count) == NBX_OK && count > 0;
-        f = std::fopen(path.c_str(), "rb");
-        if (!f) return false;
-        if (std::fseek(f, 0, SEEK_END) != 0) return false;
-        const long long size = std::ftell(f);
-        std::fseek(f, 0, SEEK_SET);
+        fd = ::open(path.c_str(), O_RDONLY);
+        if (fd < 0) return false;
+        struct stat st;
+        if (fstat(fd, &st) != 0) return false;
+        const long long size = st.st_size;
         if (size <= 0 || size % 36 != 0) return false;   // "Unexpected end of primaries file"
         count = uint64_t(size) / 36;
         return true;
     }
-    const nbx_record* batch(uint64_t first, uint64_t n) {
-        if (all) return all + first;
-        buf.resize(n);
-        return std::fread(buf.data(), 36, n, f) == n ? buf.data() : nullptr;
+    bool read(uint64_t first, uint64_t n, nbx_record* out) const {
+        if (all) {
+            std::memcpy(out, all + first, sizeof(nbx_record) * n);
+            return true;
+        }
+        char* dst = reinterpret_cast<char*>(out);
+        uint64_t left = 36 * n, off = 36 * first;
+        while (left) {
+            const ssize_t got = ::pread(fd, dst, size_t(std::min<uint64_t>(left, 1ull << 30)), off_t(off));
+            if (got <= 0) return false;
+            dst += got;
+            off += uint64_t(got);
+            left -= uint64_t(got);
+        }
+        return true;
     }
     ~PriSource() {
         if (all) nbx_free(all);
-        if (f) std::fclose(f);
+        if (fd >= 0) ::close(fd);
     }
 };
 
@@ -179,7 +200,7 @@ int main(int argc, char** argv) {
     p.add("seed", "Random seed", std::to_string(0x78c7e39b));
     p.add("sort-primaries", "Sort primary electrons before simulation", "0");
     p.add("device", "CUDA device ordinal", "0");
-    p.add("streams", "Device contexts working on batches at once (one with --energy-deposit)", "2");
+    p.add("streams", "Device contexts working on batches at once (one with --energy-deposit)", "4");
     p.add("inelastic", "Inelastic model: kieft (Kieft & Bosch) or penn (full Penn, the reference's stock build)",
           "kieft");
     p.add("energy-deposit", "Also write energy deposits, as the reference's nebula_cpu_energydep", "0");
@@ -382,7 +403,8 @@ int main(int argc, char** argv) {
             failed_ctx = c;
         }
     };
-    auto worker = [&](nbx_ctx* c) {
+    std::vector<PriWarnings> warns(ctxs.size(), PriWarnings{oct, max_energy});
+    auto worker = [&](nbx_ctx* c, PriWarnings& my_warn) {
         Batch b;
         std::vector<nbx_detected> det(1u << 20);
         std::vector<nbx_deposit> dep(energy_deposit ? (1u << 20) : 0);
@@ -395,16 +417,13 @@ int main(int argc, char** argv) {
                 b.first = next_first;
                 b.n = std::min(batch, n_pri - next_first);
                 next_first += b.n;
-                const nbx_record* pri = src.batch(b.first, b.n);
-                if (!pri) {
-                    failed_rc = NBX_ERR_FORMAT;
-                    failed_what = "primaries";
-                    std::fprintf(stderr, "Error: could not read primary electrons!\n");
-                    return;
-                }
-                b.pri.assign(pri, pri + b.n);
-                if (!sort_primaries) warn.add(pri, b.n);
             }
+            b.pri.resize(b.n);
+            if (!src.read(b.first, b.n, b.pri.data())) {
+                std::fprintf(stderr, "Error: could not read primary electrons!\n");
+                return fail_with(c, NBX_ERR_FORMAT, "primaries");
+            }
+            if (!sort_primaries) my_warn.add(b.pri.data(), b.n);
             b.part.resize(b.n);
             b.tags.resize(b.n);
             for (uint64_t i = 0; i < b.n; ++i) {
@@ -473,8 +492,9 @@ int main(int argc, char** argv) {
     timer.start();
     {
         std::vector<std::thread> threads;
-        for (nbx_ctx* c : ctxs) threads.emplace_back(worker, c);
+        for (size_t k = 0; k < ctxs.size(); ++k) threads.emplace_back(worker, ctxs[k], std::ref(warns[k]));
         for (auto& t : threads) t.join();
+        for (const auto& w : warns) warn.merge(w);
     }
     if (failed_rc != NBX_OK) {
         const int r = die(failed_ctx, failed_rc, failed_what.c_str());
