@@ -9,6 +9,10 @@ Si-like Kieft tables.  One step = one pass of the transport over the whole
 scan (every primary and its full secondary cascade).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl nbx|reference]
+                  [--workload grating|rough|holes] [--inelastic kieft|penn]
+
+The other workloads are the rough slab with mixed beam energies and the
+three-material contact-hole array (64 of its 1024 pixel rows per step).
 
 Under torchrun each rank simulates its own 256 x 256 scan (independent pixel
 rows, own seed): replicas, weak scaling, no data-path collective.  Rank 0
