@@ -307,7 +307,8 @@ def learned_fom(args, tris, mat, local, rank, prim, tags, mean_plain, var_plain,
     import nebula_b200 as nb
     from nebula_b200 import generators as g
     n = len(tags)
-    ctx = nb.setup(tris, [mat], device=local, seed=0x2545F491 + rank, blocks_per_sm=2, block_size=256,
+    ctx = nb.setup(tris, [mat], device=local, seed=0x2545F491 + rank, blocks_per_sm=args.learned_variant,
+                   block_size=args.learned_block,
                    inelastic=args.inelastic)
     try:
         ctx.build_surface_map([-180, -180, -60], [180, 180, 60], 1.0, 20.0)
@@ -338,7 +339,7 @@ def learned_fom(args, tris, mat, local, rank, prim, tags, mean_plain, var_plain,
         return {"fom_se": fom_l, "fom_se_plain": fom_plain, "gain": fom_l / fom_plain if fom_plain else None,
                 "se_yield": float(sw.mean()), "z_vs_plain": z, "run_ms": s["last_run_ms"],
                 "rr_threshold": args.rr_threshold, "rr_period": args.rr_period, "split": "off",
-                "launch": {"blocks_per_sm_variant": 2, "block_size": 256},
+                "launch": {"blocks_per_sm_variant": args.learned_variant, "block_size": args.learned_block},
                 "inferences": s["inferences"], "roulette_killed": s["roulette_killed"],
                 "steps": s["steps"], "train_samples": int(len(y)), "train_s": round(t_train, 3),
                 "train_loss": [round(float(v), 5) for v in losses]}
@@ -362,6 +363,8 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-roulette FOM comparison")
     ap.add_argument("--shared-pop", action="store_true",
                     help="all transport blocks pop primaries from one cursor (default: per-SM ranges)")
+    ap.add_argument("--learned-variant", type=int, default=4, help="transport variant of the learned leg")
+    ap.add_argument("--learned-block", type=int, default=256, help="threads per block of the learned leg")
     ap.add_argument("--rr-threshold", type=float, default=0.02)
     ap.add_argument("--rr-period", type=int, default=32)
     ap.add_argument("--inelastic", default="kieft", choices=["kieft", "penn"],
