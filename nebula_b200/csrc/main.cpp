@@ -376,12 +376,13 @@ int main(int argc, char** argv) {
     static_assert(sizeof(DepositRecord) == 28, "deposit record layout");
     const uint64_t dep_capacity = uint64_t(1) << 27;   // nbx_config default
 
-    // Worker threads, one per context, take the next batch from the file
-    // (in order, under a lock), run it and write its records (under a second
-    // lock).  A batch's primaries keep their global index as the uid of their
-    // random streams, so the records do not depend on the number of workers
-    // or on which worker ran a batch; only their order in the output does, as
-    // with the reference's worker threads.  Tags are batch-relative.
+    // Worker threads, one per context, claim the next batch of the file (in
+    // order, under a lock), read it with a positional read, run it and write
+    // its records (under a second lock).  A batch's primaries keep their
+    // global index as the uid of their random streams, so the records do not
+    // depend on the number of workers or on which worker ran a batch; only
+    // their order in the output does, as with the reference's worker threads.
+    // Tags are batch-relative.
     struct Batch {
         uint64_t first = 0, n = 0;
         std::vector<nbx_record> pri;
