@@ -117,3 +117,42 @@ def test_workload_writer(tmp_path):
     r = formats.read_pri(out["pri"])
     assert len(r) == 2 * 256 * 100 and set(np.unique(r["py"])) == {0, 1}
     assert len(formats.read_tri(out["tri"])) == len(g.grating_geometry())
+
+
+def _side_material(v, nrm, t, p, d):
+    k = _first_hit(v, p, d)
+    if k < 0:
+        return None
+    return t["mat_in"][k] if d @ nrm[k] > 0 else t["mat_out"][k]
+
+
+def test_grating_and_rough_consistently_oriented():
+    """Any point seen from two random directions lies in the same material,
+    and points above the top surface lie in vacuum: the grating and rough
+    slab meshes are closed and their normals point to the mat_out side."""
+    geoms = {"grating": (g.grating_geometry(n_lines=3, length=200.0), 60.0),
+             "rough": (g.rough_geometry(n=24, size=100.0, seed=3), 20.0)}
+    rng = np.random.default_rng(11)
+    for name, (tris, z_top) in geoms.items():
+        t = tris[tris["mat_in"] != formats.DETECTOR]
+        v = t["v"].reshape(-1, 3, 3).astype(np.float64)
+        nrm = np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0])
+        lo, hi = v.reshape(-1, 3).min(0), v.reshape(-1, 3).max(0)
+        agree = 0
+        for _ in range(400):
+            p = rng.uniform(lo + 1.0, hi - 1.0)
+            d1, d2 = rng.normal(size=3), rng.normal(size=3)
+            m1 = _side_material(v, nrm, t, p, d1 / np.linalg.norm(d1))
+            m2 = _side_material(v, nrm, t, p, d2 / np.linalg.norm(d2))
+            if m1 is None or m2 is None:
+                continue
+            assert m1 == m2, (name, p, m1, m2)
+            agree += 1
+        assert agree > 300, (name, agree)
+        # above the highest surface point: vacuum from any direction
+        for _ in range(50):
+            p = np.array([rng.uniform(lo[0] + 1, hi[0] - 1), rng.uniform(lo[1] + 1, hi[1] - 1), z_top])
+            d = rng.normal(size=3)
+            d[2] = -abs(d[2]) - 0.5
+            m = _side_material(v, nrm, t, p, d / np.linalg.norm(d))
+            assert m in (None, formats.VACUUM), (name, p, m)
