@@ -100,3 +100,24 @@ def test_material_and_config_structs_match_header():
     assert t3 == [f for f, _ in nb.Table3D._fields_]
     cfg = _header_fields(text, "typedef struct {\n    int32_t device;", "} nbx_config;")
     assert cfg == [f for f, _ in nb.Config._fields_]
+
+
+def test_documented_caller_compiles_and_reports_nodev(tmp_path):
+    """The minimal C++ caller of the integration guide compiles against
+    include/nbx.h, links against libnbx.so and, without a GPU, fails cleanly
+    at nbx_create (exit status 1, no crash)."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    m = re.search(r"```cpp\n(.*?)```", text, flags=re.S)
+    assert m
+    src = tmp_path / "caller.cpp"
+    src.write_text(m.group(1))
+    exe = tmp_path / "caller"
+    libdir = os.path.dirname(nb.LIB_PATH)
+    r = subprocess.run(["g++", "-std=c++17", "-I" + os.path.join(ROOT, "include"), str(src), "-L" + libdir, "-lnbx",
+                        "-Wl,-rpath," + libdir, "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    import torch
+    if not torch.cuda.is_available():
+        # g.tri is absent in the temporary directory: the loader fails first
+        r = subprocess.run([str(exe)], capture_output=True, text=True, cwd=str(tmp_path), timeout=60)
+        assert r.returncode == 1
