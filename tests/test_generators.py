@@ -156,3 +156,27 @@ def test_grating_and_rough_consistently_oriented():
             d[2] = -abs(d[2]) - 0.5
             m = _side_material(v, nrm, t, p, d / np.linalg.norm(d))
             assert m in (None, formats.VACUUM), (name, p, m)
+
+
+def test_banded_disc_tiles_the_polygon():
+    """The hole-floor disc (bands to inner rings, then a small fan) covers the
+    rough polygon exactly once: its triangles' signed areas sum to the
+    polygon's area, all with the orientation of the ring, and no vertex is
+    shared by more than 12 triangles (below the octree's split count)."""
+    rng = np.random.default_rng(4)
+    n = 48
+    th = 2 * np.pi * np.arange(n) / n
+    r = 20.0 + rng.uniform(-2, 2, n)
+    ring = np.stack([r * np.cos(th), r * np.sin(th), np.full(n, -100.0)], -1)[None]
+    ctr = np.array([[0.0, 0.0, -100.0]])
+    tris = g._disc(ctr, ring, 1, formats.VACUUM)
+    v = tris["v"].astype(np.float64)
+    area = 0.5 * ((v[:, 1, 0] - v[:, 0, 0]) * (v[:, 2, 1] - v[:, 0, 1]) -
+                  (v[:, 1, 1] - v[:, 0, 1]) * (v[:, 2, 0] - v[:, 0, 0]))
+    x, y = ring[0, :, 0], ring[0, :, 1]
+    poly = 0.5 * np.sum(x * np.roll(y, -1) - np.roll(x, -1) * y)
+    assert np.all(area > 0)
+    assert abs(area.sum() - poly) < 1e-3 * poly
+    assert len(tris) == 72 + 36 + 12
+    _, vid = np.unique(v.reshape(-1, 3).astype(np.float32), axis=0, return_inverse=True)
+    assert np.bincount(vid.ravel()).max() <= 12
