@@ -14,6 +14,7 @@
   reference CPU path (cpu_mt_main-style driver) within 3 sigma / chi-square.
 """
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
@@ -78,6 +79,24 @@ def test_ray_query_bit_exact_vs_reference(inputs, oracle_built, ray_sampler, geo
         assert np.array_equal(_bits(gd), _bits(rd)), "distances differ"
         assert (gt >= 0).sum() > n // 20
     ctx.close()
+
+
+def test_ray_query_matches_committed_golden_vectors(inputs):
+    """The committed golden vectors (outputs of the reference's propagate,
+    tests/golden/make_golden.py) against the kernel on the library's own
+    octree, without the reference at run time."""
+    import json
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden.json")) as f:
+        gold = json.load(f)
+    for key, tris in (("cube_rays", g.cube_geometry()), ("holes_rays", g.contact_hole_geometry(n_holes=2, seed=3))):
+        ctx = nb.setup(tris, [inputs["si"]], device=0)
+        r = gold[key]
+        gd, gt = ctx.ray_query(np.array(r["pos"], np.float32), np.array(r["dir"], np.float32),
+                               np.array(r["dist"], np.float32), np.array(r["ignore_tri"], np.int32),
+                               np.array(r["ignore_mat"], np.int32))
+        assert gt.tolist() == r["tri"], key
+        assert gd.view(np.uint32).tolist() == r["dist_bits"], key
+        ctx.close()
 
 
 @pytest.mark.parametrize("geom", ["grating", "rough", "holes"])

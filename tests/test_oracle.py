@@ -74,13 +74,14 @@ def test_golden_fixture(oracle_built, inputs):
     path = os.path.join(HERE, "golden", "golden.json")
     with open(path) as f:
         gold = json.load(f)
-    pg = oracle_built.PortGeometry(g.cube_geometry())
-    r = gold["cube_rays"]
-    od, ot = pg.propagate(np.array(r["pos"], np.float32), np.array(r["dir"], np.float32),
-                          np.array(r["dist"], np.float32), np.array(r["ignore_tri"], np.int32),
-                          np.array(r["ignore_mat"], np.int32))
-    assert ot.tolist() == r["tri"]
-    assert od.view(np.uint32).tolist() == r["dist_bits"]
+    for key, tris in (("cube_rays", g.cube_geometry()), ("holes_rays", g.contact_hole_geometry(n_holes=2, seed=3))):
+        pg = oracle_built.PortGeometry(tris)
+        r = gold[key]
+        od, ot = pg.propagate(np.array(r["pos"], np.float32), np.array(r["dir"], np.float32),
+                              np.array(r["dist"], np.float32), np.array(r["ignore_tri"], np.int32),
+                              np.array(r["ignore_mat"], np.int32))
+        assert ot.tolist() == r["tri"], key
+        assert od.view(np.uint32).tolist() == r["dist_bits"], key
 
 
 def _chi2(h1, h2):
