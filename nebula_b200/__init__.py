@@ -539,7 +539,6 @@ def run_noalloc(ctx: Context, d_particles: int, d_tags: int, n: int, uid_base: i
 
 def setup(tri_path_or_array, mat_paths, **ctx_kwargs):
     """Load geometry (.tri path or TRI_DTYPE array) and materials into a new Context."""
-    from . import formats
     if isinstance(tri_path_or_array, (str, os.PathLike)):
         tris = load_tri(tri_path_or_array)
     else:
