@@ -308,7 +308,7 @@ LinearOctree build_octree(const std::vector<Triangle>& input) {
     LinearOctree out;
 
     // Root box: union of triangle AABBs plus 1 nm (octree_builder.cpp:171-209).
-    Vec3 mn, mx;
+    Vec3 mn{}, mx{};   // set from the first triangle below
     for (size_t i = 0; i < input.size(); ++i) {
         const Vec3 A = vert(input[i], 0), B = vert(input[i], 1), C = vert(input[i], 2);
         const Vec3 tmin{fmin_ref(fmin_ref(A.x, B.x), C.x), fmin_ref(fmin_ref(A.y, B.y), C.y), fmin_ref(fmin_ref(A.z, B.z), C.z)};
