@@ -257,6 +257,49 @@ def cpu_baseline(tri_path, mat_paths, recs, tmp, count, penn=False):
             "primaries_per_s": st["n_primaries"] / secs}
 
 
+def _simulation_seconds(log):
+    """The `Simulation: <seconds>` line both programs print on stderr."""
+    for line in log.splitlines()[::-1]:
+        if "Simulation:" in line:
+            try:
+                return float(line.split(":")[-1])
+            except ValueError:
+                return None
+    return None
+
+
+def reference_gpu(tri_path, mat_paths, recs, tmp, penn=False, timeout=120):
+    """The reference's own GPU program (gpu_main.cu built for sm_100a by
+    `make -C oracle gpu`) and the nbx CLI on the same .tri/.pri/.mat files,
+    one after the other on this GPU; each program's own `Simulation:` time.
+    The reference checks for completion once a second (gpu_main.cu:410-426),
+    so its time is a whole number of seconds, an upper bound.  Test
+    infrastructure: opt-in (--reference-gpu), not part of the default run."""
+    from nebula_b200 import formats
+    binary = os.path.join(ROOT, "oracle", "_ref", "nebula_gpu" if penn else "nebula_gpu_kieft")
+    cli = os.path.join(ROOT, "nebula_b200", "nebula_b200")
+    if not (os.path.exists(binary) and os.path.exists(cli)):
+        return {"unavailable": "reference GPU program or nbx CLI not built"}
+    pri = os.path.join(tmp, "refgpu.pri")
+    formats.write_pri(pri, recs)
+    out = {"primaries": len(recs), "resolution_s": 1.0}
+    runs = (("reference", [binary]), ("nbx_cli", [cli] + (["--inelastic", "penn"] if penn else [])))
+    for name, cmd in runs:
+        try:
+            r = subprocess.run(cmd + [tri_path, pri] + list(mat_paths), stdout=subprocess.DEVNULL,
+                               stderr=subprocess.PIPE, timeout=timeout, text=True)
+        except subprocess.TimeoutExpired:
+            out[name] = {"status": "timed out after %d s" % timeout}
+            continue
+        secs = _simulation_seconds(r.stderr)
+        out[name] = {"status": r.returncode, "simulation_s": secs,
+                     "primaries_per_s": len(recs) / secs if secs else None}
+    ref_s = out.get("reference", {}).get("simulation_s")
+    nbx_s = out.get("nbx_cli", {}).get("simulation_s")
+    out["nbx_speedup_at_least"] = (ref_s - 1.0) / nbx_s if ref_s and nbx_s else None
+    return out
+
+
 def run_reference(args):
     rank, world, local = dist_env()
     if rank != 0:
@@ -361,6 +404,8 @@ def main():
     ap.add_argument("--variant", type=int, default=0, help="transport variant 2/3/4/7 (0: autotune)")
     ap.add_argument("--block", type=int, default=0, help="threads per block with --variant (0: 128)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-roulette FOM comparison")
+    ap.add_argument("--reference-gpu", action="store_true",
+                    help="also time the reference's own GPU program and the nbx CLI on the step's primaries")
     ap.add_argument("--shared-pop", action="store_true",
                     help="all transport blocks pop primaries from one cursor (default: per-SM ranges)")
     ap.add_argument("--learned-variant", type=int, default=4, help="transport variant of the learned leg")
@@ -509,6 +554,8 @@ def main():
         cpu = None if args.no_cpu_baseline else cpu_baseline(tri_path, mats, recs, tmp,
                                                               WORKLOADS[args.workload]["cpu_sample"],
                                                               penn=args.inelastic == "penn")
+        ref_gpu = reference_gpu(tri_path, mats, recs, tmp, penn=args.inelastic == "penn") \
+            if args.reference_gpu else None
         line = {
             "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
@@ -533,6 +580,7 @@ def main():
                          "kernel": "transport_kernel"},
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "reference_gpu_program": ref_gpu,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

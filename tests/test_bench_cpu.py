@@ -50,3 +50,10 @@ def test_strided_sample_spans_the_scan():
     assert len(sub) == 64
     assert set(np.unique(sub["py"])) == set(range(8))      # every row represented
     assert b.strided_sample(recs, 10**6) is recs
+
+
+def test_simulation_time_parsing():
+    b = _bench()
+    log = "Loading...\n\rProgress 100%\n\nSimulation successful!\n\n                     Simulation: 13.001\n"
+    assert b._simulation_seconds(log) == 13.001
+    assert b._simulation_seconds("no timing here") is None
