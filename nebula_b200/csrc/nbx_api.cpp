@@ -1206,29 +1206,68 @@ int nbx_build_surface_map(nbx_ctx* ctx, const float lo[3], const float hi[3], fl
         }
         const uint64_t cells = uint64_t(n[0]) * n[1] * n[2];
         if (cells > (1ull << 31)) throw ApiError(NBX_ERR_ARG, "surface map larger than 2^31 cells");
-        // candidates: triangles whose box reaches the map box grown by d_max
+        // Candidates, binned into bricks of kBrick^3 cells: a brick lists, in
+        // triangle order, every material triangle whose bounding box comes
+        // within d_max of the brick.  A triangle within d_max of a cell
+        // centre has its box within d_max of that centre, so each cell's
+        // brick list holds every triangle the nearest search could pick,
+        // and the search (strictly smaller distance wins, in list order)
+        // picks what a search over all triangles would.
+        constexpr int kBrick = 8;
+        int nb[3];
+        for (int k = 0; k < 3; ++k) nb[k] = (n[k] + kBrick - 1) / kBrick;
+        const uint64_t bricks = uint64_t(nb[0]) * nb[1] * nb[2];
+        const double bs = double(kBrick) * cell;
         std::vector<float4> t(3 * size_t(ctx->phys.geo.n_tri));
         to_host(ctx, t.data(), ctx->tris.p, sizeof(float4) * t.size(), "D2H");
-        std::vector<int32_t> cand;
+        struct Range { int b0[3], b1[3]; };
+        std::vector<std::pair<int, Range>> cand;
         for (int i = 0; i < ctx->phys.geo.n_tri; ++i) {
             const float4 r0 = t[3 * i], e1 = t[3 * i + 1], e2 = t[3 * i + 2];
-            const float xs[3] = {r0.x, r0.x + e1.x, r0.x + e2.x}, ys[3] = {r0.y, r0.y + e1.y, r0.y + e2.y},
-                        zs[3] = {r0.z, r0.z + e1.z, r0.z + e2.z};
-            const float mn[3] = {std::min({xs[0], xs[1], xs[2]}), std::min({ys[0], ys[1], ys[2]}), std::min({zs[0], zs[1], zs[2]})};
-            const float mx[3] = {std::max({xs[0], xs[1], xs[2]}), std::max({ys[0], ys[1], ys[2]}), std::max({zs[0], zs[1], zs[2]})};
-            bool near = true;
-            for (int k = 0; k < 3; ++k) near = near && mx[k] >= lo[k] - d_max && mn[k] <= hi[k] + d_max;
             int mi;
             std::memcpy(&mi, &r0.w, 4);
-            if (near && mi >= 0) cand.push_back(i);   // detector / special sheets are not material surfaces
+            if (mi < 0) continue;   // detector / special sheets are not material surfaces
+            const float xs[3] = {r0.x, r0.x + e1.x, r0.x + e2.x}, ys[3] = {r0.y, r0.y + e1.y, r0.y + e2.y},
+                        zs[3] = {r0.z, r0.z + e1.z, r0.z + e2.z};
+            const double mn[3] = {std::min({xs[0], xs[1], xs[2]}), std::min({ys[0], ys[1], ys[2]}), std::min({zs[0], zs[1], zs[2]})};
+            const double mx[3] = {std::max({xs[0], xs[1], xs[2]}), std::max({ys[0], ys[1], ys[2]}), std::max({zs[0], zs[1], zs[2]})};
+            Range r;
+            bool inside = true;
+            for (int k = 0; k < 3; ++k) {
+                const double a = std::floor((mn[k] - d_max - lo[k]) / bs) - 1, b = std::floor((mx[k] + d_max - lo[k]) / bs) + 1;
+                if (b < 0 || a > nb[k] - 1) inside = false;
+                r.b0[k] = int(std::max(a, 0.0));
+                r.b1[k] = int(std::min(b, double(nb[k] - 1)));
+            }
+            if (inside) cand.push_back({i, r});
         }
+        std::vector<uint64_t> start(bricks + 1, 0);
+        for (const auto& c : cand)
+            for (int z = c.second.b0[2]; z <= c.second.b1[2]; ++z)
+                for (int y = c.second.b0[1]; y <= c.second.b1[1]; ++y)
+                    for (int x = c.second.b0[0]; x <= c.second.b1[0]; ++x)
+                        ++start[(uint64_t(z) * nb[1] + y) * nb[0] + x + 1];
+        for (uint64_t b = 0; b < bricks; ++b) start[b + 1] += start[b];
+        if (start[bricks] > 0xFFFFFFFFull) throw ApiError(NBX_ERR_ARG, "surface map: too many brick entries");
+        std::vector<int32_t> list(std::max<uint64_t>(start[bricks], 1));
+        {
+            std::vector<uint64_t> fill(start.begin(), start.end() - 1);
+            for (const auto& c : cand)
+                for (int z = c.second.b0[2]; z <= c.second.b1[2]; ++z)
+                    for (int y = c.second.b0[1]; y <= c.second.b1[1]; ++y)
+                        for (int x = c.second.b0[0]; x <= c.second.b1[0]; ++x)
+                            list[fill[(uint64_t(z) * nb[1] + y) * nb[0] + x]++] = c.first;
+        }
+        std::vector<uint32_t> start32(start.begin(), start.end());
         ctx->smap_cells.alloc(std::max<uint64_t>(cells, 1));
-        DevBuf<int32_t> dcand;
-        dcand.alloc(std::max<size_t>(cand.size(), 1));
-        if (!cand.empty())
-            to_device(ctx, dcand.p, cand.data(), 4 * cand.size(), "H2D");
-        ck(nbx::launch_build_surface_map(ctx->tris.p, dcand.p, int(cand.size()), ctx->smap_cells.p, lo[0], lo[1], lo[2],
-                                         cell, n[0], n[1], n[2], d_max, ctx->stream), "surface map");
+        DevBuf<uint32_t> dstart;
+        DevBuf<int32_t> dlist;
+        dstart.alloc(start32.size());
+        dlist.alloc(list.size());
+        to_device(ctx, dstart.p, start32.data(), 4 * start32.size(), "H2D");
+        to_device(ctx, dlist.p, list.data(), 4 * list.size(), "H2D");
+        ck(nbx::launch_build_surface_map(ctx->tris.p, dstart.p, dlist.p, nb[0], nb[1], kBrick, ctx->smap_cells.p, lo[0],
+                                         lo[1], lo[2], cell, n[0], n[1], n[2], d_max, ctx->stream), "surface map");
         ck(cudaStreamSynchronize(ctx->stream), "surface map");
         ctx->smap.cell_tri = ctx->smap_cells.p;
         ctx->smap.lox = lo[0];

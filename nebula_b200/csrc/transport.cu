@@ -741,16 +741,18 @@ int transport_max_blocks_per_sm(int block, int variant, int mode) {
 }
 
 namespace {
-__global__ void build_surface_map_kernel(const float4* tri, const int32_t* cand, int n_cand, int32_t* map, float lox,
-                                         float loy, float loz, float cell, int nx, int ny, int nz, float d_max) {
+__global__ void build_surface_map_kernel(const float4* tri, const uint32_t* brick_start, const int32_t* brick_tris,
+                                         int nbx, int nby, int brick, int32_t* map, float lox, float loy, float loz,
+                                         float cell, int nx, int ny, int nz, float d_max) {
     const uint64_t n = uint64_t(nx) * ny * nz;
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
         const int ix = int(i % nx), iy = int((i / nx) % ny), iz = int(i / (uint64_t(nx) * ny));
         const float px = lox + (ix + 0.5f) * cell, py = loy + (iy + 0.5f) * cell, pz = loz + (iz + 0.5f) * cell;
+        const uint64_t b = (uint64_t(iz / brick) * nby + iy / brick) * nbx + ix / brick;
         float best = d_max * d_max;
         int bi = -1;
-        for (int k = 0; k < n_cand; ++k) {
-            const int ti = __ldg(cand + k);
+        for (uint32_t k = __ldg(brick_start + b), end = __ldg(brick_start + b + 1); k < end; ++k) {
+            const int ti = __ldg(brick_tris + k);
             const float d2 = dev::dist2_to_triangle(tri, ti, px, py, pz);
             if (d2 < best) {
                 best = d2;
@@ -779,13 +781,13 @@ cudaError_t launch_triangle_faces(const float4* tri, float4* face, int n, cudaSt
     return cudaGetLastError();
 }
 
-cudaError_t launch_build_surface_map(const float4* tri, const int32_t* candidates, int n_candidates, int32_t* map,
-                                     float lox, float loy, float loz, float cell, int nx, int ny, int nz, float d_max,
-                                     cudaStream_t s) {
+cudaError_t launch_build_surface_map(const float4* tri, const uint32_t* brick_start, const int32_t* brick_tris,
+                                     int nbx, int nby, int brick, int32_t* map, float lox, float loy, float loz,
+                                     float cell, int nx, int ny, int nz, float d_max, cudaStream_t s) {
     const uint64_t n = uint64_t(nx) * ny * nz;
     if (n == 0) return cudaSuccess;
-    build_surface_map_kernel<<<grid_for(n, 128), 128, 0, s>>>(tri, candidates, n_candidates, map, lox, loy, loz, cell,
-                                                              nx, ny, nz, d_max);
+    build_surface_map_kernel<<<grid_for(n, 128), 128, 0, s>>>(tri, brick_start, brick_tris, nbx, nby, brick, map, lox,
+                                                              loy, loz, cell, nx, ny, nz, d_max);
     return cudaGetLastError();
 }
 
