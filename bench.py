@@ -51,10 +51,16 @@ WORKLOAD = "grating 256x256 px x 100 primaries @ 500 eV (6,553,600 primaries), 5
 # workload), the rough-slab scan with mixed beam energies and the
 # multi-material contact-hole array.  `rows` is the default pixel-row subset
 # of one step, `cpu_sample` / `ref_sample` the primaries (evenly strided over
-# the step's scan) of the CPU-baseline run and of each reference-arm step.
+# the step's scan) of the CPU-baseline run and of each reference-arm step,
+# `learned` the nearest-surface map and training scan of the learned leg
+# (single-material workloads).
 WORKLOADS = {
-    "grating": dict(rows=256, cpu_sample=409600, ref_sample=102400, desc=WORKLOAD),
+    "grating": dict(rows=256, cpu_sample=409600, ref_sample=102400, desc=WORKLOAD,
+                    learned=dict(map_lo=(-180, -180, -60), map_hi=(180, 180, 60), cell=1.0, d_max=20.0,
+                                 train_per_pixel=4)),
     "rough": dict(rows=512, cpu_sample=163840, ref_sample=40960,
+                  learned=dict(map_lo=(-500, -500, -40), map_hi=(500, 500, 30), cell=2.0, d_max=10.0,
+                               train_per_pixel=1),
                   desc="rough slab: 512x512 Gaussian height field (RMS 3 nm, correlation 10 nm) over 1 um, "
                        "526,334 triangles; 512x512 px x 20 primaries (5,242,880) at E uniform over "
                        "{300, 1000, 3000, 5000} eV, Si-like Kieft tables"),
@@ -353,9 +359,12 @@ def learned_fom(args, tris, mat, local, rank, prim, tags, mean_plain, var_plain,
     ctx = nb.setup(tris, [mat], device=local, seed=0x2545F491 + rank, blocks_per_sm=args.learned_variant,
                    block_size=args.learned_block,
                    inelastic=args.inelastic)
+    w = workload(args.workload)
+    L = w["learned"]
     try:
-        ctx.build_surface_map([-180, -180, -60], [180, 180, 60], 1.0, 20.0)
-        train = g.scan_beam(NX, NY, 4, ENERGY, seed=0x51ED + rank)
+        ctx.build_surface_map(list(L["map_lo"]), list(L["map_hi"]), L["cell"], L["d_max"])
+        train = g.scan_beam(NX, NY, L["train_per_pixel"], ENERGY, spacing=w["spacing"], origin=w["origin"],
+                            z_start=w["z_start"], seed=0x51ED + rank, energies=w["energies"])
         ctx.set_sample_capacity(1 << 23)
         ctx.set_mode("sample")
         ctx.set_tag_range(len(train))
@@ -535,7 +544,7 @@ def main():
     d2h = n_pix * 5 * 8
 
     # the network's surface map and training scan are set up for the grating
-    learned = None if (args.no_learned or args.workload != "grating") else \
+    learned = None if (args.no_learned or "learned" not in WORKLOADS[args.workload]) else \
         learned_fom(args, tris, mats[0], local, rank, prim, tags, mean_se, var_primary, fom)
 
     line = None

@@ -1233,8 +1233,11 @@ int nbx_build_surface_map(nbx_ctx* ctx, const float lo[3], const float hi[3], fl
             const double mx[3] = {std::max({xs[0], xs[1], xs[2]}), std::max({ys[0], ys[1], ys[2]}), std::max({zs[0], zs[1], zs[2]})};
             Range r;
             bool inside = true;
+            // reach: d_max plus 1e-3 nm for the float rounding of the cell
+            // centres the kernel measures from
+            const double reach = double(d_max) + 1e-3;
             for (int k = 0; k < 3; ++k) {
-                const double a = std::floor((mn[k] - d_max - lo[k]) / bs) - 1, b = std::floor((mx[k] + d_max - lo[k]) / bs) + 1;
+                const double a = std::floor((mn[k] - reach - lo[k]) / bs), b = std::floor((mx[k] + reach - lo[k]) / bs);
                 if (b < 0 || a > nb[k] - 1) inside = false;
                 r.b0[k] = int(std::max(a, 0.0));
                 r.b1[k] = int(std::min(b, double(nb[k] - 1)));
