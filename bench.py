@@ -378,6 +378,8 @@ def learned_fom(args, tris, mat, local, rank, prim, tags, mean_plain, var_plain,
         t_train = time.perf_counter() - t0
         ctx.set_tag_range(n)
         ctx.set_mode("learned", rr_threshold=args.rr_threshold, split_threshold=2.0, rr_period=args.rr_period)
+        if args.birth_rr:
+            ctx.set_birth_roulette(*[float(v) for v in args.birth_rr.split(",")])
         ctx.reset_tallies()
         ctx.push(prim, tags)
         ctx.run()
@@ -391,6 +393,7 @@ def learned_fom(args, tris, mat, local, rank, prim, tags, mean_plain, var_plain,
         return {"fom_se": fom_l, "fom_se_plain": fom_plain, "gain": fom_l / fom_plain if fom_plain else None,
                 "se_yield": float(sw.mean()), "z_vs_plain": z, "run_ms": s["last_run_ms"],
                 "rr_threshold": args.rr_threshold, "rr_period": args.rr_period, "split": "off",
+                "birth_roulette": args.birth_rr or "off",
                 "launch": {"blocks_per_sm_variant": args.learned_variant, "block_size": args.learned_block},
                 "inferences": s["inferences"], "roulette_killed": s["roulette_killed"],
                 "steps": s["steps"], "train_samples": int(len(y)), "train_s": round(t_train, 3),
@@ -419,6 +422,8 @@ def main():
                     help="all transport blocks pop primaries from one cursor (default: per-SM ranges)")
     ap.add_argument("--learned-variant", type=int, default=4, help="transport variant of the learned leg")
     ap.add_argument("--learned-block", type=int, default=256, help="threads per block of the learned leg")
+    ap.add_argument("--birth-rr", default="",
+                    help="learned leg: roulette at birth, 'min_distance_nm,max_energy_eV,survival' (default off)")
     ap.add_argument("--rr-threshold", type=float, default=0.02)
     ap.add_argument("--rr-period", type=int, default=32)
     ap.add_argument("--inelastic", default="kieft", choices=["kieft", "penn"],

@@ -334,6 +334,13 @@ int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* ta
 #define NBX_MODE_SAMPLE 1
 #define NBX_MODE_LEARNED 2
 int nbx_set_mode(nbx_ctx* ctx, int32_t mode, float rr_threshold, float split_threshold, int32_t rr_period);
+/* Learned mode, roulette at birth (off until set): a secondary born with
+ * energy below max_energy (eV) at least min_distance (nm) from the nearest
+ * surface of the surface map (outside the map counts as far) survives with
+ * probability `survival` and then carries its parent's weight / survival; a
+ * dropped secondary's cascade is not simulated (counted in
+ * nbx_stats.roulette_killed).  survival 0 or 1 turns it off. */
+int nbx_set_birth_roulette(nbx_ctx* ctx, float min_distance, float max_energy, float survival);
 /* Nearest-triangle map over the box [lo, hi) with the given cell size (nm);
  * surfaces farther than d_max (nm) count as "far".  Needed for the distance
  * and cosine features. */

@@ -149,6 +149,7 @@ def lib():
         "nbx_step_query": (C.c_int, [_vp, _vp, C.c_uint64, _vp, _vp, _vp, _vp]),
         "nbx_set_uid_base": (C.c_int, [_vp, C.c_uint64]),
         "nbx_set_mode": (C.c_int, [_vp, C.c_int32, C.c_float, C.c_float, C.c_int32]),
+        "nbx_set_birth_roulette": (C.c_int, [_vp, C.c_float, C.c_float, C.c_float]),
         "nbx_build_surface_map": (C.c_int, [_vp, _vp, _vp, C.c_float, C.c_float]),
         "nbx_set_sample_capacity": (C.c_int, [_vp, C.c_uint64]),
         "nbx_get_samples": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.POINTER(C.c_uint64)]),
@@ -456,6 +457,10 @@ class Context:
 
     def set_mode(self, mode, rr_threshold=0.05, split_threshold=0.5, rr_period=8):
         self._ck(self.L.nbx_set_mode(self.h, self.MODES.get(mode, mode), rr_threshold, split_threshold, rr_period))
+
+    def set_birth_roulette(self, min_distance, max_energy, survival):
+        """Learned mode: roulette at a secondary's birth (see include/nbx.h)."""
+        self._ck(self.L.nbx_set_birth_roulette(self.h, min_distance, max_energy, survival))
 
     def build_surface_map(self, lo, hi, cell=1.0, d_max=20.0):
         lo = np.ascontiguousarray(lo, np.float32)

@@ -88,6 +88,19 @@ __device__ __forceinline__ float dist2_to_triangle(const float4* tri, int ti, fl
     return (px - qx) * (px - qx) + (py - qy) * (py - qy) + (pz - qz) * (pz - qz);
 }
 
+// Distance from p to the surface map's nearest triangle for p's cell, or
+// d_max where the map has none within d_max or p lies outside the map.
+__device__ __forceinline__ float surface_distance(const Geometry& g, const SurfaceMap& S, float px, float py, float pz) {
+    if (!S.cell_tri) return S.d_max;
+    const int ix = int(floorf((px - S.lox) * S.inv_cell));
+    const int iy = int(floorf((py - S.loy) * S.inv_cell));
+    const int iz = int(floorf((pz - S.loz) * S.inv_cell));
+    if (ix < 0 || iy < 0 || iz < 0 || ix >= S.nx || iy >= S.ny || iz >= S.nz) return S.d_max;
+    const int ti = __ldg(S.cell_tri + (size_t(iz) * S.ny + iy) * S.nx + ix);
+    if (ti < 0) return S.d_max;
+    return fminf(sqrtf(dist2_to_triangle(g.tri, ti, px, py, pz)), S.d_max);
+}
+
 // Feature scaling: log E over [log 12 eV, log 8 keV] -> about [0, 1]; the
 // distance over [0, d_max] -> [0, 1].
 constexpr float kLogEOffset = 2.5f;

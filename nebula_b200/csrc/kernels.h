@@ -79,6 +79,14 @@ struct TransportArgs {
     float rr_threshold;
     float split_threshold;
     int rr_period;              // infer every rr_period steps of an electron
+    // learned mode, roulette at birth: a secondary born with energy below
+    // birth_max_energy and at least birth_min_distance from the nearest
+    // surface (the surface map's distance; outside the map counts as far)
+    // survives with probability birth_survival and then carries its parent's
+    // weight / birth_survival.  birth_survival outside (0, 1): off.
+    float birth_min_distance;
+    float birth_max_energy;
+    float birth_survival;
     dev::SurfaceMap smap;
     // deposit mode: one record per scattering event that changed the energy
     // (drivers/cpu/energydeposit_cpu_driver.h:74-96), kDepositWords floats

@@ -131,6 +131,7 @@ struct nbx_ctx {
     int mode = nbx::kModePlain;
     float rr_threshold = 0.05f, split_threshold = 0.5f;
     int rr_period = 8;
+    float birth_min_distance = 0.0f, birth_max_energy = 0.0f, birth_survival = 0.0f;   // off
     DevBuf<int32_t> smap_cells;
     nbx::dev::SurfaceMap smap{};
     DevBuf<float> sample_feat, sample_label;
@@ -737,6 +738,9 @@ int nbx_run(nbx_ctx* ctx) {
             a.rr_threshold = ctx->rr_threshold;
             a.split_threshold = ctx->split_threshold;
             a.rr_period = ctx->rr_period;
+            a.birth_min_distance = ctx->birth_min_distance;
+            a.birth_max_energy = ctx->birth_max_energy;
+            a.birth_survival = ctx->birth_survival;
         }
         int mode = ctx->mode;
         if (ctx->cfg.record_deposits) {
@@ -1192,6 +1196,14 @@ int nbx_set_mode(nbx_ctx* ctx, int32_t mode, float rr_threshold, float split_thr
     ctx->rr_threshold = rr_threshold;
     ctx->split_threshold = split_threshold;
     ctx->rr_period = rr_period;
+    return NBX_OK;
+}
+
+int nbx_set_birth_roulette(nbx_ctx* ctx, float min_distance, float max_energy, float survival) {
+    if (!ctx || !(min_distance >= 0) || !(max_energy >= 0) || !(survival >= 0) || survival > 1) return NBX_ERR_ARG;
+    ctx->birth_min_distance = min_distance;
+    ctx->birth_max_energy = max_energy;
+    ctx->birth_survival = survival;
     return NBX_OK;
 }
 

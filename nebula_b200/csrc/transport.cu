@@ -137,6 +137,10 @@ __device__ __forceinline__ uint32_t mix32(uint64_t x) {
 // inference, so lanes without work idle until the whole warp is done), or
 // kModeDeposit (plain transport that also appends an energy-deposit record
 // per energy-changing scattering event).
+// Philox block of a secondary's step 0 that decides its roulette at birth
+// (the transport's own draws use blocks 0-2 and 3 + 64 at most).
+constexpr uint32_t kBirthBlock = 0x7FFFFFFFu;
+
 template <int MinBlocks, int Mode, bool Penn>
 __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transport_kernel(const dev::Physics P, const TransportArgs a) {
     // Leaf cache: 13 words per thread in dynamic shared memory sized by the
@@ -349,7 +353,22 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
         if (has_se) {
             // an inelastic step never ends its electron: st == kAlive here
             ++c_se;
-            if (dev::ends_at_init(P, se)) {
+            // learned mode: roulette at the secondary's birth (its own draw
+            // block kBirthBlock of step 0, used by nothing else)
+            float birth_w = 1.0f;
+            bool birth_dropped = false;
+            if constexpr (Mode == kModeLearned) {
+                if (a.birth_survival > 0.0f && a.birth_survival < 1.0f && se.E < a.birth_max_energy &&
+                    dev::surface_distance(P.geo, a.smap, se.px, se.py, se.pz) >= a.birth_min_distance) {
+                    if (dev::u01(dev::draw(P.seed, se, kBirthBlock).x) < a.birth_survival)
+                        birth_w = 1.0f / a.birth_survival;
+                    else
+                        birth_dropped = true;
+                }
+            }
+            if (birth_dropped) {
+                ++c_kill;   // the secondary's sub-cascade is not simulated
+            } else if (dev::ends_at_init(P, se)) {
                 // The secondary's first step would only terminate it (about a
                 // quarter of them start below the barrier): tally that step
                 // here instead of parking the parent for it.
@@ -363,6 +382,7 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                 if constexpr (kExtra) {
                     ex.rec = -1;
                     ex.flags = 0;   // the secondary inherits the weight only
+                    ex.w *= birth_w;
                 }
                 continue;
             } else {
@@ -374,7 +394,7 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                 const uint32_t slot = base + g.thread_rank();
                 if (slot < a.out_capacity) {
                     store_electron(a.out, slot, se);
-                    if constexpr (Mode == kModeLearned) a.out.c[slot].w = __float_as_uint(ex.w);
+                    if constexpr (Mode == kModeLearned) a.out.c[slot].w = __float_as_uint(ex.w * birth_w);
                 } else {
                     atomicAdd(a.counters + kCntOverflow, 1ull);
                 }
