@@ -206,3 +206,25 @@ def test_learned_roulette_unbiased(inputs):
         z = (learned.mean() - plain.mean()) / np.sqrt(learned.var() / len(learned) + plain.var() / len(plain))
         assert abs(z) < 3, z
     c.close()
+
+
+def test_birth_roulette_unbiased(inputs):
+    """Roulette at a secondary's birth (1 keV into the cube: secondaries born
+    more than 5 nm from the surface below 100 eV survive with probability
+    1/4 at weight 4) drops many sub-cascades, makes fewer steps, and keeps
+    the weighted SE and BSE yields within 4 sigma of the analogue run."""
+    recs = g.point_beam(20000, 1000.0, pos=(0.0, 0.0, 1.0))
+    a = nb.setup(inputs["cube"], [inputs["si"]], device=0, seed=88)
+    sp, se_p, bse_p, _, _ = _run(a, recs, "plain")
+    a.close()
+    b = nb.setup(inputs["cube"], [inputs["si"]], device=0, seed=99)
+    b.build_surface_map([-60, -60, -80], [60, 60, 5], 1.0, 10.0)
+    b.mlp_set_params(M.init_params(0))
+    b.set_birth_roulette(5.0, 100.0, 0.25)
+    s, _, _, sw, bw = _run(b, recs, "learned", rr_threshold=0.0, split_threshold=2.0, rr_period=1 << 30)
+    b.close()
+    assert s["roulette_killed"] > 1000 and s["inferences"] == 0
+    assert s["steps"] < 0.9 * sp["steps"]
+    for w, c in ((sw.astype(np.float64), se_p.astype(np.float64)), (bw.astype(np.float64), bse_p.astype(np.float64))):
+        z = (w.mean() - c.mean()) / np.sqrt(w.var() / len(w) + c.var() / len(c))
+        assert abs(z) < 4, z
