@@ -404,13 +404,14 @@ def learned_fom(args, tris, mat, local, rank, prim, tags, mean_plain, var_plain,
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--gpus", type=int, default=1, help="GPUs of the run (ranks come from torchrun)")
+    ap.add_argument("--steps", type=int, default=5, help="timed steps")
+    ap.add_argument("--warmup", type=int, default=3, help="untimed warm-up steps")
     ap.add_argument("--impl", default="nbx", choices=["nbx", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="grating", choices=sorted(WORKLOADS),
-                    help="grating line scan (headline) or rough slab with mixed energies")
+                    help="grating line scan (headline), rough slab with mixed energies, or the "
+                         "three-material contact-hole array")
     ap.add_argument("--rows", type=int, default=0,
                     help="pixel rows of one step (0: the workload's default, all rows but for the contact holes)")
     ap.add_argument("--variant", type=int, default=0, help="transport variant 2/3/4/7 (0: autotune)")
@@ -424,8 +425,10 @@ def main():
     ap.add_argument("--learned-block", type=int, default=256, help="threads per block of the learned leg")
     ap.add_argument("--birth-rr", default="",
                     help="learned leg: roulette at birth, 'min_distance_nm,max_energy_eV,survival' (default off)")
-    ap.add_argument("--rr-threshold", type=float, default=0.02)
-    ap.add_argument("--rr-period", type=int, default=32)
+    ap.add_argument("--rr-threshold", type=float, default=0.02,
+                    help="learned leg: importance below which the network's weight window plays roulette")
+    ap.add_argument("--rr-period", type=int, default=32,
+                    help="learned leg: warp iterations between network evaluations (a huge value turns them off)")
     ap.add_argument("--inelastic", default="kieft", choices=["kieft", "penn"],
                     help="inelastic model: Kieft & Bosch (the headline workload) or full Penn (the reference's stock build)")
     args = ap.parse_args()
