@@ -7,7 +7,8 @@
 // progress and timing go to stderr; usage errors exit with status 1.  The
 // host side calls the library only through the C ABI of include/nbx.h.
 // --prescan-size and --batch-factor are accepted for compatibility: the
-// persistent queue needs no prescan (gpu_main.cu:109-175 sized frames with it).
+// persistent queue needs no prescan (gpu_main.cu:109-175 sized frames with
+// it); they only size the batches of the --energy-deposit mode.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
