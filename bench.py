@@ -14,8 +14,11 @@ scan (every primary and its full secondary cascade).
 The other workloads are the rough slab with mixed beam energies and the
 three-material contact-hole array (64 of its 1024 pixel rows per step).
 
-Under torchrun each rank simulates its own 256 x 256 scan (independent pixel
-rows, own seed): replicas, weak scaling, no data-path collective.  Rank 0
+Under torchrun the job is one frame of the scan per rank (fixed work per GPU:
+weak scaling), sharded over the ranks by global primary index with
+nebula_b200.replicas (each rank's random streams start at its shard's global
+index), and the per-pixel FP64 sums are added up over the ranks with
+replicas.reduce_pixel_yields once, after timing; no data-path collective.  Rank 0
 prints one JSON line.  value = events/s over all ranks with the primaries
 already resident in HBM (device time of nbx_run, CUDA events on the library's
 stream, max over ranks); e2e = the same through the C ABI from pinned host
@@ -157,6 +160,30 @@ def strided_sample(recs, count):
     return recs[np.linspace(0, len(recs) - 1, count).astype(np.int64)]
 
 
+def step_moments(counts):
+    """(mean, variance) of one run's per-primary counts or weights."""
+    c = np.asarray(counts, np.float64)
+    return float(c.mean()), float(c.var())
+
+
+def fom(var_per_primary, n, seconds):
+    """Figure of merit 1 / (sigma^2 t) of a mean yield estimated from n
+    primaries in `seconds` of device time, sigma^2 = var_per_primary / n.
+    var_per_primary must be the variance of ONE run's per-primary values:
+    summing the counts of K repeated runs of the same scan before taking the
+    variance adds K times the spread of the per-pixel means, and the result
+    would grow with K."""
+    if not (var_per_primary > 0) or not (seconds > 0) or n <= 0:
+        return None
+    return 1.0 / (var_per_primary / n * seconds)
+
+
+def plain_fom(step_vars, n, step_seconds):
+    """FOM of K timed plain steps, each one independent run over the same n
+    primaries: per-step variances and device times averaged."""
+    return fom(sum(step_vars) / len(step_vars), n, sum(step_seconds) / len(step_seconds))
+
+
 class ClockSampler:
     """nvidia-smi clock/throttle sampling during the timed region."""
 
@@ -274,13 +301,26 @@ def _simulation_seconds(log):
     return None
 
 
-def reference_gpu(tri_path, mat_paths, recs, tmp, penn=False, timeout=120):
+# Workloads on which the reference's own GPU program is not run: on the
+# contact-hole scan it stops making progress (every slot holds a running
+# electron whose secondary waits for a free slot, drivers/gpu/
+# gpu_driver.inl:523-528 and gpu_particle_manager.inl:355-376), so it would
+# only run into the timeout.
+REFERENCE_GPU_STALLS = {
+    "holes": "reference program stalls on this workload (see profiles/reference_gpu_program.md)",
+}
+
+
+def reference_gpu(tri_path, mat_paths, recs, tmp, penn=False, timeout=120, workload="grating"):
     """The reference's own GPU program (gpu_main.cu built for sm_100a by
     `make -C oracle gpu`) and the nbx CLI on the same .tri/.pri/.mat files,
     one after the other on this GPU; each program's own `Simulation:` time.
     The reference checks for completion once a second (gpu_main.cu:410-426),
     so its time is a whole number of seconds, an upper bound.  Test
-    infrastructure: opt-in (--reference-gpu), not part of the default run."""
+    infrastructure: opt-in (--reference-gpu), not part of the default run,
+    and refused on the workloads of REFERENCE_GPU_STALLS."""
+    if workload in REFERENCE_GPU_STALLS:
+        return {"unavailable": REFERENCE_GPU_STALLS[workload]}
     from nebula_b200 import formats
     binary = os.path.join(ROOT, "oracle", "_ref", "nebula_gpu" if penn else "nebula_gpu_kieft")
     cli = os.path.join(ROOT, "nebula_b200", "nebula_b200")
@@ -344,15 +384,18 @@ def run_reference(args):
     return 0
 
 
-def learned_fom(args, tris, mat, local, rank, prim, tags, mean_plain, var_plain, fom_plain):
+def learned_fom(args, tris, mat, local, rank, prim, tags, plain):
     """SE-yield figure of merit of the learned roulette on the same scan.
 
     A sample-mode pass over a 4-primaries-per-pixel scan (its own seed) gives
     (features, label) pairs; the network is trained on them (8 epochs, batch
     8192, Adam lr 1e-3); then the whole scan runs once in learned mode with one
     tag per primary.  FOM = 1 / (sigma^2 t): sigma^2 = per-primary variance of
-    the weighted SE count / n, t = device time of that run.  `z` compares the
-    weighted SE yield with the plain yield of the timed steps (unbiasedness)."""
+    the weighted SE count of that one run / n, t = its device time -- the same
+    estimator as the plain FOM of one timed step.  `z` compares the weighted
+    SE and BSE yields with the plain yields of the timed steps
+    (unbiasedness).  `plain`: the plain steps' means, per-step variances,
+    step count and FOM."""
     import nebula_b200 as nb
     from nebula_b200 import generators as g
     n = len(tags)
@@ -385,13 +428,17 @@ def learned_fom(args, tris, mat, local, rank, prim, tags, mean_plain, var_plain,
         ctx.run()
         s = ctx.stats()
         sw, bw = ctx.tag_weights(0, n)
-        sw = sw.astype(np.float64)
         t = s["last_run_ms"] / 1000.0
-        var_l = float(np.var(sw))
-        fom_l = 1.0 / (var_l / n * t)
-        z = (float(sw.mean()) - mean_plain) / math.sqrt(var_l / n + var_plain / n)
-        return {"fom_se": fom_l, "fom_se_plain": fom_plain, "gain": fom_l / fom_plain if fom_plain else None,
-                "se_yield": float(sw.mean()), "z_vs_plain": z, "run_ms": s["last_run_ms"],
+        m_se, v_se = step_moments(sw)
+        m_bse, v_bse = step_moments(bw)
+        fom_l = fom(v_se, n, t)
+        k = plain["steps"]
+        z_se = (m_se - plain["mean_se"]) / math.sqrt(v_se / n + plain["var_se"] / (n * k))
+        z_bse = (m_bse - plain["mean_bse"]) / math.sqrt(v_bse / n + plain["var_bse"] / (n * k))
+        return {"fom_se": fom_l, "fom_se_plain": plain["fom"],
+                "gain": fom_l / plain["fom"] if (fom_l and plain["fom"]) else None,
+                "se_yield": m_se, "bse_yield": m_bse, "z_vs_plain": z_se, "z_bse_vs_plain": z_bse,
+                "run_ms": s["last_run_ms"],
                 "rr_threshold": args.rr_threshold, "rr_period": args.rr_period, "split": "off",
                 "birth_roulette": args.birth_rr or "off",
                 "launch": {"blocks_per_sm_variant": args.learned_variant, "block_size": args.learned_block},
@@ -441,8 +488,9 @@ def main():
     import nebula_b200 as nb
 
     tmp = tempfile.mkdtemp(prefix="nbx_bench_")
-    mats, tris, tri_path, recs = make_workload(tmp, rank, rows=range(args.rows), workload=args.workload)
-    ctx = nb.setup(tris, mats, device=local, seed=0x78C7E39B + rank, inelastic=args.inelastic,
+    from nebula_b200 import replicas
+    mats, tris, tri_path, recs = make_workload(tmp, rows=range(args.rows), workload=args.workload)
+    ctx = nb.setup(tris, mats, device=local, seed=0x78C7E39B, inelastic=args.inelastic,
                    shared_pop=args.shared_pop)
     n = len(recs)
     prim = np.zeros((n, 7), np.float32)
@@ -466,7 +514,7 @@ def main():
     # Autotune the transport launch shape on a 16-row sample of the scan.
     if args.variant:
         ctx.close()
-        ctx = nb.setup(tris, mats, device=local, seed=0x78C7E39B + rank, blocks_per_sm=args.variant,
+        ctx = nb.setup(tris, mats, device=local, seed=0x78C7E39B, blocks_per_sm=args.variant,
                        block_size=args.block or 128, inelastic=args.inelastic, shared_pop=args.shared_pop)
         ctx.set_tag_range(n)
         tuned = (args.variant, args.block or 128)
@@ -480,47 +528,59 @@ def main():
         sample = np.arange(r0 * NX * PER_PIXEL, min(n, (r0 + tune_rows) * NX * PER_PIXEL))
         tuned = ctx.autotune(prim[sample], tags[sample])
 
-    def one_step():
+    # One job of `world` frames of the scan, sharded by global primary index:
+    # this rank's shard is [g_start, g_stop) of every step's world * n
+    # primaries (one frame), simulated with the global index as its random-
+    # stream base, so the combined result does not depend on the rank count.
+    g_start, g_stop = replicas.shard_range(world * n, rank, world)
+    assert g_stop - g_start == n
+    step_no = [0]
+
+    def push_step():
+        ctx.set_uid_base(step_no[0] * world * n + g_start)
+        step_no[0] += 1
         ctx.push(pin_p, pin_t)
-        barrier(dist)
-        ctx.run()
-        return ctx.stats()
 
     for _ in range(args.warmup):
         ctx.reset_tallies()
-        one_step()
+        push_step()
+        barrier(dist)
+        ctx.run()
 
-    # Device-resident timing: primaries pushed before the timed run.
-    ctx.reset_tallies()
+    # Device-resident timing: primaries pushed before the timed run.  Each
+    # timed step is one independent run over the scan; its per-primary counts
+    # are read back after the run (outside the device-timed region) for the
+    # per-step variance of the figure of merit.
     dev_ms, events, gens, launches = [], 0, 0, 0
+    se_mom, bse_mom = [], []
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
-            s0 = ctx.stats()
-            ctx.push(pin_p, pin_t)
+            ctx.reset_tallies()
+            push_step()
             barrier(dist)
             ctx.run()
             s1 = ctx.stats()
             dev_ms.append(s1["last_run_ms"])
-            events += (s1["events_elastic"] + s1["events_inelastic"] + s1["events_boundary"]) - \
-                      (s0["events_elastic"] + s0["events_inelastic"] + s0["events_boundary"])
+            events += s1["events_elastic"] + s1["events_inelastic"] + s1["events_boundary"]
             gens = s1["generations"]
             launches += s1["generations"]
+            se_k, bse_k = ctx.tag_counts(0, n)
+            se_mom.append(step_moments(se_k))
+            bse_mom.append(step_moments(bse_k))
     clocks = clk.summary()
-    stats = ctx.stats()
     t_dev = allreduce_max(dist, sum(dev_ms) / 1000.0)
     ev_all = allreduce_sum(dist, events)
     value = ev_all / t_dev
     prim_all = allreduce_sum(dist, n * args.steps)
 
-    # SE-yield figure of merit from the timed steps' tallies: per-primary
-    # variance of the SE count, sigma^2 of the mean yield, t = device time.
-    se, bse = ctx.tag_counts(0, n)
-    mean_se = float(se.sum()) / (n * args.steps)
-    # Each tag was simulated `steps` times with independent streams, so the
-    # per-primary variance is Var(sum over the K repeats) / K.
-    var_primary = float(np.var(se.astype(np.float64))) / args.steps
-    sigma2 = var_primary / (n * args.steps) if var_primary > 0 else float("nan")
-    fom = 1.0 / (sigma2 * (sum(dev_ms) / 1000.0)) if sigma2 == sigma2 else None
+    # SE-yield figure of merit of one timed step: per-primary variance of
+    # that step's SE counts, sigma^2 of its mean yield, t = its device time.
+    plain = {"steps": args.steps,
+             "mean_se": sum(m for m, _ in se_mom) / args.steps, "var_se": sum(v for _, v in se_mom) / args.steps,
+             "mean_bse": sum(m for m, _ in bse_mom) / args.steps,
+             "var_bse": sum(v for _, v in bse_mom) / args.steps}
+    plain["fom"] = plain_fom([v for _, v in se_mom], n, [ms / 1000.0 for ms in dev_ms])
+    mean_se = plain["mean_se"]
 
     # End-to-end through the C ABI from pinned host buffers.  The scan's
     # tag -> pixel map is given once, like the geometry (setup, untimed).
@@ -534,6 +594,9 @@ def main():
     e2e_s = []
     parts = {"push_ms": 0.0, "run_ms": 0.0, "yields_ms": 0.0}
     for _ in range(args.steps):
+        ctx.reset_tallies()
+        ctx.set_uid_base(step_no[0] * world * n + g_start)
+        step_no[0] += 1
         barrier(dist)
         t0 = time.perf_counter()
         ctx.push(pin_p, pin_t)
@@ -548,12 +611,18 @@ def main():
         parts["yields_ms"] += 1000 * (t3 - t2) / args.steps
     t_e2e = allreduce_max(dist, sum(e2e_s))
     e2e_val = ev_all / t_e2e
+    # the job's image: the last step's per-pixel sums added up over the ranks
+    # (one collective, after timing)
+    image = replicas.reduce_pixel_yields(dist, out)
+    image_yield = {"frames": world, "primaries": float(image[:, 0].sum()),
+                   "se_yield": float(image[:, 1].sum() / max(image[:, 0].sum(), 1.0)),
+                   "bse_yield": float(image[:, 3].sum() / max(image[:, 0].sum(), 1.0))}
     h2d = n * 7 * 4 + n * 4
     d2h = n_pix * 5 * 8
 
     # the network's surface map and training scan are set up for the grating
     learned = None if (args.no_learned or "learned" not in WORKLOADS[args.workload]) else \
-        learned_fom(args, tris, mats[0], local, rank, prim, tags, mean_se, var_primary, fom)
+        learned_fom(args, tris, mats[0], local, rank, prim, tags, plain)
 
     line = None
     if rank == 0:
@@ -563,37 +632,49 @@ def main():
         # DRAM bytes per launch: the ncu capture's bytes per event (Kieft
         # model, this workload) times the events of one step, whose first
         # generation's launch carries the whole scan
-        traffic = None
+        traffic, dram_frac, ncu = None, None, None
         tp = os.path.join(ROOT, "profiles", "transport_kernel_traffic_%s.json" % args.workload)
         if os.path.exists(tp) and args.inelastic == "kieft":
             with open(tp) as f:
-                traffic = json.load(f)["dram_bytes_per_event"] * events / args.steps
+                prof = json.load(f)
+            traffic = prof["dram_bytes_per_event"] * events / args.steps
+            # measured DRAM bytes at this run's event rate, against the HBM peak
+            dram_frac = prof["dram_bytes_per_event"] * (events / (sum(dev_ms) / 1000.0)) / 1e9 / peak
+            ncu = {k: prof[k] for k in ("issue_active", "simt_lanes_per_instruction", "l1_hit", "l2_hit",
+                                        "source") if k in prof}
         cpu = None if args.no_cpu_baseline else cpu_baseline(tri_path, mats, recs, tmp,
                                                               WORKLOADS[args.workload]["cpu_sample"],
                                                               penn=args.inelastic == "penn")
-        ref_gpu = reference_gpu(tri_path, mats, recs, tmp, penn=args.inelastic == "penn") \
-            if args.reference_gpu else None
+        ref_gpu = reference_gpu(tri_path, mats, recs, tmp, penn=args.inelastic == "penn",
+                                workload=args.workload) if args.reference_gpu else None
         line = {
             "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": workload_name(args), "inelastic": args.inelastic,
-                       "parallelism": "replicas x%d" % world,
+                       "parallelism": "replicas x%d (one scan frame per rank, sharded by global primary index)"
+                                      % world,
                        "l2": "inputs larger than L2 (primary queue %.0f MB per step)" % (n * 48 / 1e6),
                        "autotuned": {"blocks_per_sm_variant": tuned[0], "block_size": tuned[1]},
                        "pop": "shared cursor" if args.shared_pop else "per-SM ranges"},
             "primaries_per_s": prim_all / t_dev,
             "events_per_primary": events / (n * args.steps),
-            "se_yield": mean_se, "bse_yield": float(bse.sum()) / (n * args.steps),
-            "fom_se_plain": fom,
+            "se_yield": mean_se, "bse_yield": plain["mean_bse"],
+            "fom_se_plain": plain["fom"],
             "learned_rr": learned,
+            "image": image_yield,
             "generations_per_step": gens,
             "gpu_launches": int(launches),
             "e2e": {"value": e2e_val, "unit": "events/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "pinned_host": pinned, "breakdown_ms_per_step": {k: round(v, 2) for k, v in parts.items()}},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "bytes_per_event": round(b_event, 2), "bytes_breakdown": b_parts,
+            # achieved/frac: the algorithmic bytes per event (octree, triangle,
+            # table and state gathers) at the measured event rate against the
+            # HBM peak.  L1 and L2 serve nearly all of those gathers (dram_frac
+            # is the DRAM traffic actually measured), and the kernel is bound
+            # by instruction issue under warp divergence (ncu figures).
+            "roofline": {"bound": "issue/L1-L2 latency", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "dram_frac": dram_frac, "ncu": ncu,
+                         "peak_kind": peak_kind, "bytes_per_event": round(b_event, 2), "bytes_breakdown": b_parts,
                          "kernel": "transport_kernel"},
             "clocks": clocks,
             "cpu_baseline": cpu,

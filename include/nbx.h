@@ -409,13 +409,31 @@ int nbx_features_query(nbx_ctx* ctx, const nbx_electron* electrons, uint64_t n, 
  * anything.  d_particles holds n x 7 floats (pos, dir, E), d_tags n tags;
  * uid_base numbers the primaries' random streams exactly as the n primaries
  * of an nbx_push starting at that running index, so both entry points give
- * identical tallies.  Detections are ADDED to d_se_count / d_bse_count
+ * identical per-tag counts; uid_base + n must not exceed 2^63.
+ *
+ * Plain transport only: a context in sample or learned mode, or created with
+ * record_deposits, gets NBX_ERR_STATE.  Only the per-tag counts and `counts`
+ * are produced: no detected records, histogram, per-pixel spectra or
+ * nbx_get_stats figures.  Detections are ADDED to d_se_count / d_bse_count
  * (n_tags each, caller-zeroed).  counts (host, may be null) receives
- * {elastic, inelastic, boundary, detected} of this call.  Scratch lives in a
- * fixed array of about 9.5 MB that every GPU loading the library keeps until
- * exit; the first call on a device resolves its address and should come
- * before any stream capture; calls that overlap on the GPU race on it.
- * Sizes beyond the maximum return NBX_ERR_ARG. */
+ * {elastic, inelastic, boundary, detected} of this call.
+ *
+ * Ordering: the call reads its inputs on the context's own stream, so the
+ * caller must make d_particles, d_tags and the zeroed tallies complete first
+ * (e.g. synchronise the stream that produced them).  The call returns only
+ * after the GPU has finished.
+ *
+ * Scratch lives in a fixed array of about 9.5 MB that every GPU loading the
+ * library keeps until exit.  The first call on a context looks up the array's
+ * device address and should come before any stream capture.  Calls that
+ * overlap on the GPU race on the array.
+ *
+ * Errors: sizes beyond the maximum, or uid_base + n above 2^63, return
+ * NBX_ERR_ARG.  NBX_ERR_CAPACITY means a cascade outgrew the fixed scratch
+ * (more than 65,536 secondaries waiting in one generation, or more than 256
+ * generations): electrons were lost, and the detections made before that
+ * have ALREADY been added to d_se_count / d_bse_count, so the caller should
+ * discard those tallies. */
 #define NBX_NOALLOC_MAX_PRIMARIES 65536
 int nbx_run_noalloc(nbx_ctx* ctx, const float* d_particles, const uint32_t* d_tags, uint32_t n, uint64_t uid_base,
                     uint32_t* d_se_count, uint32_t* d_bse_count, uint64_t n_tags, uint64_t counts[4]);

@@ -156,9 +156,12 @@ cudaError_t launch_pixel_yields(const uint32_t* se, const uint32_t* bse, const f
                                 const uint32_t* pixel_of_tag, uint64_t n_tags, uint64_t n_pixels, double* out,
                                 cudaStream_t s);
 // Allocation-free transport on the file-scope scratch of transport.cu
-// (see nbx_run_noalloc).  Returns 0 or an NBX_ERR_* code with *err set.
+// (see nbx_run_noalloc).  noalloc_scratch_address gives the scratch array's
+// device address on the current device; run_transport_noalloc takes it as
+// `scratch` and returns 0 or an NBX_ERR_* code with *err set.
 constexpr uint32_t kNoAllocMaxPrimaries = 65536;
-int run_transport_noalloc(const dev::Physics& P, int grid, int block, int variant, cudaStream_t s,
+cudaError_t noalloc_scratch_address(void** out);
+int run_transport_noalloc(const dev::Physics& P, int grid, int block, int variant, cudaStream_t s, void* scratch,
                           const float* d_particles,
                           const uint32_t* d_tags, uint32_t n, uint64_t uid_base, uint32_t* d_se, uint32_t* d_bse,
                           uint64_t n_tags, uint64_t counts[4], const char** err);

@@ -152,6 +152,9 @@ struct nbx_ctx {
     uint64_t pushed = 0, generations = 0;
     double last_run_ms = 0, last_kernel_ms = 0;
     int block = 256, bpsm = 0, variant = 3;
+    // device address of the allocation-free transport's scratch array,
+    // looked up by this context's first nbx_run_noalloc call
+    void* noalloc_scratch = nullptr;
 
     ~nbx_ctx() {
         for (auto* t : tables) delete t;
@@ -1486,19 +1489,36 @@ int nbx_mlp_predict(nbx_ctx* ctx, const float* features, uint64_t n, float* out)
 
 // Allocation-free transport (see include/nbx.h): device buffers in, device
 // tallies out, scratch from the library's file-scope array.  Nothing here or
-// in run_transport_noalloc allocates memory.
+// in run_transport_noalloc allocates memory.  The array's device address is
+// looked up on the context's first call, with the context's device current;
+// a context never outlives the device's primary context (cudaDeviceReset
+// invalidates its streams and buffers too), so the address cannot go stale.
 int nbx_run_noalloc(nbx_ctx* ctx, const float* d_particles, const uint32_t* d_tags, uint32_t n, uint64_t uid_base,
                     uint32_t* d_se_count, uint32_t* d_bse_count, uint64_t n_tags, uint64_t counts[4]) {
     if (!ctx || (n && (!d_particles || !d_tags)) || (n_tags && (!d_se_count || !d_bse_count))) return NBX_ERR_ARG;
     if (!ctx->have_geometry) return fail(ctx, NBX_ERR_STATE, "nbx_run_noalloc before nbx_set_geometry");
     if (n > NBX_NOALLOC_MAX_PRIMARIES)
         return fail(ctx, NBX_ERR_ARG, "nbx_run_noalloc takes at most NBX_NOALLOC_MAX_PRIMARIES (65536) primaries per call");
+    if (uid_base >= (1ull << 63) || uint64_t(n) > (1ull << 63) - uid_base)
+        return fail(ctx, NBX_ERR_ARG, "nbx_run_noalloc: uid_base + n must not exceed 2^63");
+    if (ctx->mode != nbx::kModePlain || ctx->cfg.record_deposits)
+        return fail(ctx, NBX_ERR_STATE,
+                    "nbx_run_noalloc runs plain transport only: the context is in sample or learned mode, or "
+                    "records energy deposits");
     ctx->err.clear();
     if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return fail(ctx, NBX_ERR_CUDA, "cudaSetDevice failed");
+    if (!ctx->noalloc_scratch) {
+        void* p = nullptr;
+        if (nbx::noalloc_scratch_address(&p) != cudaSuccess || !p) {
+            cudaGetLastError();
+            return fail(ctx, NBX_ERR_CUDA, "cudaGetSymbolAddress of the transport scratch failed");
+        }
+        ctx->noalloc_scratch = p;
+    }
     const char* err = "";
     const int rc = nbx::run_transport_noalloc(ctx->phys, ctx->sms * ctx->bpsm, ctx->block, ctx->variant, ctx->stream,
-                                              d_particles,
-                                              d_tags, n, uid_base, d_se_count, d_bse_count, n_tags, counts, &err);
+                                              ctx->noalloc_scratch, d_particles, d_tags, n, uid_base, d_se_count,
+                                              d_bse_count, n_tags, counts, &err);
     if (rc != 0) return fail(ctx, rc, err);
     return NBX_OK;
 }

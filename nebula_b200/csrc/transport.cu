@@ -883,12 +883,11 @@ cudaError_t launch_fill_queue(Queue q, const float* particles, const uint32_t* t
 // cursors, counters) carved from the file-scope array below: at most
 // kNoAllocMaxPrimaries primaries per call, about 9.5 MB that every GPU which
 // loads this library holds until the process exits.  Host code cannot use the
-// array's name as a device address, so the first call on each device looks the
-// address up with cudaGetSymbolAddress (with that device current) and caches
-// it; that first call should therefore come before any stream capture.  The
-// array is shared by all calls and keeps the last call's contents; each call
-// clears the cursors and counters it needs.  Calls that overlap on the GPU race
-// on the array and must be serialised by the caller.
+// array's name as a device address: the caller looks the address up with
+// noalloc_scratch_address (cudaGetSymbolAddress, with the device current) and
+// passes it in.  The array is shared by all calls and keeps the last call's
+// contents; each call clears the cursors and counters it needs.  Calls that
+// overlap on the GPU race on the array and must be serialised by the caller.
 // ---------------------------------------------------------------------------
 namespace {
 constexpr size_t kNoAllocOverflow = 1u << 16;
@@ -904,9 +903,6 @@ constexpr size_t kNoAllocScratchBytes = kOffCnt + align256(sizeof(unsigned long 
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_noalloc_mutex;
-void* g_noalloc_base[256] = {};
-
 Queue carve_queue(unsigned char* base, size_t off, size_t n) {
     Queue q;
     q.a = reinterpret_cast<float4*>(base + off);
@@ -916,7 +912,14 @@ Queue carve_queue(unsigned char* base, size_t off, size_t n) {
 }
 }  // namespace
 
-int run_transport_noalloc(const dev::Physics& P, int grid, int block, int variant, cudaStream_t s,
+cudaError_t noalloc_scratch_address(void** out) {
+    *out = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(out, g_noalloc_scratch);
+    if (e != cudaSuccess) *out = nullptr;
+    return e;
+}
+
+int run_transport_noalloc(const dev::Physics& P, int grid, int block, int variant, cudaStream_t s, void* scratch,
                           const float* d_particles,
                           const uint32_t* d_tags, uint32_t n, uint64_t uid_base, uint32_t* d_se, uint32_t* d_bse,
                           uint64_t n_tags, uint64_t counts[4], const char** err) {
@@ -925,25 +928,11 @@ int run_transport_noalloc(const dev::Physics& P, int grid, int block, int varian
         *err = "nbx_run_noalloc takes at most NBX_NOALLOC_MAX_PRIMARIES primaries per call";
         return -1;
     }
-    int device = 0;
-    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 256) {
-        *err = "cudaGetDevice failed";
+    if (!scratch) {
+        *err = "no device address for the transport scratch";
         return -3;
     }
-    unsigned char* base;
-    {
-        std::lock_guard<std::mutex> lk(g_noalloc_mutex);
-        if (!g_noalloc_base[device]) {
-            void* ptr = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-            if (e != cudaSuccess || !ptr) {
-                *err = "cudaGetSymbolAddress of the transport scratch failed";
-                return -3;
-            }
-            g_noalloc_base[device] = ptr;
-        }
-        base = static_cast<unsigned char*>(g_noalloc_base[device]);
-    }
+    unsigned char* base = static_cast<unsigned char*>(scratch);
     uint32_t* ctl = reinterpret_cast<uint32_t*>(base + kOffCtl);
     unsigned long long* cnt = reinterpret_cast<unsigned long long*>(base + kOffCnt);
     const Queue prim = carve_queue(base, kOffPrim, kNoAllocMaxPrimaries);

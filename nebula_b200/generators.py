@@ -571,8 +571,8 @@ def write_scan_pri(path, nx, ny, per_pixel, energy, rows_per_block=16, seed=0, *
     return n
 
 
-# The scans of the benchmark workloads (3 and 5): geometry,
-# materials in geometry order, and the raster scan.
+# The benchmark scans (line-space grating, rough slab with mixed beam energies,
+# contact-hole array): geometry, materials in geometry order, and the raster scan.
 SCANS = {
     "grating": dict(geometry=lambda: grating_geometry(), materials=("si",), nx=256, ny=256, per_pixel=100,
                     energy=500.0, energies=None, spacing=1.0, origin=(-128.0, -128.0), z_start=75.0),

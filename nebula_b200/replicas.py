@@ -35,11 +35,12 @@ def run_shard(ctx, records, rank: int, world: int, n_pixels: int, nx: int):
 
 def reduce_pixel_yields(dist, yields: np.ndarray) -> np.ndarray:
     """Sum the per-pixel accumulators over ranks (process group `dist`, any
-    backend; None = single process)."""
+    backend; None = single process).  The caller's array is left unchanged:
+    the all-reduce works on a copy."""
     if dist is None:
         return yields
     import torch
-    t = torch.from_numpy(np.ascontiguousarray(yields, np.float64))
+    t = torch.tensor(np.asarray(yields, np.float64))
     if dist.get_backend() == "nccl":
         t = t.cuda()
     dist.all_reduce(t, op=dist.ReduceOp.SUM)

@@ -39,9 +39,19 @@ _ref = {}
 _port = None
 
 
-def build(reference_dir="/root/reference/source"):
+def reference_source_dir():
+    """The reference's source tree: $NEBULA_REFERENCE_SOURCE, else a
+    checkout named `reference` beside this repository (reference/source)."""
+    env = os.environ.get("NEBULA_REFERENCE_SOURCE")
+    if env:
+        return env
+    return os.path.normpath(os.path.join(HERE, "..", "..", "reference", "source"))
+
+
+def build(reference_dir=None):
     """Compile the checkers (port always; ref when the reference tree exists)."""
     import subprocess
+    reference_dir = reference_dir or reference_source_dir()
     subprocess.run(["make", "-s", "-C", HERE, "port"], check=True)
     if os.path.isdir(reference_dir):
         subprocess.run(["make", "-s", "-C", HERE, "ref", "REF=" + reference_dir], check=True)

@@ -103,14 +103,12 @@ def test_material_and_config_structs_match_header():
 
 
 def test_documented_caller_compiles_and_reports_nodev(tmp_path):
-    """The minimal C++ caller of the integration guide compiles against
-    include/nbx.h, links against libnbx.so and, without a GPU, fails cleanly
-    at nbx_create (exit status 1, no crash)."""
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    m = re.search(r"```cpp\n(.*?)```", text, flags=re.S)
-    assert m
-    src = tmp_path / "caller.cpp"
-    src.write_text(m.group(1))
+    """The minimal C++ caller (examples/nbx_caller.cpp, the one the
+    integration guide points to) compiles against include/nbx.h, links
+    against libnbx.so and, without a GPU, fails cleanly at nbx_create (exit
+    status 1, no crash)."""
+    src = os.path.join(ROOT, "examples", "nbx_caller.cpp")
+    assert os.path.exists(src)
     exe = tmp_path / "caller"
     libdir = os.path.dirname(nb.LIB_PATH)
     r = subprocess.run(["g++", "-std=c++17", "-I" + os.path.join(ROOT, "include"), str(src), "-L" + libdir, "-lnbx",
