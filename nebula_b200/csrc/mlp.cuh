@@ -68,17 +68,19 @@ __device__ __forceinline__ void load_weights(Weights& w, const float* params) {
     for (int i = threadIdx.x; i < kOut; i += blockDim.x) w.b3[i] = params[kOffB3 + i];
 }
 
-// Forward pass of one warp over 32 rows: xs is the warp's [32][16] BF16
-// feature tile in shared memory (row r = lane r's electron).  Returns lane's
-// logit.  Processes the two 16-row m-tiles one after the other and streams
-// layer 2's output tiles straight into layer 3, so at most one m-tile of
-// hidden activations is live (as packed BF16 A fragments).
-__device__ __forceinline__ float warp_forward(const Weights& w, const __nv_bfloat16* xs) {
+// Forward pass of one warp over 16 * NMT rows (NMT = 1 or 2 m-tiles): xs is
+// the warp's [16 * NMT][16] BF16 feature tile in shared memory.  Returns the
+// logit of row (lane mod 16 * NMT) to each lane, so with NMT = 2 lane r gets
+// row r.  Processes the m-tiles one after the other and streams layer 2's
+// output tiles straight into layer 3, so at most one m-tile of hidden
+// activations is live (as packed BF16 A fragments).
+template <int NMT>
+__device__ __forceinline__ float warp_forward_rows(const Weights& w, const __nv_bfloat16* xs) {
     const int lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
-    float logit_lo[2], logit_hi[2];
+    float logit_lo[NMT], logit_hi[NMT];
 #pragma unroll
-    for (int mt = 0; mt < 2; ++mt) {
+    for (int mt = 0; mt < NMT; ++mt) {
         const __nv_bfloat16* xr = xs + (mt * 16) * kIn;
         uint32_t a[4];
         a[0] = ld32(xr + g * kIn + 2 * t);
@@ -124,14 +126,24 @@ __device__ __forceinline__ float warp_forward(const Weights& w, const __nv_bfloa
         logit_lo[mt] = c3[0];
         logit_hi[mt] = c3[2];
     }
-    // Deliver row r (= lane r) from lane 4 * (r % 8).
+    // Deliver row r from lane 4 * (r % 8): rows g and g + 8 of m-tile mt sit
+    // in lane 4 g (t == 0) as logit_lo[mt] and logit_hi[mt].
     const int src = 4 * (lane & 7);
+    const int hi = (lane >> 3) & 1;
     const float v0 = __shfl_sync(0xffffffffu, logit_lo[0], src);
     const float v1 = __shfl_sync(0xffffffffu, logit_hi[0], src);
-    const float v2 = __shfl_sync(0xffffffffu, logit_lo[1], src);
-    const float v3 = __shfl_sync(0xffffffffu, logit_hi[1], src);
-    const int mt = lane >> 4, hi = (lane >> 3) & 1;
-    return mt == 0 ? (hi ? v1 : v0) : (hi ? v3 : v2);
+    if constexpr (NMT == 1) {
+        return hi ? v1 : v0;
+    } else {
+        const float v2 = __shfl_sync(0xffffffffu, logit_lo[1], src);
+        const float v3 = __shfl_sync(0xffffffffu, logit_hi[1], src);
+        return (lane >> 4) == 0 ? (hi ? v1 : v0) : (hi ? v3 : v2);
+    }
+}
+
+// All 32 rows of the warp's [32][16] tile; lane r gets row r's logit.
+__device__ __forceinline__ float warp_forward(const Weights& w, const __nv_bfloat16* xs) {
+    return warp_forward_rows<2>(w, xs);
 }
 #endif
 
