@@ -60,14 +60,17 @@ WORKLOAD = "grating 256x256 px x 100 primaries @ 500 eV (6,553,600 primaries), 5
 WORKLOADS = {
     "grating": dict(rows=256, cpu_sample=409600, ref_sample=102400, desc=WORKLOAD,
                     learned=dict(map_lo=(-180, -180, -60), map_hi=(180, 180, 60), cell=1.0, d_max=20.0,
-                                 train_per_pixel=4)),
+                                 train_per_pixel=2, train_on=("grating", "rough"))),
     "rough": dict(rows=512, cpu_sample=163840, ref_sample=40960,
                   learned=dict(map_lo=(-500, -500, -40), map_hi=(500, 500, 30), cell=2.0, d_max=10.0,
-                               train_per_pixel=1),
+                               train_per_pixel=1, train_on=("grating", "rough")),
                   desc="rough slab: 512x512 Gaussian height field (RMS 3 nm, correlation 10 nm) over 1 um, "
                        "526,334 triangles; 512x512 px x 20 primaries (5,242,880) at E uniform over "
                        "{300, 1000, 3000, 5000} eV, Si-like Kieft tables"),
     "holes": dict(rows=64, tune_row=8, cpu_sample=204800, ref_sample=102400,
+                  # the map covers the default 64 pixel rows (y up to -1121 nm)
+                  learned=dict(map_lo=(-1290, -1290, -170), map_hi=(1290, -1100, 25), cell=2.0, d_max=10.0,
+                               train_per_pixel=1, train_rows=64, train_on=("holes",)),
                   desc="contact holes: 32x32 holes (40 nm diameter, 100 nm deep, +-2 nm edge roughness) in a "
                        "SiO2-like film over W-like plugs on a Si-like substrate, 2,506,772 triangles over "
                        "2.56 um; 1024x1024 px at 2.5 nm x 200 primaries at 1 keV, one step = %d pixel rows "
@@ -384,50 +387,107 @@ def run_reference(args):
     return 0
 
 
-def learned_fom(args, tris, mat, local, rank, prim, tags, plain):
-    """SE-yield figure of merit of the learned roulette on the same scan.
+# Training records per scan of the learned leg (about 4 M in all, the
+# records of the grating and the rough-slab scans for those two workloads).
+TRAIN_RECORDS = 2_000_000
 
-    A sample-mode pass over a 4-primaries-per-pixel scan (its own seed) gives
-    (features, label) pairs; the network is trained on them (8 epochs, batch
-    8192, Adam lr 1e-3); then the whole scan runs once in learned mode with one
-    tag per primary.  FOM = 1 / (sigma^2 t): sigma^2 = per-primary variance of
-    the weighted SE count of that one run / n, t = its device time -- the same
-    estimator as the plain FOM of one timed step.  `z` compares the weighted
-    SE and BSE yields with the plain yields of the timed steps
-    (unbiasedness).  `plain`: the plain steps' means, per-step variances,
-    step count and FOM."""
+
+def sample_records(name, tmp, local, rank, penn):
+    """Sample-mode run over the training scan of workload `name` (its own
+    seed): (features, labels, costs) of up to TRAIN_RECORDS newborn
+    electrons, recorded at birth."""
     import nebula_b200 as nb
     from nebula_b200 import generators as g
-    n = len(tags)
-    ctx = nb.setup(tris, [mat], device=local, seed=0x2545F491 + rank, blocks_per_sm=args.learned_variant,
-                   block_size=args.learned_block,
-                   inelastic=args.inelastic)
-    w = workload(args.workload)
+    w = workload(name)
     L = w["learned"]
+    mats = [g.make_material(os.path.join(tmp, "train_%s_%s.mat" % (name, k)), kind=k) for k in w["materials"]]
+    ctx = nb.setup(w["geometry"](), mats, device=local, seed=0x3C6EF372 + rank, inelastic=penn and "penn" or "kieft")
     try:
         ctx.build_surface_map(list(L["map_lo"]), list(L["map_hi"]), L["cell"], L["d_max"])
-        train = g.scan_beam(NX, NY, L["train_per_pixel"], ENERGY, spacing=w["spacing"], origin=w["origin"],
-                            z_start=w["z_start"], seed=0x51ED + rank, energies=w["energies"])
+        rows = range(L["train_rows"]) if "train_rows" in L else None
+        train = g.scan_beam(w["nx"], w["ny"], L["train_per_pixel"], w["energy"], spacing=w["spacing"],
+                            origin=w["origin"], z_start=w["z_start"], seed=0x51ED + rank, energies=w["energies"],
+                            rows=rows)
         ctx.set_sample_capacity(1 << 23)
         ctx.set_mode("sample")
         ctx.set_tag_range(len(train))
         ctx.reset_tallies()
         ctx.push_records(train)
         ctx.run()
-        f, y = ctx.get_samples(1 << 23)
+        f, y, c = ctx.get_samples(1 << 23, with_cost=True)
+    finally:
+        ctx.close()
+    if len(y) > TRAIN_RECORDS:
+        keep = np.random.default_rng(rank).choice(len(y), TRAIN_RECORDS, replace=False)
+        f, y, c = f[keep], y[keep], c[keep]
+    return f, y, c
+
+
+def learned_fom(args, tris, mats, local, rank, prim, tags, plain, tmp, tune_sample):
+    """SE-yield figure of merit of the learned roulette on the same scan.
+
+    Training data: sample-mode runs of the workload's training scans (for the
+    grating and the rough slab: both of them, about 4 M records recorded at
+    the birth of newborn electrons).  The network (6 -> 64 -> 64 -> 1) is
+    trained on them on the GPU (8 epochs, batch 8192, Adam lr 1e-3).  Then the
+    whole scan runs once in learned mode with one tag per primary: every
+    newborn secondary is scored at birth, plays roulette below rr_threshold
+    (default 0.05) and splits above split_threshold (default 0.5).
+    FOM = 1 / (sigma^2 t): sigma^2 = per-primary variance of the weighted SE
+    count of that one run / n, t = its device time -- the same estimator as
+    the plain FOM of one timed step.  `z` compares the weighted SE and BSE
+    yields with the plain yields of the timed steps (unbiasedness).  `plain`:
+    the plain steps' means, per-step variances, step count and FOM."""
+    import nebula_b200 as nb
+    n = len(tags)
+    w = workload(args.workload)
+    L = w["learned"]
+    penn = args.inelastic == "penn"
+    t0 = time.perf_counter()
+    parts = [sample_records(name, tmp, local, rank, penn) for name in L["train_on"]]
+    f = np.concatenate([p[0] for p in parts])
+    y = np.concatenate([p[1] for p in parts])
+    cost = np.concatenate([p[2] for p in parts])
+    t_sample = time.perf_counter() - t0
+    ctx = nb.setup(tris, mats, device=local, seed=0x2545F491 + rank, blocks_per_sm=args.learned_variant or 4,
+                   block_size=args.learned_block, inelastic=args.inelastic)
+    try:
+        ctx.build_surface_map(list(L["map_lo"]), list(L["map_hi"]), L["cell"], L["d_max"])
         ctx.mlp_set_params(nb.mlp_init_params(0))
         t0 = time.perf_counter()
         losses = ctx.mlp_train(f, y, epochs=8, batch=8192, lr=1e-3, seed=1)
         t_train = time.perf_counter() - t0
         ctx.set_tag_range(n)
-        ctx.set_mode("learned", rr_threshold=args.rr_threshold, split_threshold=2.0, rr_period=args.rr_period)
+        ctx.set_mode("learned", rr_threshold=args.rr_threshold, split_threshold=args.split_threshold,
+                     max_roulette_exp=args.max_roulette_exp)
         if args.birth_rr:
             ctx.set_birth_roulette(*[float(v) for v in args.birth_rr.split(",")])
+        cost_info = None
+        if args.learned_policy == "cost" and not args.birth_rr:
+            # cost-aware survival: mean sub-cascade cost per (material, log E)
+            # from the training records; K = steps / variance per primary of
+            # the plain timed steps
+            table, lo, hi = nb.fit_cost_table(f, cost, n_materials=len(mats))
+            value_per_cost = plain["steps_per_primary"] / plain["var_se"]
+            ctx.set_learned_cost(table, lo, hi, value_per_cost)
+            cost_info = {"value_per_cost": value_per_cost, "bins": int(table.shape[1])}
+        # launch shape, stack depth and chunk tuned in learned mode on the
+        # plain leg's tuning sample (unless --learned-variant fixes the shape)
+        tuned = ctx.autotune(prim[tune_sample], tags[tune_sample]) if not args.learned_variant else ctx.tuning()
         ctx.reset_tallies()
         ctx.push(prim, tags)
         ctx.run()
         s = ctx.stats()
         sw, bw = ctx.tag_weights(0, n)
+        # the learned kernel's own cost: the same scan with every decision
+        # off (the network still scores every newborn)
+        ctx.set_birth_roulette(0.0, 0.0, 0.0)
+        ctx.set_learned_cost(None, 0.0, 1.0, 1.0)
+        ctx.set_mode("learned", rr_threshold=0.0, split_threshold=2.0, max_roulette_exp=args.max_roulette_exp)
+        ctx.reset_tallies()
+        ctx.push(prim, tags)
+        ctx.run()
+        s_off = ctx.stats()
         t = s["last_run_ms"] / 1000.0
         m_se, v_se = step_moments(sw)
         m_bse, v_bse = step_moments(bw)
@@ -435,15 +495,24 @@ def learned_fom(args, tris, mat, local, rank, prim, tags, plain):
         k = plain["steps"]
         z_se = (m_se - plain["mean_se"]) / math.sqrt(v_se / n + plain["var_se"] / (n * k))
         z_bse = (m_bse - plain["mean_bse"]) / math.sqrt(v_bse / n + plain["var_bse"] / (n * k))
-        return {"fom_se": fom_l, "fom_se_plain": plain["fom"],
+        return {"fom_se": fom_l, "fom_se_plain": plain["fom"], "plain_ns_per_step": plain["ns_per_step"],
                 "gain": fom_l / plain["fom"] if (fom_l and plain["fom"]) else None,
                 "se_yield": m_se, "bse_yield": m_bse, "z_vs_plain": z_se, "z_bse_vs_plain": z_bse,
-                "run_ms": s["last_run_ms"],
-                "rr_threshold": args.rr_threshold, "rr_period": args.rr_period, "split": "off",
-                "birth_roulette": args.birth_rr or "off",
-                "launch": {"blocks_per_sm_variant": args.learned_variant, "block_size": args.learned_block},
-                "inferences": s["inferences"], "roulette_killed": s["roulette_killed"],
-                "steps": s["steps"], "train_samples": int(len(y)), "train_s": round(t_train, 3),
+                "run_ms": s["last_run_ms"], "var_ratio": v_se / plain["var_se"],
+                "policy": ("fixed rule at birth " + args.birth_rr) if args.birth_rr else
+                          ("network at birth, cost-aware survival" if cost_info else "network at birth, weight window"),
+                "cost_aware": cost_info,
+                "decisions_off": {"run_ms": s_off["last_run_ms"], "steps": s_off["steps"],
+                                  "ns_per_step": 1e6 * s_off["last_run_ms"] / max(s_off["steps"], 1),
+                                  "inferences": s_off["inferences"]},
+                "rr_threshold": args.rr_threshold, "split_threshold": args.split_threshold,
+                "max_roulette_exp": args.max_roulette_exp,
+                "autotuned": tuned,
+                "inferences": s["inferences"], "roulette_killed": s["roulette_killed"], "splits": s["splits"],
+                "steps": s["steps"], "train_on": list(L["train_on"]), "train_samples": int(len(y)),
+                "train_positive_rate": float(y.mean()) if len(y) else None,
+                "train_mean_cost": float(cost.mean()) if len(cost) else None,
+                "sample_s": round(t_sample, 3), "train_s": round(t_train, 3),
                 "train_loss": [round(float(v), 5) for v in losses]}
     finally:
         ctx.close()
@@ -468,14 +537,21 @@ def main():
                     help="also time the reference's own GPU program and the nbx CLI on the step's primaries")
     ap.add_argument("--shared-pop", action="store_true",
                     help="all transport blocks pop primaries from one cursor (default: per-SM ranges)")
-    ap.add_argument("--learned-variant", type=int, default=4, help="transport variant of the learned leg")
+    ap.add_argument("--learned-variant", type=int, default=0,
+                    help="transport variant of the learned leg (0: autotuned in learned mode)")
     ap.add_argument("--learned-block", type=int, default=256, help="threads per block of the learned leg")
     ap.add_argument("--birth-rr", default="",
-                    help="learned leg: roulette at birth, 'min_distance_nm,max_energy_eV,survival' (default off)")
-    ap.add_argument("--rr-threshold", type=float, default=0.02,
-                    help="learned leg: importance below which the network's weight window plays roulette")
-    ap.add_argument("--rr-period", type=int, default=32,
-                    help="learned leg: warp iterations between network evaluations (a huge value turns them off)")
+                    help="learned leg: a fixed rule at birth instead of the network, "
+                         "'min_distance_nm,max_energy_eV,survival' (default off)")
+    ap.add_argument("--rr-threshold", type=float, default=0.05,
+                    help="learned leg: importance below which a newborn secondary plays roulette")
+    ap.add_argument("--split-threshold", type=float, default=0.5,
+                    help="learned leg: importance above which a newborn secondary splits in two")
+    ap.add_argument("--max-roulette-exp", type=int, default=6,
+                    help="learned leg: lowest roulette survival is 2^-this")
+    ap.add_argument("--learned-policy", default="window", choices=["window", "cost"],
+                    help="learned leg: weight window on the network's importance (rr/split thresholds), or "
+                         "cost-aware survival w sqrt(p K / c)")
     ap.add_argument("--inelastic", default="kieft", choices=["kieft", "penn"],
                     help="inelastic model: Kieft & Bosch (the headline workload) or full Penn (the reference's stock build)")
     args = ap.parse_args()
@@ -512,21 +588,23 @@ def main():
     pin_t[:] = tags
     ctx.set_tag_range(n)
     # Autotune the transport launch shape on a 16-row sample of the scan.
+    tune_n = 0
+    # the autotuner's sample: at least 16 pixel rows and about 1.6 M primaries
+    # (records are row-major; short runs rank the launch shapes by their
+    # tails) from `tune_row` (the contact holes' first band of holes; the
+    # grating and the slab are uniform)
+    tune_rows = min(args.rows, max(16, -(-1600000 // (NX * PER_PIXEL))))
+    r0 = min(WORKLOADS[args.workload].get("tune_row", 0), max(0, args.rows - tune_rows))
+    tune_sample = np.arange(r0 * NX * PER_PIXEL, min(n, (r0 + tune_rows) * NX * PER_PIXEL))
     if args.variant:
         ctx.close()
         ctx = nb.setup(tris, mats, device=local, seed=0x78C7E39B, blocks_per_sm=args.variant,
                        block_size=args.block or 128, inelastic=args.inelastic, shared_pop=args.shared_pop)
         ctx.set_tag_range(n)
-        tuned = (args.variant, args.block or 128)
+        tuned = ctx.tuning()
     else:
-        # records are row-major: at least 16 pixel rows and about 1.6 M
-        # primaries (short runs rank the launch shapes by their tails) from
-        # `tune_row` (the contact holes' first band of holes; the grating and
-        # the slab are uniform)
-        tune_rows = min(args.rows, max(16, -(-1600000 // (NX * PER_PIXEL))))
-        r0 = min(WORKLOADS[args.workload].get("tune_row", 0), max(0, args.rows - tune_rows))
-        sample = np.arange(r0 * NX * PER_PIXEL, min(n, (r0 + tune_rows) * NX * PER_PIXEL))
-        tuned = ctx.autotune(prim[sample], tags[sample])
+        tuned = ctx.autotune(prim[tune_sample], tags[tune_sample])
+        tune_n = len(tune_sample)
 
     # One job of `world` frames of the scan, sharded by global primary index:
     # this rank's shard is [g_start, g_stop) of every step's world * n
@@ -551,7 +629,7 @@ def main():
     # timed step is one independent run over the scan; its per-primary counts
     # are read back after the run (outside the device-timed region) for the
     # per-step variance of the figure of merit.
-    dev_ms, events, gens, launches = [], 0, 0, 0
+    dev_ms, events, gens, launches, plain_steps = [], 0, 0, 0, 0
     se_mom, bse_mom = [], []
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
@@ -562,6 +640,7 @@ def main():
             s1 = ctx.stats()
             dev_ms.append(s1["last_run_ms"])
             events += s1["events_elastic"] + s1["events_inelastic"] + s1["events_boundary"]
+            plain_steps += s1["steps"]
             gens = s1["generations"]
             launches += s1["generations"]
             se_k, bse_k = ctx.tag_counts(0, n)
@@ -578,7 +657,9 @@ def main():
     plain = {"steps": args.steps,
              "mean_se": sum(m for m, _ in se_mom) / args.steps, "var_se": sum(v for _, v in se_mom) / args.steps,
              "mean_bse": sum(m for m, _ in bse_mom) / args.steps,
-             "var_bse": sum(v for _, v in bse_mom) / args.steps}
+             "var_bse": sum(v for _, v in bse_mom) / args.steps,
+             "steps_per_primary": plain_steps / (n * args.steps),
+             "ns_per_step": 1e6 * sum(dev_ms) / max(plain_steps, 1)}
     plain["fom"] = plain_fom([v for _, v in se_mom], n, [ms / 1000.0 for ms in dev_ms])
     mean_se = plain["mean_se"]
 
@@ -620,9 +701,9 @@ def main():
     h2d = n * 7 * 4 + n * 4
     d2h = n_pix * 5 * 8
 
-    # the network's surface map and training scan are set up for the grating
+    # every workload defines the learned leg's surface map and training scans
     learned = None if (args.no_learned or "learned" not in WORKLOADS[args.workload]) else \
-        learned_fom(args, tris, mats[0], local, rank, prim, tags, plain)
+        learned_fom(args, tris, mats, local, rank, prim, tags, plain, tmp, tune_sample)
 
     line = None
     if rank == 0:
@@ -655,7 +736,8 @@ def main():
                        "parallelism": "replicas x%d (one scan frame per rank, sharded by global primary index)"
                                       % world,
                        "l2": "inputs larger than L2 (primary queue %.0f MB per step)" % (n * 48 / 1e6),
-                       "autotuned": {"blocks_per_sm_variant": tuned[0], "block_size": tuned[1]},
+                       "autotuned": dict(tuned, tuned_on="%d primaries of the scan" % tune_n if tune_n else
+                                         "not tuned (--variant given)"),
                        "pop": "shared cursor" if args.shared_pop else "per-SM ranges"},
             "primaries_per_s": prim_all / t_dev,
             "events_per_primary": events / (n * args.steps),

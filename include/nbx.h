@@ -216,9 +216,9 @@ typedef struct {
     uint64_t records_dropped;
     uint64_t generations;     /* kernel launches of the last nbx_run */
     uint64_t queue_overflow;
-    uint64_t inferences;      /* warp-level network evaluations (learned mode) */
-    uint64_t roulette_killed; /* electrons ended by Russian roulette (learned mode) */
-    uint64_t splits;          /* electrons split in two (learned mode) */
+    uint64_t inferences;      /* warp-level network evaluations at birth (learned mode) */
+    uint64_t roulette_killed; /* newborn secondaries dropped by Russian roulette (learned mode) */
+    uint64_t splits;          /* newborn secondaries split in two (learned mode) */
     uint64_t samples;         /* training samples recorded (sample mode) */
     double last_run_ms;       /* device time of the last nbx_run (CUDA events) */
     double last_kernel_ms;    /* device time of its transport launches only */
@@ -295,15 +295,31 @@ int nbx_get_pixel_spectra(nbx_ctx* ctx, float* out);
 int nbx_get_spectrum(nbx_ctx* ctx, uint64_t* counts, uint32_t n_bins, float* bin_width);
 int nbx_reset_tallies(nbx_ctx* ctx);
 
-/* Autotuner (no counterpart in the reference, whose launch shape is fixed at
- * 32-thread blocks over the whole capacity, drivers/gpu/gpu_driver.inl:64):
- * runs the given sample once per transport variant (2, 3, 4 resident
- * 256-thread blocks per SM, 7 resident 128-thread blocks) and block size
- * (256, 128) -- twice on the same random streams, timing the second pass --
- * keeps the fastest, and resets the tallies.  Random streams of later pushes
- * are unaffected. */
-int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n,
-                 int32_t* blocks_per_sm, int32_t* block_size);
+/* Launch and queue settings of the transport (no counterpart in the
+ * reference, whose launch shape is fixed at 32-thread blocks over the whole
+ * slot capacity, drivers/gpu/gpu_driver.inl:64, and whose frame and batch
+ * sizes come from a prescan, gpu_main.cu:139-157). */
+typedef struct {
+    int32_t blocks_per_sm;   /* transport variant: 2, 3 or 4 resident 256-thread blocks per SM, or 7
+                                resident 128-thread blocks */
+    int32_t block_size;      /* threads per block (multiple of 32; at most 128 for variant 7) */
+    int32_t stack_depth;     /* parked ancestors per thread (1..64, default 16): a secondary born deeper
+                                in its cascade goes to the next generation's queue */
+    int32_t chunk;           /* generation launches queued between two host reads (1..64, default 8) */
+    uint64_t queue_capacity; /* out: entries of each overflow queue in the last run */
+    double sample_ms;        /* out (nbx_autotune): the sample's device time with these settings */
+} nbx_tuning;
+int nbx_set_tuning(nbx_ctx* ctx, const nbx_tuning* tuning);
+int nbx_get_tuning(nbx_ctx* ctx, nbx_tuning* tuning);
+/* Autotuner: runs the given sample in the context's current mode -- twice
+ * per setting on the same random streams, timing the second pass -- first
+ * over every transport variant x block size (256, 128), then over the stack
+ * depths 8 and 32 against the default 16, then over the chunk sizes 2 and 16
+ * against 8, keeping the fastest at each stage; applies the result, reports
+ * it in *out (may be NULL) and resets the tallies.  Random streams of later
+ * pushes are unaffected.  There is no refill threshold to tune: a thread
+ * takes its next electron from the queue the moment its current one ends. */
+int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n, nbx_tuning* out);
 
 /* ---- escape-probability network (no counterpart in the reference) ------- */
 /* MLP 6 -> 64 -> 64 -> 1 (SiLU, sigmoid), BF16 tensor-core kernels with FP32
@@ -317,37 +333,56 @@ int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* ta
 #define NBX_MLP_PARAMS 5768
 
 /* Transport modes.  PLAIN: analogue transport (the reference's method).
- * SAMPLE: plain transport that also records, for about one in sixteen steps
- * of each electron in a material (at most one record per electron), the
- * network features with the label "this electron's sub-cascade produced a
- * detected electron below 50 eV" (nbx_set_sample_capacity, nbx_get_samples).
- * LEARNED: every rr_period iterations of a warp the network predicts that
- * probability p for each of its electrons in a material, and a weight window
- * acts on it: the target weight is min(rr_threshold / p, 32) when
- * p < rr_threshold and 1 otherwise; an electron lighter than half its target
- * plays Russian roulette (survives with weight / target, then carries the
- * target weight); one heavier than twice its target with p > split_threshold
- * is split into two halves.  The expected weighted tally is unchanged (the
- * method stays unbiased).  Weighted detections go to nbx_get_tag_weights;
- * the per-tag counts stay unweighted. */
+ * SAMPLE: plain transport that also records about one in sixteen newborn
+ * electrons (secondaries at their birth, in a material): the network
+ * features there, the label "this electron's sub-cascade produced a detected
+ * electron below 50 eV" and the number of steps that sub-cascade took
+ * (nbx_set_sample_capacity, nbx_get_samples).
+ * LEARNED: plain transport of weighted electrons.  Every newborn secondary
+ * is scored at its birth by the network (the warp's newborns together, on
+ * the tensor cores): importance p = predicted escape probability.  With
+ * p < rr_threshold it plays Russian roulette: it survives with probability
+ * q = p / rr_threshold rounded to a power of two (q >= 2^-max_roulette_exp)
+ * and then carries its parent's weight / q; a lost secondary's cascade is not
+ * simulated.  With p > split_threshold it is split into two electrons of
+ * half the weight that run on different random streams.  Weights are powers
+ * of two, at most 2^12 and at least 2^-4.  The expected weighted tally
+ * equals the analogue one (the method stays unbiased).  Weighted detections
+ * go to nbx_get_tag_weights and nbx_pixel_yields; the per-tag counts and
+ * detected records stay unweighted. */
 #define NBX_MODE_PLAIN 0
 #define NBX_MODE_SAMPLE 1
 #define NBX_MODE_LEARNED 2
-int nbx_set_mode(nbx_ctx* ctx, int32_t mode, float rr_threshold, float split_threshold, int32_t rr_period);
-/* Learned mode, roulette at birth (off until set): a secondary born with
- * energy below max_energy (eV) at least min_distance (nm) from the nearest
- * surface of the surface map (outside the map counts as far) survives with
- * probability `survival` and then carries its parent's weight / survival; a
- * dropped secondary's cascade is not simulated (counted in
+int nbx_set_mode(nbx_ctx* ctx, int32_t mode, float rr_threshold, float split_threshold, int32_t max_roulette_exp);
+/* Learned mode, a fixed rule at birth instead of the network (off until
+ * set): a secondary born with energy below max_energy (eV) at least
+ * min_distance (nm) from the nearest surface of the surface map (outside the
+ * map counts as far) survives with probability `survival` rounded to a power
+ * of two, 2^-k with 1 <= k <= max_roulette_exp, and then carries its parent's
+ * weight * 2^k; a dropped secondary's cascade is not simulated (counted in
  * nbx_stats.roulette_killed).  survival 0 or 1 turns it off. */
 int nbx_set_birth_roulette(nbx_ctx* ctx, float min_distance, float max_energy, float survival);
+/* Learned mode, cost-aware survival (off until set; n_bins = 0 turns it off
+ * again): minimising the variance x cost of the tally, a newborn of weight
+ * w, importance p and mean sub-cascade cost c survives with
+ * q = w * sqrt(p * value_per_cost / c), rounded to a power of two (roulette
+ * below 1 with q >= 2^-max_roulette_exp, a split in two from sqrt(2) up); this
+ * replaces the rr_threshold / split_threshold window.  c is looked up in
+ * mean_cost[material * n_bins + bin], bins uniform in log(E / eV) over
+ * [log_e_min, log_e_max) (clamped at the ends); costs are in transport steps
+ * (e.g. the mean of nbx_get_samples' costs per bin).  value_per_cost is the
+ * steps per primary divided by the per-primary variance of the detected SE
+ * count of an analogue run. */
+int nbx_set_learned_cost(nbx_ctx* ctx, const float* mean_cost, int32_t n_materials, int32_t n_bins,
+                         float log_e_min, float log_e_max, float value_per_cost);
 /* Nearest-triangle map over the box [lo, hi) with the given cell size (nm);
  * surfaces farther than d_max (nm) count as "far".  Needed for the distance
  * and cosine features. */
 int nbx_build_surface_map(nbx_ctx* ctx, const float lo[3], const float hi[3], float cell, float d_max);
 int nbx_set_sample_capacity(nbx_ctx* ctx, uint64_t capacity);
-/* Copy out (and clear) the recorded samples: features n x 6, labels n. */
-int nbx_get_samples(nbx_ctx* ctx, float* features, float* labels, uint64_t cap, uint64_t* n);
+/* Copy out (and clear) the recorded samples: features n x 6, labels n and,
+ * when costs is not NULL, the sub-cascade step counts n. */
+int nbx_get_samples(nbx_ctx* ctx, float* features, float* labels, float* costs, uint64_t cap, uint64_t* n);
 int nbx_get_tag_weights(nbx_ctx* ctx, uint64_t first_tag, uint64_t n, float* se_w, float* bse_w);
 int nbx_mlp_set_params(nbx_ctx* ctx, const float* params);
 int nbx_mlp_get_params(nbx_ctx* ctx, float* params);

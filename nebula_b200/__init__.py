@@ -76,6 +76,14 @@ class Config(C.Structure):
                 ("record_deposits", C.c_int32), ("deposit_capacity", C.c_uint64), ("shared_pop", C.c_int32)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("blocks_per_sm", C.c_int32), ("block_size", C.c_int32), ("stack_depth", C.c_int32),
+                ("chunk", C.c_int32), ("queue_capacity", C.c_uint64), ("sample_ms", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class Stats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "primaries_pushed", "primaries_done", "steps", "events_elastic", "events_inelastic", "events_boundary",
@@ -152,7 +160,7 @@ def lib():
         "nbx_set_birth_roulette": (C.c_int, [_vp, C.c_float, C.c_float, C.c_float]),
         "nbx_build_surface_map": (C.c_int, [_vp, _vp, _vp, C.c_float, C.c_float]),
         "nbx_set_sample_capacity": (C.c_int, [_vp, C.c_uint64]),
-        "nbx_get_samples": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.POINTER(C.c_uint64)]),
+        "nbx_get_samples": (C.c_int, [_vp, _vp, _vp, _vp, C.c_uint64, C.POINTER(C.c_uint64)]),
         "nbx_get_tag_weights": (C.c_int, [_vp, C.c_uint64, C.c_uint64, _vp, _vp]),
         "nbx_features_query": (C.c_int, [_vp, _vp, C.c_uint64, _vp]),
         "nbx_mlp_set_params": (C.c_int, [_vp, _vp]),
@@ -160,7 +168,10 @@ def lib():
         "nbx_mlp_grad": (C.c_int, [_vp, _vp, _vp, C.c_uint64, _vp, C.POINTER(C.c_float)]),
         "nbx_mlp_train": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.c_int32, C.c_int32, C.c_float, C.c_uint32, _vp]),
         "nbx_mlp_predict": (C.c_int, [_vp, _vp, C.c_uint64, _vp]),
-        "nbx_autotune": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+        "nbx_autotune": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.POINTER(Tuning)]),
+        "nbx_set_tuning": (C.c_int, [_vp, C.POINTER(Tuning)]),
+        "nbx_set_learned_cost": (C.c_int, [_vp, _vp, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float]),
+        "nbx_get_tuning": (C.c_int, [_vp, C.POINTER(Tuning)]),
         "nbx_run_noalloc": (C.c_int, [_vp, _vp, _vp, C.c_uint32, C.c_uint64, _vp, _vp, C.c_uint64,
                                       C.POINTER(C.c_uint64)]),
     }
@@ -338,14 +349,23 @@ class Context:
     def set_uid_base(self, base):
         self._ck(self.L.nbx_set_uid_base(self.h, base))
 
-    def autotune(self, particles: np.ndarray, tags: np.ndarray):
-        """Pick the fastest transport variant / block size on a sample; returns (blocks_per_sm, block)."""
+    def autotune(self, particles: np.ndarray, tags: np.ndarray) -> dict:
+        """Pick the fastest launch shape, stack depth and chunk size on a
+        sample, in the context's current mode; returns the chosen settings."""
         p = np.ascontiguousarray(particles, np.float32).reshape(-1, 7)
         t = np.ascontiguousarray(tags, np.uint32)
-        v = C.c_int32()
-        b = C.c_int32()
-        self._ck(self.L.nbx_autotune(self.h, _ptr(p), _ptr(t), len(t), C.byref(v), C.byref(b)))
-        return v.value, b.value
+        out = Tuning()
+        self._ck(self.L.nbx_autotune(self.h, _ptr(p), _ptr(t), len(t), C.byref(out)))
+        return out.as_dict()
+
+    def set_tuning(self, blocks_per_sm, block_size, stack_depth=16, chunk=8):
+        tu = Tuning(blocks_per_sm, block_size, stack_depth, chunk, 0, 0.0)
+        self._ck(self.L.nbx_set_tuning(self.h, C.byref(tu)))
+
+    def tuning(self) -> dict:
+        out = Tuning()
+        self._ck(self.L.nbx_get_tuning(self.h, C.byref(out)))
+        return out.as_dict()
 
     def stats(self) -> dict:
         s = Stats()
@@ -455,12 +475,29 @@ class Context:
     # ---- learned roulette -------------------------------------------------
     MODES = {"plain": 0, "sample": 1, "learned": 2}
 
-    def set_mode(self, mode, rr_threshold=0.05, split_threshold=0.5, rr_period=8):
-        self._ck(self.L.nbx_set_mode(self.h, self.MODES.get(mode, mode), rr_threshold, split_threshold, rr_period))
+    def set_mode(self, mode, rr_threshold=0.05, split_threshold=0.5, max_roulette_exp=6):
+        """plain / sample / learned (see include/nbx.h); in learned mode a
+        newborn secondary of importance p < rr_threshold plays roulette with
+        survival p / rr_threshold rounded to a power of two (at least
+        2^-max_roulette_exp) and one with p > split_threshold splits in two."""
+        self._ck(self.L.nbx_set_mode(self.h, self.MODES.get(mode, mode), rr_threshold, split_threshold,
+                                     max_roulette_exp))
 
     def set_birth_roulette(self, min_distance, max_energy, survival):
         """Learned mode: roulette at a secondary's birth (see include/nbx.h)."""
         self._ck(self.L.nbx_set_birth_roulette(self.h, min_distance, max_energy, survival))
+
+    def set_learned_cost(self, mean_cost, log_e_min, log_e_max, value_per_cost):
+        """Cost-aware survival of the learned mode (see include/nbx.h):
+        mean_cost is n_materials x n_bins steps; None turns it off."""
+        if mean_cost is None:
+            self._ck(self.L.nbx_set_learned_cost(self.h, None, 0, 0, 0.0, 1.0, 1.0))
+            return
+        t = np.ascontiguousarray(mean_cost, np.float32)
+        if t.ndim == 1:
+            t = t[None, :]
+        self._ck(self.L.nbx_set_learned_cost(self.h, _ptr(t), t.shape[0], t.shape[1], log_e_min, log_e_max,
+                                             value_per_cost))
 
     def build_surface_map(self, lo, hi, cell=1.0, d_max=20.0):
         lo = np.ascontiguousarray(lo, np.float32)
@@ -470,11 +507,17 @@ class Context:
     def set_sample_capacity(self, n):
         self._ck(self.L.nbx_set_sample_capacity(self.h, n))
 
-    def get_samples(self, cap):
+    def get_samples(self, cap, with_cost=False):
+        """Recorded training samples (and clears them): features n x 6 at
+        birth, labels n, and with `with_cost` the steps of each sample's
+        sub-cascade."""
         f = np.zeros((cap, 6), np.float32)
         y = np.zeros(cap, np.float32)
+        c = np.zeros(cap, np.float32)
         n = C.c_uint64()
-        self._ck(self.L.nbx_get_samples(self.h, _ptr(f), _ptr(y), cap, C.byref(n)))
+        self._ck(self.L.nbx_get_samples(self.h, _ptr(f), _ptr(y), _ptr(c), cap, C.byref(n)))
+        if with_cost:
+            return f[: n.value], y[: n.value], c[: n.value]
         return f[: n.value], y[: n.value]
 
     def tag_weights(self, first, n):
@@ -554,6 +597,33 @@ def setup(tri_path_or_array, mat_paths, **ctx_kwargs):
     for p in mat_paths:
         ctx.add_material(HostMaterial(p))
     return ctx
+
+
+def fit_cost_table(features, costs, n_materials=1, n_bins=32):
+    """Mean sub-cascade cost per (material, log-energy bin) from sample-mode
+    records (features as recorded: f[0] = (log E - 2.5) / 6.5, material
+    one-hot in f[3:6]), for nbx_set_learned_cost: returns (table
+    n_materials x n_bins, log_e_min, log_e_max).  Empty bins take the
+    nearest filled bin of the same material (1 step if the material has
+    none)."""
+    f = np.asarray(features, np.float64)
+    c = np.asarray(costs, np.float64)
+    log_e = f[:, 0] * 6.5 + 2.5
+    lo, hi = 2.5, 9.0
+    b = np.clip(((log_e - lo) / (hi - lo) * n_bins).astype(np.int64), 0, n_bins - 1)
+    mat = np.argmax(f[:, 3:6], axis=1) if f.shape[1] >= 6 else np.zeros(len(f), np.int64)
+    table = np.ones((n_materials, n_bins), np.float64)
+    for m in range(n_materials):
+        sel = mat == m
+        s = np.bincount(b[sel], weights=c[sel], minlength=n_bins)
+        k = np.bincount(b[sel], minlength=n_bins)
+        filled = np.flatnonzero(k)
+        if len(filled) == 0:
+            continue
+        mean = np.where(k > 0, s / np.maximum(k, 1), 0.0)
+        nearest = filled[np.abs(np.arange(n_bins)[:, None] - filled[None, :]).argmin(axis=1)]
+        table[m] = np.maximum(mean[nearest], 1.0)
+    return table.astype(np.float32), lo, hi
 
 
 def mlp_init_params(seed=0) -> np.ndarray:

@@ -106,8 +106,9 @@ __device__ __forceinline__ float surface_distance(const Geometry& g, const Surfa
 constexpr float kLogEOffset = 2.5f;
 constexpr float kLogEScale = 1.0f / 6.5f;
 
-// f[6] for an electron at p with unit direction d in material `mat` (>= 0).
-__device__ __forceinline__ void electron_features(const Geometry& g, const SurfaceMap& S, float px, float py, float pz,
+// f[6] for an electron at p with unit direction d in material `mat` (>= 0);
+// tri: the geometry's triangle records (Geometry::tri).
+__device__ __forceinline__ void electron_features(const float4* tri, const SurfaceMap& S, float px, float py, float pz,
                                                   float dx, float dy, float dz, float logE, int mat, float f[6]) {
     f[0] = (logE - kLogEOffset) * kLogEScale;
     f[1] = 1.0f;
@@ -122,7 +123,7 @@ __device__ __forceinline__ void electron_features(const Geometry& g, const Surfa
     if (ix < 0 || iy < 0 || iz < 0 || ix >= S.nx || iy >= S.ny || iz >= S.nz) return;
     const int ti = __ldg(S.cell_tri + (size_t(iz) * S.ny + iy) * S.nx + ix);
     if (ti < 0) return;
-    const float4 a = __ldg(g.tri + 3 * ti), b = __ldg(g.tri + 3 * ti + 1), c = __ldg(g.tri + 3 * ti + 2);
+    const float4 a = __ldg(tri + 3 * ti), b = __ldg(tri + 3 * ti + 1), c = __ldg(tri + 3 * ti + 2);
     float qx, qy, qz;
     closest_point_on_triangle(px, py, pz, a, b, c, &qx, &qy, &qz);
     const float dist = sqrtf((px - qx) * (px - qx) + (py - qy) * (py - qy) + (pz - qz) * (pz - qz));
@@ -134,6 +135,10 @@ __device__ __forceinline__ void electron_features(const Geometry& g, const Surfa
     const float sgn = (__float_as_int(a.w) == mat) ? 1.0f : -1.0f;
     f[1] = fminf(dist, S.d_max) / S.d_max;
     f[2] = sgn * (nx * dx + ny * dy + nz * dz) * inv;
+}
+__device__ __forceinline__ void electron_features(const Geometry& g, const SurfaceMap& S, float px, float py, float pz,
+                                                  float dx, float dy, float dz, float logE, int mat, float f[6]) {
+    electron_features(g.tri, S, px, py, pz, dx, dy, dz, logE, mat, f);
 }
 #endif
 

@@ -67,23 +67,39 @@ struct TransportArgs {
     unsigned long long* hist;   // detected-energy histogram
     int n_bins;
     float inv_bin_width;
-    // sample mode: one (features, label) record per sampled electron
-    float* sample_feat;         // [capacity][6]
+    // sample mode: one (features, label, cost) record per sampled newborn electron
+    float* sample_feat;         // [capacity][6]: features at birth
     float* sample_label;        // [capacity]: sub-cascade produced a detected SE
+    float* sample_cost;         // [capacity]: steps of the sub-cascade (nullptr: not kept)
     uint32_t* sample_count;
     uint32_t sample_capacity;
-    // learned mode: weighted roulette / splitting driven by the network
+    // learned mode: every newborn secondary is scored by the network at birth
+    // (mlp_params); importance p < rr_threshold: Russian roulette with
+    // survival p / rr_threshold rounded to a power of two, at least
+    // 2^-max_roulette_exp; p > split_threshold: split in two
     const float* mlp_params;
     float* se_w;                // per-tag weighted detections below / at or above 50 eV
     float* bse_w;
     float rr_threshold;
     float split_threshold;
-    int rr_period;              // infer every rr_period steps of an electron
-    // learned mode, roulette at birth: a secondary born with energy below
-    // birth_max_energy and at least birth_min_distance from the nearest
-    // surface (the surface map's distance; outside the map counts as far)
-    // survives with probability birth_survival and then carries its parent's
-    // weight / birth_survival.  birth_survival outside (0, 1): off.
+    int max_roulette_exp;
+    // learned mode, cost-aware survival (cost_bins > 0): a newborn of weight
+    // 2^wexp, importance p and mean sub-cascade cost c survives with
+    // q = 2^wexp sqrt(p * value_per_cost / c); c = cost_table[mat * cost_bins
+    // + bin of log E over [cost_log_e_min, cost_log_e_min + cost_bins /
+    // cost_inv_width)]
+    const float* cost_table;
+    int cost_bins;
+    int cost_materials;
+    float cost_log_e_min;
+    float cost_inv_width;
+    float value_per_cost;
+    // learned mode, fixed rule at birth instead of the network: a secondary
+    // born with energy below birth_max_energy and at least birth_min_distance
+    // from the nearest surface (the surface map's distance; outside the map
+    // counts as far) survives with probability birth_survival rounded to a
+    // power of two and then carries its parent's weight / survival.
+    // birth_survival outside (0, 1): off.
     float birth_min_distance;
     float birth_max_energy;
     float birth_survival;
@@ -94,9 +110,10 @@ struct TransportArgs {
     float* dep;
     unsigned long long* dep_cursor;   // records handed out (chunks of kDepositChunk)
     unsigned long long dep_capacity;  // records the buffer holds
-    // parked-ancestor stacks, 3 * kLocalStack float4 per launched thread
-    // (nullptr: a local-memory array)
+    // parked-ancestor stacks, 3 * stack_depth float4 per launched thread
+    // (nullptr: a local-memory array of kLocalStack entries)
     float4* stack_mem;
+    int stack_depth;            // 1 .. kMaxStack: parked ancestors per thread in stack_mem
     // per-pixel exit spectra (nullptr: off): pix_spec[pixel * pix_bins + bin]
     // counts (weights in learned mode) of detections, pixel = pixel_of_tag[tag]
     float* pix_spec;
@@ -115,10 +132,11 @@ constexpr uint32_t kDepositEmpty = 0xFFFFFFFFu;
 
 enum : int { kModePlain = 0, kModeSample = 1, kModeLearned = 2, kModeDeposit = 3 };
 
-#ifndef NBX_LOCAL_STACK
-#define NBX_LOCAL_STACK 16
-#endif
-constexpr int kLocalStack = NBX_LOCAL_STACK;  // per-thread stack of parked ancestors (depth-first cascades)
+// Per-thread stack of parked ancestors (depth-first cascades): the depth of
+// the local-memory array used without a stack buffer, and the largest depth
+// a stack buffer may be given.
+constexpr int kLocalStack = 16;
+constexpr int kMaxStack = 64;
 
 // variant: resident blocks per SM the kernel was compiled for (2, 3 or 4);
 // mode: kModePlain, kModeSample or kModeLearned.

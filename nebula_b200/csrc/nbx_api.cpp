@@ -79,7 +79,6 @@ struct QueueBuf {
 };
 
 constexpr int kMaxGenerations = 4096;
-constexpr int kChunk = 8;
 constexpr int kHistBins = 20000;
 constexpr float kHistWidth = 0.5f;
 
@@ -130,11 +129,14 @@ struct nbx_ctx {
     // transport mode (plain / sample / learned) and its buffers
     int mode = nbx::kModePlain;
     float rr_threshold = 0.05f, split_threshold = 0.5f;
-    int rr_period = 8;
+    int max_roulette_exp = 6;
     float birth_min_distance = 0.0f, birth_max_energy = 0.0f, birth_survival = 0.0f;   // off
+    DevBuf<float> cost_table;      // cost-aware survival (nbx_set_learned_cost)
+    int cost_bins = 0, cost_materials = 0;
+    float cost_log_e_min = 0, cost_inv_width = 0, value_per_cost = 0;
     DevBuf<int32_t> smap_cells;
     nbx::dev::SurfaceMap smap{};
-    DevBuf<float> sample_feat, sample_label;
+    DevBuf<float> sample_feat, sample_label, sample_cost;
     DevBuf<uint32_t> sample_count;
     uint64_t sample_cap = 0;
     DevBuf<float> se_w, bse_w;
@@ -152,6 +154,9 @@ struct nbx_ctx {
     uint64_t pushed = 0, generations = 0;
     double last_run_ms = 0, last_kernel_ms = 0;
     int block = 256, bpsm = 0, variant = 3;
+    int stack_depth = 16;   // parked ancestors per thread before a secondary goes to the next generation
+    int chunk = 8;          // generation launches queued between two 4-byte host reads
+    uint64_t queue_capacity = 0;   // overflow-queue entries of the last run
     // device address of the allocation-free transport's scratch array,
     // looked up by this context's first nbx_run_noalloc call
     void* noalloc_scratch = nullptr;
@@ -700,6 +705,7 @@ int nbx_run(nbx_ctx* ctx) {
             ctx->qb.ensure(want);
         }
         const uint32_t cap = uint32_t(std::min(ctx->qa.cap, ctx->qb.cap));
+        ctx->queue_capacity = cap;
         uint32_t* ctl = ctx->ctl.p;
         ck(cudaMemsetAsync(ctl, 0, sizeof(uint32_t) * (2 * kMaxGenerations + 2), ctx->stream), "memset");
         const uint32_t nq = uint32_t(ctx->n_queued);
@@ -730,6 +736,7 @@ int nbx_run(nbx_ctx* ctx) {
             if (!ctx->sample_cap) throw ApiError(NBX_ERR_STATE, "sample mode without nbx_set_sample_capacity");
             a.sample_feat = ctx->sample_feat.p;
             a.sample_label = ctx->sample_label.p;
+            a.sample_cost = ctx->sample_cost.p;
             a.sample_count = ctx->sample_count.p;
             a.sample_capacity = uint32_t(std::min<uint64_t>(ctx->sample_cap, 0xFFFFFFF0ull));
         }
@@ -740,7 +747,15 @@ int nbx_run(nbx_ctx* ctx) {
             a.bse_w = ctx->bse_w.p;
             a.rr_threshold = ctx->rr_threshold;
             a.split_threshold = ctx->split_threshold;
-            a.rr_period = ctx->rr_period;
+            a.max_roulette_exp = ctx->max_roulette_exp;
+            if (ctx->cost_bins > 0) {
+                a.cost_table = ctx->cost_table.p;
+                a.cost_bins = ctx->cost_bins;
+                a.cost_materials = ctx->cost_materials;
+                a.cost_log_e_min = ctx->cost_log_e_min;
+                a.cost_inv_width = ctx->cost_inv_width;
+                a.value_per_cost = ctx->value_per_cost;
+            }
             a.birth_min_distance = ctx->birth_min_distance;
             a.birth_max_energy = ctx->birth_max_energy;
             a.birth_survival = ctx->birth_survival;
@@ -757,8 +772,9 @@ int nbx_run(nbx_ctx* ctx) {
         const int bpsm = nbx::transport_max_blocks_per_sm(ctx->block, ctx->variant, mode);
         const int grid = ctx->sms * bpsm;
         // parked-ancestor stacks of the launched threads (grow-only)
-        ctx->stack_mem.ensure(uint64_t(grid) * uint64_t(ctx->block) * 3 * nbx::kLocalStack);
+        ctx->stack_mem.ensure(uint64_t(grid) * uint64_t(ctx->block) * 3 * uint64_t(ctx->stack_depth));
         a.stack_mem = ctx->stack_mem.p;
+        a.stack_depth = ctx->stack_depth;
         // The primaries are popped from per-SM ranges (neighbouring queue
         // entries stay on one SM); the secondary generations, written in
         // arbitrary order, from one shared cursor.
@@ -772,7 +788,7 @@ int nbx_run(nbx_ctx* ctx) {
         int g = 0;
         bool done = false;
         while (!done) {
-            for (int k = 0; k < kChunk && g < kMaxGenerations; ++k, ++g) {
+            for (int k = 0; k < ctx->chunk && g < kMaxGenerations; ++k, ++g) {
                 const QueueBuf* in = g == 0 ? &ctx->prim : (g % 2 == 1 ? &ctx->qa : &ctx->qb);
                 const QueueBuf* out = (g % 2 == 0) ? &ctx->qa : &ctx->qb;
                 a.in = in->q();
@@ -1145,32 +1161,68 @@ int nbx_step_query(nbx_ctx* ctx, nbx_electron* electrons, uint64_t n, int32_t* s
     });
 }
 
-int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n,
-                 int32_t* blocks_per_sm, int32_t* block_size) {
+int nbx_set_tuning(nbx_ctx* ctx, const nbx_tuning* t) {
+    if (!ctx || !t) return NBX_ERR_ARG;
+    const int v = t->blocks_per_sm, b = t->block_size;
+    if (!((v >= 2 && v <= 4) || v == 7) || b <= 0 || b % 32 != 0 || b > (v == 7 ? 128 : 256) ||
+        t->stack_depth < 1 || t->stack_depth > nbx::kMaxStack || t->chunk < 1 || t->chunk > 64)
+        return fail(ctx, NBX_ERR_ARG, "nbx_set_tuning: variant 2/3/4 with blocks of 32..256 threads or 7 with "
+                                      "32..128, stack depth 1..64, chunk 1..64");
+    return guarded(ctx, [&] {
+        ctx->variant = v;
+        ctx->block = b;
+        ctx->bpsm = nbx::transport_max_blocks_per_sm(b, v);
+        ctx->stack_depth = t->stack_depth;
+        ctx->chunk = t->chunk;
+        return NBX_OK;
+    });
+}
+
+int nbx_get_tuning(nbx_ctx* ctx, nbx_tuning* t) {
+    if (!ctx || !t) return NBX_ERR_ARG;
+    t->blocks_per_sm = ctx->variant;
+    t->block_size = ctx->block;
+    t->stack_depth = ctx->stack_depth;
+    t->chunk = ctx->chunk;
+    t->queue_capacity = ctx->queue_capacity;
+    t->sample_ms = 0;
+    return NBX_OK;
+}
+
+int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n, nbx_tuning* out) {
     if (!ctx || !particles || !tags || n == 0) return NBX_ERR_ARG;
     if (!ctx->have_geometry) return fail(ctx, NBX_ERR_STATE, "nbx_autotune before nbx_set_geometry");
     if (ctx->n_queued) return fail(ctx, NBX_ERR_STATE, "nbx_autotune with primaries queued");
+    const uint64_t uid_save = ctx->uid_next;
+    // Time the sample with the context's current settings (its mode
+    // included): twice on the same random streams, the first pass also
+    // paying one-time costs (module load, buffer growth); the second is kept.
+    auto time_it = [&](double* ms) {
+        for (int rep = 0; rep < 2; ++rep) {
+            ctx->uid_next = uid_save;
+            int rc = nbx_push(ctx, particles, tags, n, nullptr);
+            if (rc == NBX_OK) rc = nbx_run(ctx);
+            if (rc != NBX_OK) return rc;
+        }
+        *ms = ctx->last_run_ms;
+        return NBX_OK;
+    };
+    double best = 1e300;
+    // 1. launch shape: transport variant x block size
+    int best_v = ctx->variant, best_b = ctx->block;
     const int variants[4] = {2, 3, 4, 7};
     const int blocks[2] = {256, 128};
-    double best = 1e300;
-    int best_v = ctx->variant, best_b = ctx->block;
-    const uint64_t uid_save = ctx->uid_next;
     for (int v : variants) {
         for (int b : blocks) {
             if (v == 7 && b > 128) continue;   // 128-thread variant
             ctx->variant = v;
             ctx->block = b;
             ctx->bpsm = nbx::transport_max_blocks_per_sm(b, v);
-            // Twice on the same random streams: the first pass also pays the
-            // kernel's one-time module load, the second is the timing kept.
-            for (int rep = 0; rep < 2; ++rep) {
-                ctx->uid_next = uid_save;
-                int rc = nbx_push(ctx, particles, tags, n, nullptr);
-                if (rc == NBX_OK) rc = nbx_run(ctx);
-                if (rc != NBX_OK) return rc;
-            }
-            if (ctx->last_run_ms < best) {
-                best = ctx->last_run_ms;
+            double ms = 0;
+            const int rc = time_it(&ms);
+            if (rc != NBX_OK) return rc;
+            if (ms < best) {
+                best = ms;
                 best_v = v;
                 best_b = b;
             }
@@ -1179,9 +1231,40 @@ int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* ta
     ctx->variant = best_v;
     ctx->block = best_b;
     ctx->bpsm = nbx::transport_max_blocks_per_sm(best_b, best_v);
+    // 2. parked-stack depth: a shallower stack sends deep cascades' secondaries
+    // through the next generation's queue sooner; a deeper one holds more
+    // global memory per thread
+    int best_depth = ctx->stack_depth;
+    for (int d : {8, 32}) {
+        ctx->stack_depth = d;
+        double ms = 0;
+        const int rc = time_it(&ms);
+        if (rc != NBX_OK) return rc;
+        if (ms < best) {
+            best = ms;
+            best_depth = d;
+        }
+    }
+    ctx->stack_depth = best_depth;
+    // 3. generation launches queued between two host reads of the last
+    // generation's size
+    int best_chunk = ctx->chunk;
+    for (int c : {2, 16}) {
+        ctx->chunk = c;
+        double ms = 0;
+        const int rc = time_it(&ms);
+        if (rc != NBX_OK) return rc;
+        if (ms < best) {
+            best = ms;
+            best_chunk = c;
+        }
+    }
+    ctx->chunk = best_chunk;
     ctx->uid_next = uid_save;
-    if (blocks_per_sm) *blocks_per_sm = best_v;
-    if (block_size) *block_size = best_b;
+    if (out) {
+        nbx_get_tuning(ctx, out);
+        out->sample_ms = best;
+    }
     return nbx_reset_tallies(ctx);
 }
 
@@ -1192,13 +1275,14 @@ int nbx_set_uid_base(nbx_ctx* ctx, uint64_t base) {
     return NBX_OK;
 }
 
-int nbx_set_mode(nbx_ctx* ctx, int32_t mode, float rr_threshold, float split_threshold, int32_t rr_period) {
-    if (!ctx || mode < 0 || mode > 2 || !(rr_threshold >= 0) || !(split_threshold > 0) || rr_period <= 0)
+int nbx_set_mode(nbx_ctx* ctx, int32_t mode, float rr_threshold, float split_threshold, int32_t max_roulette_exp) {
+    if (!ctx || mode < 0 || mode > 2 || !(rr_threshold >= 0) || !(split_threshold > 0) || max_roulette_exp < 1 ||
+        max_roulette_exp > 12)
         return NBX_ERR_ARG;
     ctx->mode = mode;
     ctx->rr_threshold = rr_threshold;
     ctx->split_threshold = split_threshold;
-    ctx->rr_period = rr_period;
+    ctx->max_roulette_exp = max_roulette_exp;
     return NBX_OK;
 }
 
@@ -1208,6 +1292,31 @@ int nbx_set_birth_roulette(nbx_ctx* ctx, float min_distance, float max_energy, f
     ctx->birth_max_energy = max_energy;
     ctx->birth_survival = survival;
     return NBX_OK;
+}
+
+int nbx_set_learned_cost(nbx_ctx* ctx, const float* mean_cost, int32_t n_materials, int32_t n_bins,
+                         float log_e_min, float log_e_max, float value_per_cost) {
+    if (!ctx || n_bins < 0) return NBX_ERR_ARG;
+    if (n_bins == 0) {
+        ctx->cost_bins = 0;
+        return NBX_OK;
+    }
+    if (!mean_cost || n_materials < 1 || n_materials > NBX_MAX_MATERIALS || n_bins > 4096 ||
+        !(log_e_max > log_e_min) || !(value_per_cost > 0))
+        return fail(ctx, NBX_ERR_ARG, "nbx_set_learned_cost: bad table shape, energy range or value per cost");
+    for (int64_t i = 0; i < int64_t(n_materials) * n_bins; ++i)
+        if (!(mean_cost[i] > 0) || !std::isfinite(mean_cost[i]))
+            return fail(ctx, NBX_ERR_ARG, "nbx_set_learned_cost: costs must be positive and finite");
+    return guarded(ctx, [&] {
+        ctx->cost_table.alloc(uint64_t(n_materials) * n_bins);
+        to_device(ctx, ctx->cost_table.p, mean_cost, sizeof(float) * size_t(n_materials) * n_bins, "H2D");
+        ctx->cost_bins = n_bins;
+        ctx->cost_materials = n_materials;
+        ctx->cost_log_e_min = log_e_min;
+        ctx->cost_inv_width = float(n_bins) / (log_e_max - log_e_min);
+        ctx->value_per_cost = value_per_cost;
+        return NBX_OK;
+    });
 }
 
 int nbx_build_surface_map(nbx_ctx* ctx, const float lo[3], const float hi[3], float cell, float d_max) {
@@ -1305,15 +1414,17 @@ int nbx_set_sample_capacity(nbx_ctx* ctx, uint64_t capacity) {
     return guarded(ctx, [&] {
         ctx->sample_feat.alloc(6 * capacity);
         ctx->sample_label.alloc(capacity);
+        ctx->sample_cost.alloc(capacity);
         ctx->sample_count.alloc(1);
         zero(ctx, ctx->sample_count.p, 4, "memset");
         zero(ctx, ctx->sample_label.p, 4 * capacity, "memset");
+        zero(ctx, ctx->sample_cost.p, 4 * capacity, "memset");
         ctx->sample_cap = capacity;
         return NBX_OK;
     });
 }
 
-int nbx_get_samples(nbx_ctx* ctx, float* features, float* labels, uint64_t cap, uint64_t* n) {
+int nbx_get_samples(nbx_ctx* ctx, float* features, float* labels, float* costs, uint64_t cap, uint64_t* n) {
     if (!ctx || !n || (cap && (!features || !labels))) return NBX_ERR_ARG;
     return guarded(ctx, [&] {
         *n = 0;
@@ -1325,9 +1436,11 @@ int nbx_get_samples(nbx_ctx* ctx, float* features, float* labels, uint64_t cap, 
         if (take) {
             to_host(ctx, features, ctx->sample_feat.p, 24 * take, "D2H");
             to_host(ctx, labels, ctx->sample_label.p, 4 * take, "D2H");
+            if (costs) to_host(ctx, costs, ctx->sample_cost.p, 4 * take, "D2H");
         }
         zero(ctx, ctx->sample_count.p, 4, "memset");
         zero(ctx, ctx->sample_label.p, 4 * ctx->sample_cap, "memset");
+        zero(ctx, ctx->sample_cost.p, 4 * ctx->sample_cap, "memset");
         *n = take;
         return NBX_OK;
     });

@@ -62,44 +62,86 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
     return v;
 }
 
-// Largest weight the roulette may give a survivor.
-constexpr float kMaxWeight = 32.0f;
+// Learned mode: statistical weights are powers of two, 2^wexp, so every
+// roulette survivor's weight 1 / q is exact and fits in a few bits of the
+// parked material word; wexp stays within [kMinWeightExp, kMaxWeightExp].
+constexpr int kMaxWeightExp = 12;   // at most 4096 (a chain of roulettes)
+constexpr int kMinWeightExp = -4;   // at least 1/16 (a chain of splits)
+// An overflowed newborn secondary of the learned mode carries its weight
+// exponent in the queue's last-triangle word (a secondary has no last
+// triangle): kWeightTag | uint8(wexp); no real triangle index has these bits.
+constexpr uint32_t kWeightTag = 0xFFFFFE00u;
 
 struct LearnedSmem {
     mlp::Weights w;
-    __nv_bfloat16 xs[8 * 32 * mlp::kIn];
+    __nv_bfloat16 xs[8 * 32 * mlp::kIn];   // one 32 x 16 feature tile per warp
 };
+// The learned-mode kernels' network image and feature tiles (only the
+// kernels that call birth_logit hold it).
+__shared__ __align__(16) LearnedSmem g_lsm;
 
-// Per-electron state of the sample and learned modes, parked alongside the
-// electron on the cascade stack.
+// Network logit of this lane's newborn secondary (valid where cand): the
+// warp's candidates (ballot m) are packed into the first rows of the warp's
+// feature tile and one m-tile (up to 16 candidates) or two go through the
+// tensor cores.  Called by the whole warp.  Not inlined, so the network's
+// register demand does not raise the transport loop's.
+__device__ __noinline__ float birth_logit(unsigned m, bool cand, const float4* tri, const dev::SurfaceMap S, float px,
+                                          float py, float pz, float dx, float dy, float dz, float E, int mat) {
+    const int lane = threadIdx.x & 31;
+    const int rank = __popc(m & ((1u << lane) - 1u));
+    __nv_bfloat16* xs = g_lsm.xs + (threadIdx.x >> 5) * 32 * mlp::kIn;
+    if (cand) {
+        float f[6];
+        const dev::V3 d = dev::normalised(dev::V3{dx, dy, dz});
+        dev::electron_features(tri, S, px, py, pz, d.x, d.y, d.z, logf(E), mat, f);
+        __nv_bfloat16* row = xs + rank * mlp::kIn;
+#pragma unroll
+        for (int k = 0; k < mlp::kIn; ++k) row[k] = __float2bfloat16_rn(k < 6 ? f[k] : 0.0f);
+    }
+    __syncwarp();
+    const float logit =
+        __popc(m) <= 16 ? mlp::warp_forward_rows<1>(g_lsm.w, xs) : mlp::warp_forward_rows<2>(g_lsm.w, xs);
+    const float mine = __shfl_sync(0xffffffffu, logit, rank);
+    __syncwarp();
+    return mine;
+}
+
+// Per-electron state of the sample mode, parked alongside the electron.
 struct Extra {
-    float w;          // statistical weight (learned mode)
-    int rec;          // sample record slot, -1 none (sample mode)
-    uint32_t flags;   // bit 0: sub-cascade produced a detected SE; bit 1: already split
+    int rec;          // sample record slot, -1 none
+    uint32_t flags;   // bit 0: sub-cascade produced a detected SE
+    uint32_t c0;      // the thread's step count when the record was taken
 };
 
 // Parked ancestors of a thread's cascade, in global memory laid out per
-// thread (kLocalStack entries of three float4: (pos, E), (dir, material),
+// thread (stack_depth entries of three float4: (pos, E), (dir, material),
 // (uid, step, last triangle)).  A local-memory array interleaves threads word
 // by word, so lanes parked at different depths scatter each of an entry's 13
 // words into its own sector; here an entry is 48 contiguous bytes (two
 // sectors, three 16-byte accesses).  The tag is not stored: every electron of
-// a thread's cascade carries its primary's tag.  base == nullptr: use the
-// local array instead (callers without a stack buffer).
+// a thread's cascade carries its primary's tag.  With kW (learned mode) the
+// material word also carries the weight exponent in its upper 16 bits (the
+// material index fits the lower 16).  base == nullptr: use the local array
+// instead (callers without a stack buffer).
 struct ParkedStack {
     float4* base;
-    __device__ __forceinline__ void put(int i, const dev::Electron& e, dev::Electron* local) const {
+    template <bool kW>
+    __device__ __forceinline__ void put(int i, const dev::Electron& e, dev::Electron* local, int wexp) const {
+        const int mw = kW ? int((uint32_t(e.mat) & 0xFFFFu) | (uint32_t(wexp) << 16)) : e.mat;
         if (base) {
             float4* p = base + 3 * i;
             p[0] = make_float4(e.px, e.py, e.pz, e.E);
-            p[1] = make_float4(e.dx, e.dy, e.dz, __int_as_float(e.mat));
+            p[1] = make_float4(e.dx, e.dy, e.dz, __int_as_float(mw));
             p[2] = make_float4(__uint_as_float(uint32_t(e.uid)), __uint_as_float(uint32_t(e.uid >> 32)),
                                __uint_as_float(e.step), __int_as_float(e.last_tri));
         } else {
             local[i] = e;
+            local[i].mat = mw;
         }
     }
-    __device__ __forceinline__ void get(int i, dev::Electron& e, const dev::Electron* local) const {
+    template <bool kW>
+    __device__ __forceinline__ void get(int i, dev::Electron& e, const dev::Electron* local, int& wexp) const {
+        int mw;
         if (base) {
             const float4* p = base + 3 * i;
             const float4 a = p[0], b = p[1], c = p[2];
@@ -110,12 +152,19 @@ struct ParkedStack {
             e.dx = b.x;
             e.dy = b.y;
             e.dz = b.z;
-            e.mat = __float_as_int(b.w);
+            mw = __float_as_int(b.w);
             e.uid = uint64_t(__float_as_uint(c.x)) | (uint64_t(__float_as_uint(c.y)) << 32);
             e.step = __float_as_uint(c.z);
             e.last_tri = __float_as_int(c.w);
         } else {
             e = local[i];
+            mw = e.mat;
+        }
+        if constexpr (kW) {
+            e.mat = int(int16_t(mw & 0xFFFF));
+            wexp = mw >> 16;
+        } else {
+            e.mat = mw;
         }
     }
 };
@@ -127,20 +176,58 @@ __device__ __forceinline__ uint32_t mix32(uint64_t x) {
     return uint32_t(x);
 }
 
-// MinBlocks: resident blocks per SM the register allocation must allow --
-// 256-thread blocks for 2 (128 registers), 3 (80) and 4 (64); 128-thread
-// blocks for 7 (72 registers, 28 warps); the host picks the variant.
-// Mode: kModePlain (analogue transport), kModeSample (plain transport that
-// also records one (features, label) training sample per sampled electron)
-// or kModeLearned (weighted roulette / splitting with the network as the
-// importance function; the warp stays converged for the tensor-core
-// inference, so lanes without work idle until the whole warp is done), or
-// kModeDeposit (plain transport that also appends an energy-deposit record
-// per energy-changing scattering event).
 // Philox block of a secondary's step 0 that decides its roulette at birth
 // (the transport's own draws use blocks 0-2 and 3 + 64 at most).
 constexpr uint32_t kBirthBlock = 0x7FFFFFFFu;
 
+// Birth decision of the learned mode for a newborn secondary of weight
+// 2^wexp and importance p (the network's escape probability): returns the
+// change of its weight exponent -- k > 0 for Russian roulette with survival
+// 2^-k (the survivor's weight is 2^(wexp + k)), -1 to split it in two halves,
+// 0 to keep it as it is.
+//
+// Weight window (no cost table): the target weight of importance p is
+// rr_threshold / p below rr_threshold (rounded to a power of two, at most
+// 2^max_k) and 1 above it; a newborn lighter than its target plays roulette
+// up to it, so a lineage is not rouletted twice for the same importance.
+// Above split_threshold a newborn of weight >= 1 splits in two.
+//
+// Cost-aware (cost table set): minimising variance x cost of the tally, a
+// particle of weight w whose sub-cascade scores with probability p at mean
+// cost c should survive with q = w sqrt(p K / c), K = cost / variance per
+// primary of the analogue run; q is rounded to a power of two (roulette
+// below 1, at least 2^-max_k; a split in two from sqrt(2) up).
+__device__ __forceinline__ int birth_decision(const TransportArgs& a, float p, int wexp, float E, int mat) {
+    const float pc = fmaxf(p, 1e-30f);
+    if (a.cost_bins > 0) {
+        const int m = mat < 0 ? 0 : (mat >= a.cost_materials ? a.cost_materials - 1 : mat);
+        int b = int(floorf((__logf(E) - a.cost_log_e_min) * a.cost_inv_width));
+        b = b < 0 ? 0 : (b >= a.cost_bins ? a.cost_bins - 1 : b);
+        const float c = fmaxf(__ldg(a.cost_table + m * a.cost_bins + b), 1.0f);
+        const float l2q = float(wexp) + 0.5f * __log2f(pc * a.value_per_cost / c);
+        const int k = -int(rintf(l2q));
+        if (k >= 1) return k > a.max_roulette_exp ? a.max_roulette_exp : k;
+        return k <= -1 ? -1 : 0;
+    }
+    if (p > a.split_threshold) return wexp >= 0 ? -1 : 0;
+    if (!(p < a.rr_threshold)) return 0;
+    int kt = int(rintf(__log2f(a.rr_threshold / pc)));
+    kt = kt < 0 ? 0 : (kt > a.max_roulette_exp ? a.max_roulette_exp : kt);
+    return kt > wexp ? kt - wexp : 0;
+}
+
+// MinBlocks: resident blocks per SM the register allocation must allow --
+// 256-thread blocks for 2 (128 registers), 3 (80) and 4 (64); 128-thread
+// blocks for 7 (72 registers, 28 warps); the host picks the variant.
+// Mode: kModePlain (analogue transport), kModeSample (plain transport that
+// also records one (features, label, cost) training sample for about one in
+// sixteen newborn secondaries), kModeLearned (plain transport of weighted
+// electrons: every newborn secondary is scored at birth by the network,
+// batched per warp on the tensor cores, and plays Russian roulette or splits
+// on that importance; a warp stays in the loop until all its lanes are done,
+// so the tensor-core call always has the whole warp), or kModeDeposit (plain
+// transport that also appends an energy-deposit record per energy-changing
+// scattering event).
 template <int MinBlocks, int Mode, bool Penn>
 __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transport_kernel(const dev::Physics P, const TransportArgs a) {
     // Leaf cache: 13 words per thread in dynamic shared memory sized by the
@@ -151,11 +238,16 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
     const dev::LeafCache cache{leaf_cache + threadIdx.x, int(blockDim.x)};
     cache.f(0) = 0.0f;   // location 0: empty
     cache.f(1) = 0.0f;
-    constexpr bool kExtra = (Mode != kModePlain);
-    // network weights and one 32 x 16 feature tile per warp (learned mode only)
-    __shared__ __align__(16) typename std::conditional<Mode == kModeLearned, LearnedSmem, char>::type lsm;
-    if constexpr (Mode == kModeLearned) {
-        mlp::load_weights(lsm.w, a.mlp_params);
+    constexpr bool kExtra = (Mode == kModeSample);
+    constexpr bool kW = (Mode == kModeLearned);
+    bool use_net = false, use_rule = false;
+    int rule_k = 0;
+    if constexpr (kW) {
+        // the fixed (distance, energy) rule at birth, when set, replaces the network
+        use_rule = a.birth_survival > 0.0f && a.birth_survival < 1.0f;
+        rule_k = use_rule ? max(1, min(a.max_roulette_exp, int(rintf(-__log2f(a.birth_survival))))) : 0;
+        use_net = !use_rule && a.mlp_params != nullptr;
+        if (use_net) mlp::load_weights(g_lsm.w, a.mlp_params);
         __syncthreads();
     }
     const uint32_t n_in = min(*a.n_in, a.in_capacity);
@@ -164,12 +256,13 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
     // parent is parked here and the secondary is simulated at once, so the
     // stack only ever holds the current electron's ancestors.
     dev::Electron stack[kLocalStack];
-    const ParkedStack ps{a.stack_mem ? a.stack_mem + (size_t(blockIdx.x) * blockDim.x + threadIdx.x) * 3 * kLocalStack
+    const ParkedStack ps{a.stack_mem ? a.stack_mem + (size_t(blockIdx.x) * blockDim.x + threadIdx.x) * 3 * a.stack_depth
                                      : nullptr};
-    Extra ex{1.0f, -1, 0u};
-    Extra exs[kExtra ? kLocalStack : 1];
+    const int depth = a.stack_mem ? a.stack_depth : kLocalStack;
+    Extra ex{-1, 0u, 0u};
+    Extra exs[kExtra ? kMaxStack : 1];
+    int wexp = 0;   // learned mode: the current electron's weight is 2^wexp
     int sp = 0;
-    int warp_iter = 0;
     bool alive = false, drained = false;
     uint32_t probe = 0;   // ranges this thread has found used up (range_cursor)
     uint32_t carry_hit = 0;
@@ -182,10 +275,27 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
     // record buffer, taken kDepositChunk records at a time with one atomic.
     unsigned long long dep_pos = 0, dep_end = 0;
     bool dep_full = false;
+    // Hand an electron to the next generation's queue (warp-aggregated push
+    // over the lanes that push together).
+    auto push_next = [&](const dev::Electron& x, int x_wexp) {
+        cg::coalesced_group g = cg::coalesced_threads();
+        uint32_t base = 0;
+        if (g.thread_rank() == 0) base = atomicAdd(a.out_tail, g.size());
+        base = g.shfl(base, 0);
+        const uint32_t slot = base + g.thread_rank();
+        if (slot < a.out_capacity) {
+            store_electron(a.out, slot, x);
+            if constexpr (kW) {
+                if (x_wexp != 0) a.out.c[slot].w = kWeightTag | (uint32_t(x_wexp) & 0xFFu);
+            }
+        } else {
+            atomicAdd(a.counters + kCntOverflow, 1ull);
+        }
+    };
     for (;;) {
         if (!alive && !drained) {
             if (sp > 0) {
-                ps.get(--sp, e, stack);
+                ps.get<kW>(--sp, e, stack, wexp);
                 if constexpr (kExtra) {
                     ex = exs[sp];
                     ex.flags |= carry_hit;
@@ -230,9 +340,14 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                     drained = true;
                 } else {
                     load_electron(a.in, idx, e);
+                    if constexpr (kW) {
+                        wexp = 0;
+                        if ((uint32_t(e.last_tri) & 0xFFFFFF00u) == kWeightTag) {
+                            wexp = int(int8_t(uint32_t(e.last_tri) & 0xFFu));
+                            e.last_tri = -1;
+                        }
+                    }
                     if constexpr (kExtra) {
-                        const uint32_t wbits = a.in.c[idx].w;
-                        ex.w = (Mode == kModeLearned && wbits != 0xFFFFFFFFu) ? __uint_as_float(wbits) : 1.0f;
                         ex.rec = -1;
                         ex.flags = 0;
                         carry_hit = 0;
@@ -242,64 +357,16 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                 }
             }
         }
-        if constexpr (Mode == kModeLearned) {
+        if constexpr (kW) {
+            // the whole warp stays in the loop until all its lanes are done
             if (__all_sync(0xffffffffu, !alive)) break;
-            // Every rr_period iterations of the (converged) warp, all its
-            // electrons in a material are scored together on the tensor cores.
-            if (++warp_iter == a.rr_period) {
-                warp_iter = 0;
-                const bool want = alive && e.mat >= 0;
-                if (__any_sync(0xffffffffu, want)) {
-                    ++c_inf;
-                    __nv_bfloat16* xs = lsm.xs + (threadIdx.x >> 5) * 32 * mlp::kIn;
-                    float f[6] = {0, 0, 0, 0, 0, 0};
-                    if (want) {
-                        const dev::V3 d = dev::normalised(dev::V3{e.dx, e.dy, e.dz});
-                        dev::electron_features(P.geo, a.smap, e.px, e.py, e.pz, d.x, d.y, d.z, logf(e.E), e.mat, f);
-                    }
-                    const int lane = threadIdx.x & 31;
-#pragma unroll
-                    for (int k = 0; k < mlp::kIn; ++k)
-                        xs[lane * mlp::kIn + k] = __float2bfloat16_rn(k < 6 ? f[k] : 0.0f);
-                    __syncwarp();
-                    const float logit = mlp::warp_forward(lsm.w, xs);
-                    __syncwarp();
-                    if (want) {
-                        // Weight window on the importance p: target weight
-                        // min(rr_threshold / p, w_max) below the threshold, 1
-                        // above it.  Lighter than half the target: Russian
-                        // roulette up to the target; heavier than twice it
-                        // and important (p > split_threshold): split in two.
-                        const float pr = mlp::sigmoid(logit);
-                        const float target =
-                            pr < a.rr_threshold ? fminf(a.rr_threshold / fmaxf(pr, 1e-12f), kMaxWeight) : 1.0f;
-                        if (ex.w < 0.5f * target) {
-                            const float q = ex.w / target;
-                            const float u = dev::u01(dev::draw(P.seed, e, 2).x);
-                            if (u < q) {
-                                ex.w = target;
-                            } else {
-                                alive = false;
-                                ++c_kill;
-                            }
-                        } else if (pr > a.split_threshold && ex.w > 2.0f * target && sp < kLocalStack) {
-                            ex.w *= 0.5f;
-                            dev::Electron twin = e;
-                            twin.uid = dev::secondary_uid(e.uid ^ 0x5DEECE66Dull, e.step);
-                            ps.put(sp, twin, stack);
-                            exs[sp] = ex;
-                            ++sp;
-                            ++c_split;
-                        }
-                    }
-                }
-            }
-            if (!alive) continue;
         } else {
             if (!alive) break;
         }
         if constexpr (Mode == kModeSample) {
-            if (ex.rec < 0 && e.mat >= 0 && (mix32(e.uid ^ (uint64_t(e.step) << 40)) & 15u) == 0) {
+            // one in sixteen electrons is recorded at its birth (step 0) in a
+            // material: features now; label and sub-cascade cost when it ends
+            if (ex.rec < 0 && e.step == 0 && e.mat >= 0 && (mix32(e.uid) & 15u) == 0) {
                 const uint32_t slot = atomicAdd(a.sample_count, 1u);
                 if (slot < a.sample_capacity) {
                     float f[6];
@@ -308,16 +375,52 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
 #pragma unroll
                     for (int k = 0; k < 6; ++k) a.sample_feat[size_t(slot) * 6 + k] = f[k];
                     ex.rec = int(slot);
+                    ex.c0 = c_steps;
                     ++c_smp;
                 }
             }
         }
-        int ev;
-        bool has_se;
+        int ev = dev::kEvNone;
+        bool has_se = false;
         dev::Electron se;
+        int st = dev::kAlive;
         [[maybe_unused]] const float E_before = e.E;
-        int st = dev::step<Penn>(P, e, &ev, &se, &has_se, cache);
-        ++c_steps;
+        if (!kW || alive) {
+            st = dev::step<Penn>(P, e, &ev, &se, &has_se, cache);
+            ++c_steps;
+        }
+        // Learned mode: birth decision for every newborn secondary of the warp
+        // (k > 0 roulette at survival 2^-k, -1 split, 0 keep; drop = lost the
+        // roulette).  The network scores the warp's candidates together: they
+        // are packed into the first rows of the warp's feature tile and one
+        // (up to 16 candidates) or two m-tiles go through the tensor cores.
+        int bk = 0;
+        bool drop = false;
+        if constexpr (kW) {
+            const bool cand = has_se && !dev::ends_at_init(P, se);
+            if (use_rule) {
+                if (cand && se.E < a.birth_max_energy &&
+                    dev::surface_distance(P.geo, a.smap, se.px, se.py, se.pz) >= a.birth_min_distance)
+                    bk = rule_k;
+            } else if (use_net) {
+                const unsigned m = __ballot_sync(0xffffffffu, cand);
+                if (m) {
+                    const float logit = birth_logit(m, cand, P.geo.tri, a.smap, se.px, se.py, se.pz, se.dx, se.dy,
+                                                    se.dz, se.E, se.mat);
+                    if ((threadIdx.x & 31) == 0) ++c_inf;
+                    if (cand) bk = birth_decision(a, mlp::sigmoid(logit), wexp, se.E, se.mat);
+                }
+            }
+            if (bk > 0) {
+                // Russian roulette: survive with probability 2^-bk at weight
+                // 2^(wexp + bk); the draw is the secondary's own birth block
+                if (wexp + bk > kMaxWeightExp) bk = kMaxWeightExp - wexp;
+                if (bk > 0 && !(ldexpf(dev::u01(dev::draw(P.seed, se, kBirthBlock).x), bk) < 1.0f)) drop = true;
+            } else if (bk < 0 && wexp <= kMinWeightExp) {
+                bk = 0;   // the lineage is already split as far as it may be
+            }
+            if (!alive) continue;
+        }
         if constexpr (Mode == kModeDeposit) {
             // energydeposit_cpu_driver::simulate_to_end (drivers/cpu/
             // energydeposit_cpu_driver.h:74-96): scattering events only, and
@@ -353,20 +456,7 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
         if (has_se) {
             // an inelastic step never ends its electron: st == kAlive here
             ++c_se;
-            // learned mode: roulette at the secondary's birth (its own draw
-            // block kBirthBlock of step 0, used by nothing else)
-            float birth_w = 1.0f;
-            bool birth_dropped = false;
-            if constexpr (Mode == kModeLearned) {
-                if (a.birth_survival > 0.0f && a.birth_survival < 1.0f && se.E < a.birth_max_energy &&
-                    dev::surface_distance(P.geo, a.smap, se.px, se.py, se.pz) >= a.birth_min_distance) {
-                    if (dev::u01(dev::draw(P.seed, se, kBirthBlock).x) < a.birth_survival)
-                        birth_w = 1.0f / a.birth_survival;
-                    else
-                        birth_dropped = true;
-                }
-            }
-            if (birth_dropped) {
+            if (drop) {
                 ++c_kill;   // the secondary's sub-cascade is not simulated
             } else if (dev::ends_at_init(P, se)) {
                 // The secondary's first step would only terminate it (about a
@@ -374,30 +464,39 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                 // here instead of parking the parent for it.
                 ++c_steps;
                 ++c_term;
-            } else if (sp < kLocalStack) {
-                ps.put(sp, e, stack);
-                if constexpr (kExtra) exs[sp] = ex;
-                ++sp;
-                e = se;
-                if constexpr (kExtra) {
-                    ex.rec = -1;
-                    ex.flags = 0;   // the secondary inherits the weight only
-                    ex.w *= birth_w;
-                }
-                continue;
             } else {
-                // Deep cascade: hand the secondary to the next generation.
-                cg::coalesced_group g = cg::coalesced_threads();
-                uint32_t base = 0;
-                if (g.thread_rank() == 0) base = atomicAdd(a.out_tail, g.size());
-                base = g.shfl(base, 0);
-                const uint32_t slot = base + g.thread_rank();
-                if (slot < a.out_capacity) {
-                    store_electron(a.out, slot, se);
-                    if constexpr (Mode == kModeLearned) a.out.c[slot].w = __float_as_uint(ex.w * birth_w);
-                } else {
-                    atomicAdd(a.counters + kCntOverflow, 1ull);
+                // the newborn's weight exponent: roulette survivors gain bk,
+                // both halves of a split lose one
+                const int se_wexp = wexp + (bk < 0 ? -1 : bk);
+                if (bk < 0) {
+                    // split: the twin takes its own random streams
+                    dev::Electron twin = se;
+                    twin.uid = dev::secondary_uid(se.uid ^ 0x5DEECE66Dull, 0u);
+                    ++c_split;
+                    if (sp + 1 < depth) {
+                        ps.put<kW>(sp, e, stack, wexp);
+                        ps.put<kW>(sp + 1, twin, stack, se_wexp);
+                        sp += 2;
+                        e = se;
+                        wexp = se_wexp;
+                        continue;
+                    }
+                    push_next(twin, se_wexp);
                 }
+                if (sp < depth) {
+                    ps.put<kW>(sp, e, stack, wexp);
+                    if constexpr (kExtra) exs[sp] = ex;
+                    ++sp;
+                    e = se;
+                    wexp = se_wexp;
+                    if constexpr (kExtra) {
+                        ex.rec = -1;
+                        ex.flags = 0;
+                    }
+                    continue;
+                }
+                // Deep cascade: hand the secondary to the next generation.
+                push_next(se, se_wexp);
             }
         }
         if (st == dev::kAlive) {
@@ -417,9 +516,10 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
             hit = is_se ? 1u : 0u;
             c_dse += is_se;
             c_dbse += !is_se;
+            [[maybe_unused]] const float wt = kW ? ldexpf(1.0f, wexp) : 1.0f;
             if (e.tag < a.n_tags) {
                 atomicAdd(is_se ? a.se_count + e.tag : a.bse_count + e.tag, 1u);
-                if constexpr (Mode == kModeLearned) atomicAdd(is_se ? a.se_w + e.tag : a.bse_w + e.tag, ex.w);
+                if constexpr (kW) atomicAdd(is_se ? a.se_w + e.tag : a.bse_w + e.tag, wt);
             }
             if (a.hist) {
                 int bin = dev::floor_to_int(e.E * a.inv_bin_width);
@@ -430,11 +530,7 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                 // per-pixel exit spectrum; energies past the last bin are not binned
                 const uint32_t px = a.pixel_of_tag[e.tag];
                 const int bin = dev::floor_to_int(e.E * a.pix_inv_width);
-                if (px < a.n_pixels && bin >= 0 && bin < a.pix_bins) {
-                    float wt = 1.0f;
-                    if constexpr (Mode == kModeLearned) wt = ex.w;
-                    atomicAdd(a.pix_spec + size_t(px) * a.pix_bins + bin, wt);
-                }
+                if (px < a.n_pixels && bin >= 0 && bin < a.pix_bins) atomicAdd(a.pix_spec + size_t(px) * a.pix_bins + bin, wt);
             }
             if (a.rec_a) {
                 const uint32_t slot = atomicAdd(a.rec_count, 1u);
@@ -448,7 +544,10 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
         }
         if constexpr (Mode == kModeSample) {
             const uint32_t sub = (ex.flags | hit) & 1u;
-            if (ex.rec >= 0) a.sample_label[ex.rec] = float(sub);
+            if (ex.rec >= 0) {
+                a.sample_label[ex.rec] = float(sub);
+                if (a.sample_cost) a.sample_cost[ex.rec] = float(c_steps - ex.c0);
+            }
             carry_hit = sub;
         }
     }

@@ -489,7 +489,7 @@ def test_learned_pixel_yields_are_weighted(inputs):
     ctx = nb.setup(inputs["cube"], [inputs["si"]], device=0, seed=15)
     ctx.build_surface_map([-50, -50, -40], [50, 50, 20], 1.0, 20.0)
     ctx.mlp_set_params(nb.mlp_init_params(0))
-    ctx.set_mode("learned", rr_threshold=0.0, split_threshold=2.0, rr_period=4)
+    ctx.set_mode("learned", rr_threshold=0.0, split_threshold=2.0)
     _run_gpu(ctx, recs)
     w = ctx.pixel_yields(pix, 64)
     se, bse = ctx.tag_counts(0, len(recs))

@@ -162,10 +162,15 @@ def test_sample_mode_does_not_change_transport(inputs):
     ss, se_s, bse_s, _, _ = _run(b, recs, "sample")
     assert np.array_equal(se_p, se_s) and np.array_equal(bse_p, bse_s)
     assert sp["steps"] == ss["steps"]
-    f, y = b.get_samples(1 << 20)
+    f, y, c = b.get_samples(1 << 20, with_cost=True)
     assert len(f) == ss["samples"] > 1000
     assert set(np.unique(y)) <= {0.0, 1.0}
     assert 0.001 < y.mean() < 0.5
+    # recorded at birth: a whole number of steps, at least the newborn's own
+    # first one, and never more than the run made
+    assert np.all(c >= 1) and np.all(c == np.round(c)) and c.max() < ss["steps"]
+    # a sub-cascade that produced a detected SE took at least one boundary step
+    assert c[y == 1].min() >= 2
     b.close()
 
 
@@ -177,31 +182,46 @@ def test_learned_mode_disabled_equals_plain(inputs):
     b = nb.setup(inputs["grating_small"], [inputs["si"]], device=0, seed=55)
     b.build_surface_map([-100, -100, -40], [100, 100, 70], 1.0, 20.0)
     b.mlp_set_params(M.init_params(0))
-    s, se_l, bse_l, sw, bw = _run(b, recs, "learned", rr_threshold=0.0, split_threshold=2.0, rr_period=4)
+    s, se_l, bse_l, sw, bw = _run(b, recs, "learned", rr_threshold=0.0, split_threshold=2.0)
     assert s["inferences"] > 0 and s["roulette_killed"] == 0 and s["splits"] == 0
     assert np.array_equal(se_p, se_l) and np.array_equal(bse_p, bse_l)
     assert np.array_equal(sw, se_l.astype(np.float32)) and np.array_equal(bw, bse_l.astype(np.float32))
     b.close()
 
 
-def test_learned_roulette_unbiased(inputs):
-    """Train on sample-mode records, then compare weighted yields with plain."""
+@pytest.mark.parametrize("policy", ["window", "cost"])
+def test_learned_roulette_unbiased(inputs, policy):
+    """Train on sample-mode records (recorded at birth), then compare the
+    weighted yields of the learned mode with plain: the weight window on the
+    network's importance, and the cost-aware survival w sqrt(p K / c) with
+    the cost table fitted to the records' sub-cascade costs.  Both play
+    roulette at birth and stay within 3 sigma of the analogue yields."""
     tris = inputs["grating_small"]
     train_recs = g.scan_beam(32, 32, 8, 500.0, origin=(-16.0, -16.0), seed=11)
     c = nb.setup(tris, [inputs["si"]], device=0, seed=66)
     c.build_surface_map([-100, -100, -40], [100, 100, 70], 1.0, 20.0)
     c.set_sample_capacity(1 << 22)
     _run(c, train_recs, "sample")
-    f, y = c.get_samples(1 << 22)
+    f, y, cost = c.get_samples(1 << 22, with_cost=True)
     c.mlp_set_params(M.init_params(1))
     c.mlp_train(f, y, epochs=4, batch=8192, lr=1e-3, seed=2)
     recs = g.scan_beam(16, 16, 40, 500.0, origin=(-8.0, -8.0), seed=12)
     sp, se_p, bse_p, _, _ = _run(c, recs, "plain")
-    # A threshold well above the positive rate, so that the roulette acts even
-    # where the briefly trained network is close to constant.
-    th = max(0.1, 3.0 * float(y.mean()))
-    sl, se_l, bse_l, sw, bw = _run(c, recs, "learned", rr_threshold=th, split_threshold=0.5, rr_period=8)
-    assert sl["roulette_killed"] > 0
+    if policy == "cost":
+        table, lo, hi = nb.fit_cost_table(f, cost)
+        assert table.shape == (1, 32) and np.all(table >= 1)
+        k = sp["steps"] / len(recs) / se_p.astype(float).var()
+        # a value per cost well below the analogue one, so that the roulette
+        # acts even where the briefly trained network is close to constant
+        c.set_learned_cost(table, lo, hi, 0.05 * k)
+        sl, se_l, bse_l, sw, bw = _run(c, recs, "learned")
+    else:
+        # twice the median importance the network gives the training records:
+        # about half the newborns are lighter than their target weight
+        th = 2.0 * float(np.median(c.mlp_predict(f)))
+        sl, se_l, bse_l, sw, bw = _run(c, recs, "learned", rr_threshold=th, split_threshold=0.99)
+    assert sl["roulette_killed"] > 0 and sl["inferences"] > 0
+    assert sl["steps"] < sp["steps"]
     for plain, learned in ((se_p.astype(float), sw.astype(float)), (bse_p.astype(float), bw.astype(float))):
         z = (learned.mean() - plain.mean()) / np.sqrt(learned.var() / len(learned) + plain.var() / len(plain))
         assert abs(z) < 3, z
@@ -209,10 +229,11 @@ def test_learned_roulette_unbiased(inputs):
 
 
 def test_birth_roulette_unbiased(inputs):
-    """Roulette at a secondary's birth (1 keV into the cube: secondaries born
-    more than 5 nm from the surface below 100 eV survive with probability
-    1/4 at weight 4) drops many sub-cascades, makes fewer steps, and keeps
-    the weighted SE and BSE yields within 4 sigma of the analogue run."""
+    """The fixed rule at a secondary's birth (1 keV into the cube:
+    secondaries born more than 5 nm from the surface below 100 eV survive
+    with probability 1/4 at weight 4) drops many sub-cascades, makes fewer
+    steps, and keeps the weighted SE and BSE yields within 3 sigma of the
+    analogue run."""
     recs = g.point_beam(20000, 1000.0, pos=(0.0, 0.0, 1.0))
     a = nb.setup(inputs["cube"], [inputs["si"]], device=0, seed=88)
     sp, se_p, bse_p, _, _ = _run(a, recs, "plain")
@@ -221,10 +242,35 @@ def test_birth_roulette_unbiased(inputs):
     b.build_surface_map([-60, -60, -80], [60, 60, 5], 1.0, 10.0)
     b.mlp_set_params(M.init_params(0))
     b.set_birth_roulette(5.0, 100.0, 0.25)
-    s, _, _, sw, bw = _run(b, recs, "learned", rr_threshold=0.0, split_threshold=2.0, rr_period=1 << 30)
+    s, _, _, sw, bw = _run(b, recs, "learned", rr_threshold=0.0, split_threshold=2.0)
     b.close()
     assert s["roulette_killed"] > 1000 and s["inferences"] == 0
     assert s["steps"] < 0.9 * sp["steps"]
+    # weights are 1 or 4 per detection: sums of those
+    assert np.all(np.isin(np.unique(np.mod(sw, 1.0)), [0.0]))
     for w, c in ((sw.astype(np.float64), se_p.astype(np.float64)), (bw.astype(np.float64), bse_p.astype(np.float64))):
         z = (w.mean() - c.mean()) / np.sqrt(w.var() / len(w) + c.var() / len(c))
-        assert abs(z) < 4, z
+        assert abs(z) < 3, z
+
+
+def test_split_at_birth_unbiased(inputs):
+    """Splitting at birth: with split_threshold near 0 every newborn
+    secondary splits in two halves (down to weight 1/16 along a lineage), so
+    the run makes more steps than the analogue one, the per-tag weights are
+    multiples of 1/16, and the weighted SE and BSE yields stay within 3 sigma
+    of the analogue run."""
+    recs = g.scan_beam(16, 16, 8, 500.0, origin=(-8.0, -8.0), seed=13)
+    a = nb.setup(inputs["grating_small"], [inputs["si"]], device=0, seed=57)
+    sp, se_p, bse_p, _, _ = _run(a, recs, "plain")
+    a.close()
+    b = nb.setup(inputs["grating_small"], [inputs["si"]], device=0, seed=58)
+    b.build_surface_map([-100, -100, -40], [100, 100, 70], 1.0, 20.0)
+    b.mlp_set_params(M.init_params(0))
+    s, _, _, sw, bw = _run(b, recs, "learned", rr_threshold=0.0, split_threshold=1e-6)
+    b.close()
+    assert s["splits"] > 1000 and s["roulette_killed"] == 0
+    assert s["steps"] > 1.5 * sp["steps"]
+    assert np.all(np.mod(sw * 16.0, 1.0) == 0) and np.all(np.mod(bw * 16.0, 1.0) == 0)
+    for w, c in ((sw.astype(np.float64), se_p.astype(np.float64)), (bw.astype(np.float64), bse_p.astype(np.float64))):
+        z = (w.mean() - c.mean()) / np.sqrt(w.var() / len(w) + c.var() / len(c))
+        assert abs(z) < 3, z
