@@ -387,6 +387,10 @@ def run_reference(args):
     return 0
 
 
+# Grid of the network's importance table (scaled log energy x distance to
+# the surface x cosine toward its normal).
+IMPORTANCE_GRID = (48, 32, 16)
+
 # Training records per scan of the learned leg (about 4 M in all, the
 # records of the grating and the rough-slab scans for those two workloads).
 TRAIN_RECORDS = 2_000_000
@@ -471,6 +475,8 @@ def learned_fom(args, tris, mats, local, rank, prim, tags, plain, tmp, tune_samp
             value_per_cost = plain["steps_per_primary"] / plain["var_se"]
             ctx.set_learned_cost(table, lo, hi, value_per_cost)
             cost_info = {"value_per_cost": value_per_cost, "bins": int(table.shape[1])}
+        if args.learned_eval == "table" and not args.birth_rr:
+            ctx.set_importance_table(*IMPORTANCE_GRID)
         # launch shape, stack depth and chunk tuned in learned mode on the
         # plain leg's tuning sample (unless --learned-variant fixes the shape)
         tuned = ctx.autotune(prim[tune_sample], tags[tune_sample]) if not args.learned_variant else ctx.tuning()
@@ -483,7 +489,8 @@ def learned_fom(args, tris, mats, local, rank, prim, tags, plain, tmp, tune_samp
         # off (the network still scores every newborn)
         ctx.set_birth_roulette(0.0, 0.0, 0.0)
         ctx.set_learned_cost(None, 0.0, 1.0, 1.0)
-        ctx.set_mode("learned", rr_threshold=0.0, split_threshold=2.0, max_roulette_exp=args.max_roulette_exp)
+        # decisions off, network (or table) still consulted for every newborn
+        ctx.set_mode("learned", rr_threshold=1e-30, split_threshold=0.99999, max_roulette_exp=args.max_roulette_exp)
         ctx.reset_tallies()
         ctx.push(prim, tags)
         ctx.run()
@@ -500,7 +507,10 @@ def learned_fom(args, tris, mats, local, rank, prim, tags, plain, tmp, tune_samp
                 "se_yield": m_se, "bse_yield": m_bse, "z_vs_plain": z_se, "z_bse_vs_plain": z_bse,
                 "run_ms": s["last_run_ms"], "var_ratio": v_se / plain["var_se"],
                 "policy": ("fixed rule at birth " + args.birth_rr) if args.birth_rr else
-                          ("network at birth, cost-aware survival" if cost_info else "network at birth, weight window"),
+                          ("network at birth (%s), %s" % (
+                              "importance table %dx%dx%d" % IMPORTANCE_GRID if args.learned_eval == "table"
+                              else "tensor cores per newborn",
+                              "cost-aware survival" if cost_info else "weight window")),
                 "cost_aware": cost_info,
                 "decisions_off": {"run_ms": s_off["last_run_ms"], "steps": s_off["steps"],
                                   "ns_per_step": 1e6 * s_off["last_run_ms"] / max(s_off["steps"], 1),
@@ -549,6 +559,9 @@ def main():
                     help="learned leg: importance above which a newborn secondary splits in two")
     ap.add_argument("--max-roulette-exp", type=int, default=6,
                     help="learned leg: lowest roulette survival is 2^-this")
+    ap.add_argument("--learned-eval", default="table", choices=["table", "fused"],
+                    help="learned leg: network tabulated once over its inputs (table) or evaluated on the tensor "
+                         "cores for every newborn (fused)")
     ap.add_argument("--learned-policy", default="window", choices=["window", "cost"],
                     help="learned leg: weight window on the network's importance (rr/split thresholds), or "
                          "cost-aware survival w sqrt(p K / c)")

@@ -375,6 +375,17 @@ int nbx_set_birth_roulette(nbx_ctx* ctx, float min_distance, float max_energy, f
  * count of an analogue run. */
 int nbx_set_learned_cost(nbx_ctx* ctx, const float* mean_cost, int32_t n_materials, int32_t n_bins,
                          float log_e_min, float log_e_max, float value_per_cost);
+/* Learned mode, importance table (off until set; any count 0 turns it off
+ * again): instead of running the network for every newborn, the network is
+ * evaluated once, on the tensor cores, at the centres of a grid over its
+ * inputs -- n_energy bins of the scaled log energy, n_distance of the scaled
+ * distance to the nearest surface, n_cosine of the cosine toward its normal,
+ * for every material -- and a newborn's importance is its grid cell's value.
+ * The birth decisions are then those of the network at the cell centre, and
+ * the transport needs no warp-synchronous step.  The table is rebuilt
+ * automatically when the parameters change (nbx_mlp_set_params,
+ * nbx_mlp_train). */
+int nbx_set_importance_table(nbx_ctx* ctx, int32_t n_energy, int32_t n_distance, int32_t n_cosine);
 /* Nearest-triangle map over the box [lo, hi) with the given cell size (nm);
  * surfaces farther than d_max (nm) count as "far".  Needed for the distance
  * and cosine features. */

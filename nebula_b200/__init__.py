@@ -171,6 +171,7 @@ def lib():
         "nbx_autotune": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.POINTER(Tuning)]),
         "nbx_set_tuning": (C.c_int, [_vp, C.POINTER(Tuning)]),
         "nbx_set_learned_cost": (C.c_int, [_vp, _vp, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float]),
+        "nbx_set_importance_table": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32]),
         "nbx_get_tuning": (C.c_int, [_vp, C.POINTER(Tuning)]),
         "nbx_run_noalloc": (C.c_int, [_vp, _vp, _vp, C.c_uint32, C.c_uint64, _vp, _vp, C.c_uint64,
                                       C.POINTER(C.c_uint64)]),
@@ -498,6 +499,12 @@ class Context:
             t = t[None, :]
         self._ck(self.L.nbx_set_learned_cost(self.h, _ptr(t), t.shape[0], t.shape[1], log_e_min, log_e_max,
                                              value_per_cost))
+
+    def set_importance_table(self, n_energy=48, n_distance=32, n_cosine=16):
+        """Learned mode: birth decisions from the network tabulated on a grid
+        over its inputs (see include/nbx.h); set_importance_table(0, 0, 0)
+        returns to the network evaluated for every newborn."""
+        self._ck(self.L.nbx_set_importance_table(self.h, n_energy, n_distance, n_cosine))
 
     def build_surface_map(self, lo, hi, cell=1.0, d_max=20.0):
         lo = np.ascontiguousarray(lo, np.float32)

@@ -88,6 +88,14 @@ struct TransportArgs {
     // q = 2^wexp sqrt(p * value_per_cost / c); c = cost_table[mat * cost_bins
     // + bin of log E over [cost_log_e_min, cost_log_e_min + cost_bins /
     // cost_inv_width)]
+    // learned mode, importance table (imp_table != nullptr, kModeWeighted):
+    // the network's escape probability tabulated at the centres of a grid over
+    // its inputs, imp_table[((mat * imp_ne + e) * imp_nd + d) * imp_nc + c]
+    // for the scaled log energy f0 in [0, 1) (imp_ne bins), the scaled
+    // distance f1 in [0, 1] (imp_nd bins, the last one closed) and the cosine
+    // f2 in [-1, 1] (imp_nc bins); features outside are clamped
+    const float* imp_table;
+    int imp_ne, imp_nd, imp_nc, imp_materials;
     const float* cost_table;
     int cost_bins;
     int cost_materials;
@@ -130,7 +138,11 @@ constexpr int kDepositWords = 6;
 constexpr uint32_t kDepositChunk = 32;
 constexpr uint32_t kDepositEmpty = 0xFFFFFFFFu;
 
-enum : int { kModePlain = 0, kModeSample = 1, kModeLearned = 2, kModeDeposit = 3 };
+// kModeLearned: weighted transport, the network evaluated on the tensor
+// cores for every newborn (warp-synchronous); kModeWeighted: weighted
+// transport whose birth decisions come from the network's importance table
+// or the fixed rule (no warp-synchronous step).
+enum : int { kModePlain = 0, kModeSample = 1, kModeLearned = 2, kModeDeposit = 3, kModeWeighted = 4 };
 
 // Per-thread stack of parked ancestors (depth-first cascades): the depth of
 // the local-memory array used without a stack buffer, and the largest depth

@@ -131,6 +131,12 @@ struct nbx_ctx {
     float rr_threshold = 0.05f, split_threshold = 0.5f;
     int max_roulette_exp = 6;
     float birth_min_distance = 0.0f, birth_max_energy = 0.0f, birth_survival = 0.0f;   // off
+    // importance table (nbx_set_importance_table): the network's escape
+    // probability on a grid over its inputs, rebuilt when the parameters change
+    DevBuf<float> imp_table;
+    int imp_ne = 0, imp_nd = 0, imp_nc = 0, imp_materials = 0;
+    uint64_t imp_version = ~0ull;  // mlp_version the table was built from
+    uint64_t mlp_version = 0;      // bumped by every parameter change
     DevBuf<float> cost_table;      // cost-aware survival (nbx_set_learned_cost)
     int cost_bins = 0, cost_materials = 0;
     float cost_log_e_min = 0, cost_inv_width = 0, value_per_cost = 0;
@@ -682,6 +688,54 @@ int nbx_push(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, 
     });
 }
 
+namespace {
+void mlp_upload(nbx_ctx* ctx, const float* features, const float* labels, uint64_t n);
+
+// Evaluates the network at the centres of the importance table's grid (one
+// row of features per cell, on the tensor cores) into ctx->imp_table.
+void build_importance_table(nbx_ctx* ctx) {
+    const int nm = std::max(1, ctx->n_mat), ne = ctx->imp_ne, nd = ctx->imp_nd, nc = ctx->imp_nc;
+    const uint64_t cells = uint64_t(nm) * ne * nd * nc;
+    std::vector<float> f(cells * nbx::mlp::kFeatures, 0.0f);
+    uint64_t r = 0;
+    for (int m = 0; m < nm; ++m)
+        for (int ie = 0; ie < ne; ++ie)
+            for (int id = 0; id < nd; ++id)
+                for (int ic = 0; ic < nc; ++ic, ++r) {
+                    float* x = f.data() + r * nbx::mlp::kFeatures;
+                    x[0] = (ie + 0.5f) / float(ne);
+                    x[1] = (id + 0.5f) / float(nd);
+                    x[2] = -1.0f + 2.0f * (ic + 0.5f) / float(nc);
+                    if (m < 3) x[3 + m] = 1.0f;
+                }
+    mlp_upload(ctx, f.data(), nullptr, cells);
+    ctx->imp_table.ensure(cells);
+    ck(nbx::mlp::launch_predict(ctx->mlp_params.p, ctx->mlp_feat.p, cells, ctx->imp_table.p, ctx->stream),
+       "predict kernel");
+    ck(cudaStreamSynchronize(ctx->stream), "sync");
+    ctx->imp_materials = nm;
+    ctx->imp_version = ctx->mlp_version;
+}
+}  // namespace
+
+int nbx_set_importance_table(nbx_ctx* ctx, int32_t n_energy, int32_t n_distance, int32_t n_cosine) {
+    if (!ctx || n_energy < 0 || n_distance < 0 || n_cosine < 0 || n_energy > 1024 || n_distance > 1024 ||
+        n_cosine > 1024)
+        return NBX_ERR_ARG;
+    if (n_energy == 0 || n_distance == 0 || n_cosine == 0) {
+        ctx->imp_ne = ctx->imp_nd = ctx->imp_nc = 0;
+        return NBX_OK;
+    }
+    if (!ctx->mlp_ready) return fail(ctx, NBX_ERR_STATE, "importance table without network parameters");
+    return guarded(ctx, [&] {
+        ctx->imp_ne = n_energy;
+        ctx->imp_nd = n_distance;
+        ctx->imp_nc = n_cosine;
+        build_importance_table(ctx);
+        return NBX_OK;
+    });
+}
+
 int nbx_run(nbx_ctx* ctx) {
     if (!ctx) return NBX_ERR_ARG;
     if (!ctx->have_geometry) return fail(ctx, NBX_ERR_STATE, "nbx_run before nbx_set_geometry");
@@ -761,6 +815,20 @@ int nbx_run(nbx_ctx* ctx) {
             a.birth_survival = ctx->birth_survival;
         }
         int mode = ctx->mode;
+        if (mode == nbx::kModeLearned &&
+            (ctx->imp_ne > 0 || (ctx->birth_survival > 0.0f && ctx->birth_survival < 1.0f))) {
+            // birth decisions from the importance table or the fixed rule: the
+            // weighted transport without a warp-synchronous network call
+            mode = nbx::kModeWeighted;
+            if (ctx->imp_ne > 0) {
+                if (ctx->imp_version != ctx->mlp_version) build_importance_table(ctx);
+                a.imp_table = ctx->imp_table.p;
+                a.imp_ne = ctx->imp_ne;
+                a.imp_nd = ctx->imp_nd;
+                a.imp_nc = ctx->imp_nc;
+                a.imp_materials = ctx->imp_materials;
+            }
+        }
         if (ctx->cfg.record_deposits) {
             // energy-deposit records (cpu_energydep.cpp's driver) ride on plain transport
             if (mode != nbx::kModePlain) throw ApiError(NBX_ERR_STATE, "energy deposits need the plain mode");
@@ -1514,6 +1582,7 @@ int nbx_mlp_set_params(nbx_ctx* ctx, const float* params) {
         zero(ctx, ctx->mlp_v.p, 4 * nbx::mlp::kParams, "memset");
         ctx->mlp_step = 0;
         ctx->mlp_ready = true;
+        ++ctx->mlp_version;
         return NBX_OK;
     });
 }
@@ -1582,6 +1651,7 @@ int nbx_mlp_train(nbx_ctx* ctx, const float* features, const float* labels, uint
             ck(cudaStreamSynchronize(ctx->stream), "sync");
             if (loss_per_epoch) loss_per_epoch[ep] = l / float(std::max<uint64_t>(n_batches, 1));
         }
+        ++ctx->mlp_version;
         return NBX_OK;
     });
 }

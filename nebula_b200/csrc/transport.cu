@@ -216,6 +216,19 @@ __device__ __forceinline__ int birth_decision(const TransportArgs& a, float p, i
     return kt > wexp ? kt - wexp : 0;
 }
 
+// The network's importance of a newborn from the importance table: its
+// features at birth, each clamped into the table's range, select the cell.
+__device__ __forceinline__ float table_importance(const TransportArgs& a, const float4* tri, const dev::Electron& se) {
+    float f[6];
+    const dev::V3 d = dev::normalised(dev::V3{se.dx, se.dy, se.dz});
+    dev::electron_features(tri, a.smap, se.px, se.py, se.pz, d.x, d.y, d.z, __logf(se.E), se.mat, f);
+    const int m = se.mat < 0 ? 0 : (se.mat >= a.imp_materials ? a.imp_materials - 1 : se.mat);
+    const int ie = min(max(int(floorf(f[0] * float(a.imp_ne))), 0), a.imp_ne - 1);
+    const int id = min(max(int(floorf(f[1] * float(a.imp_nd))), 0), a.imp_nd - 1);
+    const int ic = min(max(int(floorf((f[2] + 1.0f) * 0.5f * float(a.imp_nc))), 0), a.imp_nc - 1);
+    return __ldg(a.imp_table + ((size_t(m) * a.imp_ne + ie) * a.imp_nd + id) * a.imp_nc + ic);
+}
+
 // MinBlocks: resident blocks per SM the register allocation must allow --
 // 256-thread blocks for 2 (128 registers), 3 (80) and 4 (64); 128-thread
 // blocks for 7 (72 registers, 28 warps); the host picks the variant.
@@ -239,16 +252,24 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
     cache.f(0) = 0.0f;   // location 0: empty
     cache.f(1) = 0.0f;
     constexpr bool kExtra = (Mode == kModeSample);
-    constexpr bool kW = (Mode == kModeLearned);
+    constexpr bool kNet = (Mode == kModeLearned);                   // tensor-core inference at birth
+    constexpr bool kW = (Mode == kModeLearned || Mode == kModeWeighted);   // weighted electrons
     bool use_net = false, use_rule = false;
     int rule_k = 0;
     if constexpr (kW) {
         // the fixed (distance, energy) rule at birth, when set, replaces the network
         use_rule = a.birth_survival > 0.0f && a.birth_survival < 1.0f;
         rule_k = use_rule ? max(1, min(a.max_roulette_exp, int(rintf(-__log2f(a.birth_survival))))) : 0;
-        use_net = !use_rule && a.mlp_params != nullptr;
-        if (use_net) mlp::load_weights(g_lsm.w, a.mlp_params);
-        __syncthreads();
+        // the network (or its importance table) is only consulted when its
+        // answer can change something
+        const bool can_act = a.cost_bins > 0 || a.rr_threshold > 0.0f || a.split_threshold < 1.0f;
+        if constexpr (kNet) {
+            use_net = !use_rule && a.mlp_params != nullptr && can_act;
+            if (use_net) mlp::load_weights(g_lsm.w, a.mlp_params);
+            __syncthreads();
+        } else {
+            use_net = !use_rule && a.imp_table != nullptr && can_act;
+        }
     }
     const uint32_t n_in = min(*a.n_in, a.in_capacity);
     dev::Electron e;
@@ -357,8 +378,9 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                 }
             }
         }
-        if constexpr (kW) {
+        if constexpr (kNet) {
             // the whole warp stays in the loop until all its lanes are done
+            // (the tensor-core call at birth needs every lane)
             if (__all_sync(0xffffffffu, !alive)) break;
         } else {
             if (!alive) break;
@@ -385,7 +407,7 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
         dev::Electron se;
         int st = dev::kAlive;
         [[maybe_unused]] const float E_before = e.E;
-        if (!kW || alive) {
+        if (!kNet || alive) {
             st = dev::step<Penn>(P, e, &ev, &se, &has_se, cache);
             ++c_steps;
         }
@@ -403,12 +425,17 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                     dev::surface_distance(P.geo, a.smap, se.px, se.py, se.pz) >= a.birth_min_distance)
                     bk = rule_k;
             } else if (use_net) {
-                const unsigned m = __ballot_sync(0xffffffffu, cand);
-                if (m) {
-                    const float logit = birth_logit(m, cand, P.geo.tri, a.smap, se.px, se.py, se.pz, se.dx, se.dy,
-                                                    se.dz, se.E, se.mat);
-                    if ((threadIdx.x & 31) == 0) ++c_inf;
-                    if (cand) bk = birth_decision(a, mlp::sigmoid(logit), wexp, se.E, se.mat);
+                if constexpr (kNet) {
+                    const unsigned m = __ballot_sync(0xffffffffu, cand);
+                    if (m) {
+                        const float logit = birth_logit(m, cand, P.geo.tri, a.smap, se.px, se.py, se.pz, se.dx,
+                                                        se.dy, se.dz, se.E, se.mat);
+                        if ((threadIdx.x & 31) == 0) ++c_inf;
+                        if (cand) bk = birth_decision(a, mlp::sigmoid(logit), wexp, se.E, se.mat);
+                    }
+                } else if (cand) {
+                    ++c_inf;
+                    bk = birth_decision(a, table_importance(a, P.geo.tri, se), wexp, se.E, se.mat);
                 }
             }
             if (bk > 0) {
@@ -419,7 +446,9 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
             } else if (bk < 0 && wexp <= kMinWeightExp) {
                 bk = 0;   // the lineage is already split as far as it may be
             }
-            if (!alive) continue;
+            if constexpr (kNet) {
+                if (!alive) continue;
+            }
         }
         if constexpr (Mode == kModeDeposit) {
             // energydeposit_cpu_driver::simulate_to_end (drivers/cpu/
@@ -827,6 +856,7 @@ static cudaError_t launch_model(const dev::Physics& P, const TransportArgs& a, i
     if (mode == kModeSample) return launch_mode<kModeSample, Penn>(P, a, grid, block, variant, s);
     if (mode == kModeLearned) return launch_mode<kModeLearned, Penn>(P, a, grid, block, variant, s);
     if (mode == kModeDeposit) return launch_mode<kModeDeposit, Penn>(P, a, grid, block, variant, s);
+    if (mode == kModeWeighted) return launch_mode<kModeWeighted, Penn>(P, a, grid, block, variant, s);
     return launch_mode<kModePlain, Penn>(P, a, grid, block, variant, s);
 }
 
@@ -856,6 +886,7 @@ int transport_max_blocks_per_sm(int block, int variant, int mode) {
     if (mode == kModeSample) return max_blocks_mode<kModeSample>(block, variant);
     if (mode == kModeLearned) return max_blocks_mode<kModeLearned>(block, variant);
     if (mode == kModeDeposit) return max_blocks_mode<kModeDeposit>(block, variant);
+    if (mode == kModeWeighted) return max_blocks_mode<kModeWeighted>(block, variant);
     return max_blocks_mode<kModePlain>(block, variant);
 }
 

@@ -189,13 +189,14 @@ def test_learned_mode_disabled_equals_plain(inputs):
     b.close()
 
 
-@pytest.mark.parametrize("policy", ["window", "cost"])
+@pytest.mark.parametrize("policy", ["window", "cost", "table"])
 def test_learned_roulette_unbiased(inputs, policy):
     """Train on sample-mode records (recorded at birth), then compare the
     weighted yields of the learned mode with plain: the weight window on the
-    network's importance, and the cost-aware survival w sqrt(p K / c) with
-    the cost table fitted to the records' sub-cascade costs.  Both play
-    roulette at birth and stay within 3 sigma of the analogue yields."""
+    network's importance (evaluated for every newborn, or read from the
+    importance table), and the cost-aware survival w sqrt(p K / c) with the
+    cost table fitted to the records' sub-cascade costs.  All play roulette
+    at birth and stay within 3 sigma of the analogue yields."""
     tris = inputs["grating_small"]
     train_recs = g.scan_beam(32, 32, 8, 500.0, origin=(-16.0, -16.0), seed=11)
     c = nb.setup(tris, [inputs["si"]], device=0, seed=66)
@@ -219,6 +220,8 @@ def test_learned_roulette_unbiased(inputs, policy):
         # twice the median importance the network gives the training records:
         # about half the newborns are lighter than their target weight
         th = 2.0 * float(np.median(c.mlp_predict(f)))
+        if policy == "table":
+            c.set_importance_table(24, 16, 8)
         sl, se_l, bse_l, sw, bw = _run(c, recs, "learned", rr_threshold=th, split_threshold=0.99)
     assert sl["roulette_killed"] > 0 and sl["inferences"] > 0
     assert sl["steps"] < sp["steps"]
@@ -274,3 +277,24 @@ def test_split_at_birth_unbiased(inputs):
     for w, c in ((sw.astype(np.float64), se_p.astype(np.float64)), (bw.astype(np.float64), bse_p.astype(np.float64))):
         z = (w.mean() - c.mean()) / np.sqrt(w.var() / len(w) + c.var() / len(c))
         assert abs(z) < 3, z
+
+
+def test_importance_table_without_decisions_equals_plain(inputs):
+    """With the importance table and thresholds that can never act, the
+    weighted transport runs every electron exactly as the plain mode: equal
+    per-tag counts, unit weights, and one table lookup per newborn that is
+    simulated."""
+    recs = g.scan_beam(16, 16, 4, 500.0, origin=(-8.0, -8.0), seed=14)
+    a = nb.setup(inputs["grating_small"], [inputs["si"]], device=0, seed=59)
+    sp, se_p, bse_p, _, _ = _run(a, recs, "plain")
+    a.close()
+    b = nb.setup(inputs["grating_small"], [inputs["si"]], device=0, seed=59)
+    b.build_surface_map([-100, -100, -40], [100, 100, 70], 1.0, 20.0)
+    b.mlp_set_params(M.init_params(0))
+    b.set_importance_table(8, 8, 4)
+    s, se_l, bse_l, sw, bw = _run(b, recs, "learned", rr_threshold=1e-30, split_threshold=0.99999)
+    b.close()
+    assert s["inferences"] > 0 and s["roulette_killed"] == 0 and s["splits"] == 0
+    assert s["steps"] == sp["steps"]
+    assert np.array_equal(se_p, se_l) and np.array_equal(bse_p, bse_l)
+    assert np.array_equal(sw, se_l.astype(np.float32)) and np.array_equal(bw, bse_l.astype(np.float32))
