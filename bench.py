@@ -59,18 +59,19 @@ WORKLOAD = "grating 256x256 px x 100 primaries @ 500 eV (6,553,600 primaries), 5
 # (single-material workloads).
 WORKLOADS = {
     "grating": dict(rows=256, cpu_sample=409600, ref_sample=102400, desc=WORKLOAD,
+                    # config 4 as written: weight window 0.05, splitting above 0.5
                     learned=dict(map_lo=(-180, -180, -60), map_hi=(180, 180, 60), cell=1.0, d_max=20.0,
-                                 train_per_pixel=2, train_on=("grating", "rough"))),
+                                 train_per_pixel=2, train_on=("grating", "rough"), policy="window")),
     "rough": dict(rows=512, cpu_sample=163840, ref_sample=40960,
                   learned=dict(map_lo=(-500, -500, -40), map_hi=(500, 500, 30), cell=2.0, d_max=10.0,
-                               train_per_pixel=1, train_on=("grating", "rough")),
+                               train_per_pixel=1, train_on=("grating", "rough"), policy="cost"),
                   desc="rough slab: 512x512 Gaussian height field (RMS 3 nm, correlation 10 nm) over 1 um, "
                        "526,334 triangles; 512x512 px x 20 primaries (5,242,880) at E uniform over "
                        "{300, 1000, 3000, 5000} eV, Si-like Kieft tables"),
     "holes": dict(rows=64, tune_row=8, cpu_sample=204800, ref_sample=102400,
                   # the map covers the default 64 pixel rows (y up to -1121 nm)
                   learned=dict(map_lo=(-1290, -1290, -170), map_hi=(1290, -1100, 25), cell=2.0, d_max=10.0,
-                               train_per_pixel=1, train_rows=64, train_on=("holes",)),
+                               train_per_pixel=1, train_rows=64, train_on=("holes",), policy="cost"),
                   desc="contact holes: 32x32 holes (40 nm diameter, 100 nm deep, +-2 nm edge roughness) in a "
                        "SiO2-like film over W-like plugs on a Si-like substrate, 2,506,772 triangles over "
                        "2.56 um; 1024x1024 px at 2.5 nm x 200 primaries at 1 keV, one step = %d pixel rows "
@@ -462,12 +463,16 @@ def learned_fom(args, tris, mats, local, rank, prim, tags, plain, tmp, tune_samp
         losses = ctx.mlp_train(f, y, epochs=8, batch=8192, lr=1e-3, seed=1)
         t_train = time.perf_counter() - t0
         ctx.set_tag_range(n)
-        ctx.set_mode("learned", rr_threshold=args.rr_threshold, split_threshold=args.split_threshold,
+        policy = args.learned_policy or L["policy"]
+        # the cost-aware survival runs without splitting: a split adds
+        # near-surface work, the most expensive steps of the scan
+        split = 2.0 if policy == "cost" else args.split_threshold
+        ctx.set_mode("learned", rr_threshold=args.rr_threshold, split_threshold=split,
                      max_roulette_exp=args.max_roulette_exp)
         if args.birth_rr:
             ctx.set_birth_roulette(*[float(v) for v in args.birth_rr.split(",")])
         cost_info = None
-        if args.learned_policy == "cost" and not args.birth_rr:
+        if policy == "cost" and not args.birth_rr:
             # cost-aware survival: mean sub-cascade cost per (material, log E)
             # from the training records; K = steps / variance per primary of
             # the plain timed steps
@@ -515,7 +520,7 @@ def learned_fom(args, tris, mats, local, rank, prim, tags, plain, tmp, tune_samp
                 "decisions_off": {"run_ms": s_off["last_run_ms"], "steps": s_off["steps"],
                                   "ns_per_step": 1e6 * s_off["last_run_ms"] / max(s_off["steps"], 1),
                                   "inferences": s_off["inferences"]},
-                "rr_threshold": args.rr_threshold, "split_threshold": args.split_threshold,
+                "rr_threshold": args.rr_threshold, "split_threshold": split,
                 "max_roulette_exp": args.max_roulette_exp,
                 "autotuned": tuned,
                 "inferences": s["inferences"], "roulette_killed": s["roulette_killed"], "splits": s["splits"],
@@ -562,9 +567,10 @@ def main():
     ap.add_argument("--learned-eval", default="table", choices=["table", "fused"],
                     help="learned leg: network tabulated once over its inputs (table) or evaluated on the tensor "
                          "cores for every newborn (fused)")
-    ap.add_argument("--learned-policy", default="window", choices=["window", "cost"],
-                    help="learned leg: weight window on the network's importance (rr/split thresholds), or "
-                         "cost-aware survival w sqrt(p K / c)")
+    ap.add_argument("--learned-policy", default="", choices=["", "window", "cost"],
+                    help="learned leg: weight window on the network's importance (rr/split thresholds; the "
+                         "grating's default, BASELINE's learned config), or cost-aware survival w sqrt(p K / c) "
+                         "without splitting (the rough slab's and the contact holes' default)")
     ap.add_argument("--inelastic", default="kieft", choices=["kieft", "penn"],
                     help="inelastic model: Kieft & Bosch (the headline workload) or full Penn (the reference's stock build)")
     args = ap.parse_args()

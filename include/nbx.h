@@ -357,17 +357,20 @@ int nbx_set_mode(nbx_ctx* ctx, int32_t mode, float rr_threshold, float split_thr
 /* Learned mode, a fixed rule at birth instead of the network (off until
  * set): a secondary born with energy below max_energy (eV) at least
  * min_distance (nm) from the nearest surface of the surface map (outside the
- * map counts as far) survives with probability `survival` rounded to a power
- * of two, 2^-k with 1 <= k <= max_roulette_exp, and then carries its parent's
- * weight * 2^k; a dropped secondary's cascade is not simulated (counted in
+ * map counts as far) is given the target weight 1 / survival, rounded to a
+ * power of two 2^k with 1 <= k <= max_roulette_exp; lighter than that, it
+ * plays Russian roulette up to it (survives with probability weight / 2^k,
+ * then carries 2^k), so a lineage is rouletted once, not again at every
+ * generation.  A dropped secondary's cascade is not simulated (counted in
  * nbx_stats.roulette_killed).  survival 0 or 1 turns it off. */
 int nbx_set_birth_roulette(nbx_ctx* ctx, float min_distance, float max_energy, float survival);
 /* Learned mode, cost-aware survival (off until set; n_bins = 0 turns it off
  * again): minimising the variance x cost of the tally, a newborn of weight
  * w, importance p and mean sub-cascade cost c survives with
  * q = w * sqrt(p * value_per_cost / c), rounded to a power of two (roulette
- * below 1 with q >= 2^-max_roulette_exp, a split in two from sqrt(2) up); this
- * replaces the rr_threshold / split_threshold window.  c is looked up in
+ * below 1 with q >= 2^-max_roulette_exp, a split in two from sqrt(2) up when
+ * p > split_threshold; split_threshold >= 1 turns splitting off); this
+ * replaces the rr_threshold window.  c is looked up in
  * mean_cost[material * n_bins + bin], bins uniform in log(E / eV) over
  * [log_e_min, log_e_max) (clamped at the ends); costs are in transport steps
  * (e.g. the mean of nbx_get_samples' costs per bin).  value_per_cost is the

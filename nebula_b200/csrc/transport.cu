@@ -196,7 +196,8 @@ constexpr uint32_t kBirthBlock = 0x7FFFFFFFu;
 // particle of weight w whose sub-cascade scores with probability p at mean
 // cost c should survive with q = w sqrt(p K / c), K = cost / variance per
 // primary of the analogue run; q is rounded to a power of two (roulette
-// below 1, at least 2^-max_k; a split in two from sqrt(2) up).
+// below 1, at least 2^-max_k; a split in two from sqrt(2) up, for p above
+// split_threshold).
 __device__ __forceinline__ int birth_decision(const TransportArgs& a, float p, int wexp, float E, int mat) {
     const float pc = fmaxf(p, 1e-30f);
     if (a.cost_bins > 0) {
@@ -207,7 +208,7 @@ __device__ __forceinline__ int birth_decision(const TransportArgs& a, float p, i
         const float l2q = float(wexp) + 0.5f * __log2f(pc * a.value_per_cost / c);
         const int k = -int(rintf(l2q));
         if (k >= 1) return k > a.max_roulette_exp ? a.max_roulette_exp : k;
-        return k <= -1 ? -1 : 0;
+        return (k <= -1 && p > a.split_threshold) ? -1 : 0;
     }
     if (p > a.split_threshold) return wexp >= 0 ? -1 : 0;
     if (!(p < a.rr_threshold)) return 0;
@@ -421,9 +422,11 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
         if constexpr (kW) {
             const bool cand = has_se && !dev::ends_at_init(P, se);
             if (use_rule) {
-                if (cand && se.E < a.birth_max_energy &&
+                // roulette up to the rule's weight 2^rule_k: a newborn that
+                // already carries it (its ancestor survived the rule) is kept
+                if (cand && wexp < rule_k && se.E < a.birth_max_energy &&
                     dev::surface_distance(P.geo, a.smap, se.px, se.py, se.pz) >= a.birth_min_distance)
-                    bk = rule_k;
+                    bk = rule_k - wexp;
             } else if (use_net) {
                 if constexpr (kNet) {
                     const unsigned m = __ballot_sync(0xffffffffu, cand);

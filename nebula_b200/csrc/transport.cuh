@@ -3,9 +3,10 @@
 // Single-precision arithmetic follows the reference's order and grouping
 // operation by operation; the translation unit is compiled with
 // -fmad=false and IEEE division/square root, so octree ray queries and table
-// lookups are bit-identical to the reference CPU path.  Transcendentals are
-// CUDA's accurate logf/expf/expm1f/sincospif, except the free-path sampling
-// of step() (hardware approximations, see there).
+// lookups are bit-identical to the reference CPU path.  The physics that is
+// compared only statistically (free-path sampling, the scattering and
+// boundary tails) uses the hardware's approximate forms (namespace approx,
+// __logf, __expf), except expm1f, which stays accurate.
 #pragma once
 
 #include <cstdint>
@@ -142,33 +143,60 @@ __device__ __forceinline__ V3 normalised(V3 a) {
     const float inv = 1.0f / sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
     return {a.x * inv, a.y * inv, a.z * inv};
 }
+// ---------------------------------------------------------------------------
+// Approximate forms for the statistical-only physics: the scattering and
+// boundary tails are compared with the reference by their statistics, not
+// bit for bit, so they use the hardware's approximate reciprocal square
+// root, quotient, exponential, logarithm and sine/cosine (a few ulp) instead
+// of the correctly rounded or accurate library forms.  Nothing that feeds
+// octree::propagate or a table index comparison with the reference goes
+// through these.
+// ---------------------------------------------------------------------------
+namespace approx {
+// sqrt(x) for x >= 0 as x / sqrt(x) with the hardware reciprocal square root
+__device__ __forceinline__ float sqrt(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+__device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ V3 normalised(V3 a) {
+    const float inv = rsqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
+    return {a.x * inv, a.y * inv, a.z * inv};
+}
+// sin and cos of 2 pi u for u in [0, 1): the angle is shifted into
+// [-pi, pi) where the hardware sine and cosine are accurate, and the signs
+// restored (sin(x + pi) = -sin(x), cos(x + pi) = -cos(x)).
+__device__ __forceinline__ void sincos_2pi(float u, float* s, float* c) {
+    __sincosf(6.28318530717958648f * u - 3.14159265358979324f, s, c);
+    *s = -*s;
+    *c = -*c;
+}
 // make_normal_vec (vector_math.h:171-186) with the rotation angle given as a
 // uniform u (phi = 2 pi u).  The reference takes cos and sin of
 // atan2(dir.y, dir.x); here they are dir.x / r and dir.y / r with
 // r = |(dir.x, dir.y)| (azimuth 0 when r = 0), the same values without the
-// two transcendental calls, and sin/cos(2 pi u) come from sincospif(2 u).
-// Scattering angles are compared statistically, not bit for bit.
+// two transcendental calls.
 __device__ __forceinline__ V3 make_normal_vec(V3 dir, float u_phi) {
-    const float r = sqrtf(dir.x * dir.x + dir.y * dir.y);
-    float sin_az = 0.0f, cos_az = 1.0f;
-    if (r > 0.0f) {
-        cos_az = dir.x / r;
-        sin_az = dir.y / r;
+    const float r2 = dir.x * dir.x + dir.y * dir.y;
+    float sin_az = 0.0f, cos_az = 1.0f, r = 0.0f;
+    if (r2 > 0.0f) {
+        const float inv = rsqrtf(r2);
+        cos_az = dir.x * inv;
+        sin_az = dir.y * inv;
+        r = r2 * inv;
     }
     const V3 v{dir.z * cos_az, dir.z * sin_az, -r};
     const V3 u = cross(v, dir);
     float sp, cp;
-    sincospif(2.0f * u_phi, &sp, &cp);
+    sincos_2pi(u_phi, &sp, &cp);
     return {u.x * cp + v.x * sp, u.y * cp + v.y * sp, u.z * cp + v.z * sp};
 }
-// make_unit_vec (vector_math.h:194-206), phi = 2 pi u_phi as above.
+// make_unit_vec (vector_math.h:194-206), phi = 2 pi u_phi
 __device__ __forceinline__ V3 make_unit_vec(float cos_theta, float u_phi) {
     float sp, cp;
-    sincospif(2.0f * u_phi, &sp, &cp);
+    sincos_2pi(u_phi, &sp, &cp);
     cos_theta = clampr(cos_theta, -1, 1);
-    const float st = sqrtf(1 - cos_theta * cos_theta);
+    const float st = approx::sqrt(1 - cos_theta * cos_theta);
     return {st * cp, st * sp, cos_theta};
 }
+}  // namespace approx
 
 // ---------------------------------------------------------------------------
 // Geometry
@@ -392,7 +420,7 @@ __device__ __forceinline__ float propagate(const Geometry& g, V3 start, V3 dir, 
 // n = normalised(make_normal_vec(d, phi)).
 __device__ __forceinline__ void elastic_finish(const Material& m, Electron& e, float icdf_value, V3 d, V3 n) {
     const float cos_theta = clampr(icdf_value, -1, 1);
-    const float sin_theta = sqrtf(1 - cos_theta * cos_theta);
+    const float sin_theta = approx::sqrt(1 - cos_theta * cos_theta);
     e.dx = d.x * cos_theta + n.x * sin_theta;
     e.dy = d.y * cos_theta + n.y * sin_theta;
     e.dz = d.z * cos_theta + n.z * sin_theta;
@@ -410,7 +438,7 @@ __device__ __forceinline__ void elastic_finish(const Material& m, Electron& e, f
 __device__ __forceinline__ bool inelastic_finish(const Material& m, Electron& e, float log_omega0, V3 d, V3 n,
                                                  float u_bind, float u_omega, float u_v1, float u_v2, Electron* se) {
     const float K = e.E;
-    const float omega0 = expf(log_omega0);
+    const float omega0 = __expf(log_omega0);
     // log(omega0) is the ICDF value itself (the reference takes the log of
     // its exponential); the rounddown lookup sees the same coordinate.
     float binding = table2d_rounddown(m.ion, log_omega0, u_bind);
@@ -420,16 +448,17 @@ __device__ __forceinline__ bool inelastic_finish(const Material& m, Electron& e,
         float omega_min = omega0;
         float w0 = min_ref(omega0 - 1, max_ref(0, binding) - m.fermi);
         if (K > 2 * omega0) {
-            omega_min = 0.5f * (K + omega0 - sqrtf(K * (K - 2 * omega0)));
+            omega_min = 0.5f * (K + omega0 - approx::sqrt(K * (K - 2 * omega0)));
             w0 = omega0;
         }
         const float U = u_omega;
         if ((w0 > 0) && (omega_min > w0) && (omega_min < omega_max)) {
-            const float f_min = 1 / w0 * logf((omega_min - w0) / omega_min);
-            const float f_max = 1 / w0 * logf((omega_max - w0) / omega_max);
-            omega = -w0 / expm1f(w0 * (f_min * (1 - U) + f_max * U));
+            const float inv_w0 = approx::div(1.0f, w0);
+            const float f_min = inv_w0 * __logf(approx::div(omega_min - w0, omega_min));
+            const float f_max = inv_w0 * __logf(approx::div(omega_max - w0, omega_max));
+            omega = approx::div(-w0, expm1f(w0 * (f_min * (1 - U) + f_max * U)));
         } else {
-            omega = omega0 * omega_max / (omega0 * (1 - U) + omega_max * U);
+            omega = approx::div(omega0 * omega_max, omega0 * (1 - U) + omega_max * U);
         }
     }
     if (binding < 0) {
@@ -446,18 +475,18 @@ __device__ __forceinline__ bool inelastic_finish(const Material& m, Electron& e,
 
     const float Kp = e.E - m.fermi + 2 * binding;
     const float dK = binding + omega;
-    const float cos_theta = sqrtf(dK / Kp);
-    const float sin_theta = sqrtf(1 - clampr(cos_theta * cos_theta, 0, 1));
+    const float cos_theta = approx::sqrt(approx::div(dK, Kp));
+    const float sin_theta = approx::sqrt(1 - clampr(cos_theta * cos_theta, 0, 1));
     V3 s{d.x * cos_theta + n.x * sin_theta, d.y * cos_theta + n.y * sin_theta, d.z * cos_theta + n.z * sin_theta};
-    s = normalised(s);
+    s = approx::normalised(s);
     {
-        const V3 uv = make_unit_vec(2 * u_v1 - 1, u_v2);
-        const float a = sqrtf(binding / dK);
+        const V3 uv = approx::make_unit_vec(2 * u_v1 - 1, u_v2);
+        const float a = approx::sqrt(approx::div(binding, dK));
         s.x += a * uv.x;
         s.y += a * uv.y;
         s.z += a * uv.z;
     }
-    s = normalised(s);
+    s = approx::normalised(s);
 
     se->px = e.px;
     se->py = e.py;
@@ -493,9 +522,9 @@ constexpr uint32_t kMaxPlasmonRounds = 64;
 __device__ __forceinline__ bool penn_finish(const Physics& P, const Material& m, Electron& e, float log_omega,
                                             float logE, V3 d, V3 n, uint4 r1, Electron* se) {
     const float K = e.E;
-    const float omega = expf(log_omega);
+    const float omega = __expf(log_omega);
     // ionisation table at (log K, log(omega / K), P)
-    const float binding = table3d_rounddown(m.ion3, logE, logf(omega / K), u01(r1.x));
+    const float binding = table3d_rounddown(m.ion3, logE, __logf(approx::div(omega, K)), u01(r1.x));
     V3 sdir;
     float se_E;
     if (binding <= 0) {
@@ -509,22 +538,22 @@ __device__ __forceinline__ bool penn_finish(const Physics& P, const Material& m,
             return false;
         }
         // Fermi-sea excitation; q = hbar q / sqrt(2m) in eV^1/2
-        const float q = table3d_get(m.q, logE, omega / K, u01(r1.y));
-        const float c1 = clampr((omega + q * q) / (2 * sqrtf(K) * q), -1, 1);
-        const float s1 = sqrtf(1 - c1 * c1);
-        const V3 q_dir = normalised(V3{d.x * c1 + n.x * s1, d.y * c1 + n.y * s1, d.z * c1 + n.z * s1});
-        const V3 q_normal = normalised(make_normal_vec(q_dir, u01(r1.z)));
-        const float c2 = clampr((2 * K - omega - q * q) / (2 * sqrtf(K * (K - omega))), -1, 1);
-        const float s2 = sqrtf(1 - c2 * c2);
+        const float q = table3d_get(m.q, logE, approx::div(omega, K), u01(r1.y));
+        const float c1 = clampr(approx::div(omega + q * q, 2 * approx::sqrt(K) * q), -1, 1);
+        const float s1 = approx::sqrt(1 - c1 * c1);
+        const V3 q_dir = approx::normalised(V3{d.x * c1 + n.x * s1, d.y * c1 + n.y * s1, d.z * c1 + n.z * s1});
+        const V3 q_normal = approx::normalised(approx::make_normal_vec(q_dir, u01(r1.z)));
+        const float c2 = clampr(approx::div(2 * K - omega - q * q, 2 * approx::sqrt(K * (K - omega))), -1, 1);
+        const float s2 = approx::sqrt(1 - c2 * c2);
         e.E = K - omega;
         e.dx = d.x * c2 + n.x * s2;
         e.dy = d.y * c2 + n.y * s2;
         e.dz = d.z * c2 + n.z * s2;
-        const float k_fermi = sqrtf(m.fermi);
-        const float k_fermi_omega = sqrtf(m.fermi + omega);
+        const float k_fermi = approx::sqrt(m.fermi);
+        const float k_fermi_omega = approx::sqrt(m.fermi + omega);
         if (q < k_fermi_omega - k_fermi) {
             // plasmon decay: x = E_i / omega from p(x) ~ sqrt(x (x + 1)) on [0, f]
-            const float f = m.fermi / omega;
+            const float f = approx::div(m.fermi, omega);
             float x;
             if (f < 0.1f) {
                 const float U = cbrtf(u01(r1.w));
@@ -534,26 +563,27 @@ __device__ __forceinline__ bool penn_finish(const Physics& P, const Material& m,
                 const float upper = f;
                 const float d1 = upper - lower;
                 const float d2 = upper * upper - lower * lower;
-                const float alpha = d2 / (d1 + d2);
+                const float alpha = approx::div(d2, d1 + d2);
                 for (uint32_t k = 0;; ++k) {
                     const uint4 rk = draw(P.seed, e, 4 + k);
                     const float U1 = u01(rk.x);
                     const float U2 = u01(rk.y);
-                    x = (U1 < alpha) ? sqrtf(d2 * U2 + lower * lower) : d1 * U2 + lower;
-                    if (!(u01(rk.z) > sqrtf(x * x + x) / (x + 0.5f)) || k + 1 == kMaxPlasmonRounds) break;
+                    x = (U1 < alpha) ? approx::sqrt(d2 * U2 + lower * lower) : d1 * U2 + lower;
+                    if (!(u01(rk.z) > approx::div(approx::sqrt(x * x + x), x + 0.5f)) || k + 1 == kMaxPlasmonRounds)
+                        break;
                 }
             }
             se_E = x * omega + omega;
             const uint4 r3 = draw(P.seed, e, 3);
-            sdir = make_unit_vec(2 * u01(r3.x) - 1, u01(r3.y));
+            sdir = approx::make_unit_vec(2 * u01(r3.x) - 1, u01(r3.y));
         } else if (q < k_fermi_omega + k_fermi) {
             // single excitation from the annulus of allowed initial k around q
-            const float ki_parr = (omega - q * q) / (2 * q);
+            const float ki_parr = approx::div(omega - q * q, 2 * q);
             const float kf_parr = ki_parr + q;
             const float ki_perp_min_sq = max_ref(0, m.fermi - kf_parr * kf_parr);
             const float ki_perp_max_sq = m.fermi - ki_parr * ki_parr;
             const float ki_perp_sq = max_ref(0, ki_perp_min_sq + (ki_perp_max_sq - ki_perp_min_sq) * u01(r1.w));
-            const float kp = sqrtf(ki_perp_sq);
+            const float kp = approx::sqrt(ki_perp_sq);
             const V3 ki{ki_parr * q_dir.x + kp * q_normal.x, ki_parr * q_dir.y + kp * q_normal.y,
                         ki_parr * q_dir.z + kp * q_normal.z};
             se_E = (ki.x * ki.x + ki.y * ki.y + ki.z * ki.z) + omega;
@@ -565,17 +595,17 @@ __device__ __forceinline__ bool penn_finish(const Physics& P, const Material& m,
         // inner-shell excitation (Ivanchenko angles, as kieft_inelastic)
         const float Kp = K - m.fermi + 2 * binding;
         const float dK = binding + omega;
-        const float cos_theta = sqrtf(dK / Kp);
-        const float sin_theta = sqrtf(1 - clampr(cos_theta * cos_theta, 0, 1));
+        const float cos_theta = approx::sqrt(approx::div(dK, Kp));
+        const float sin_theta = approx::sqrt(1 - clampr(cos_theta * cos_theta, 0, 1));
         V3 s{d.x * cos_theta + n.x * sin_theta, d.y * cos_theta + n.y * sin_theta, d.z * cos_theta + n.z * sin_theta};
-        s = normalised(s);
+        s = approx::normalised(s);
         const uint4 r3 = draw(P.seed, e, 3);
-        const V3 uv = make_unit_vec(2 * u01(r3.x) - 1, u01(r3.y));
-        const float a = sqrtf(binding / dK);
+        const V3 uv = approx::make_unit_vec(2 * u01(r3.x) - 1, u01(r3.y));
+        const float a = approx::sqrt(approx::div(binding, dK));
         s.x += a * uv.x;
         s.y += a * uv.y;
         s.z += a * uv.z;
-        s = normalised(s);
+        s = approx::normalised(s);
         se_E = m.fermi + omega - binding;
         sdir = s;
         e.E = K - omega;
@@ -603,8 +633,8 @@ __device__ __forceinline__ bool penn_finish(const Physics& P, const Material& m,
 __device__ __forceinline__ int boundary(const Physics& P, Electron& e, float u) {
     int mi, mo;
     const V3 face = load_face(P.geo, e.last_tri, mi, mo);
-    const V3 nd = normalised(V3{e.dx, e.dy, e.dz});
-    const V3 n = normalised(face);
+    const V3 nd = approx::normalised(V3{e.dx, e.dy, e.dz});
+    const V3 n = approx::normalised(face);
     const float cos_theta = dot(n, nd);
     int in, out;
     if (cos_theta > 0) {
@@ -637,8 +667,8 @@ __device__ __forceinline__ int boundary(const Physics& P, Electron& e, float u) 
     if (in >= 0) dU -= P.mat[in].barrier;
     if (out >= 0) dU += P.mat[out].barrier;
     if (e.E * cos_theta * cos_theta + dU > 0) {
-        const float s = sqrtf(1 + dU / (e.E * cos_theta * cos_theta));
-        const float T = 4 * s / ((1 + s) * (1 + s));
+        const float s = approx::sqrt(1 + approx::div(dU, e.E * cos_theta * cos_theta));
+        const float T = approx::div(4 * s, (1 + s) * (1 + s));
         if (u < T) {
             e.dx = (nd.x - n.x * cos_theta) + s * n.x * cos_theta;
             e.dy = (nd.y - n.y * cos_theta) + s * n.y * cos_theta;
@@ -732,7 +762,7 @@ __device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, E
             const Material& m = P.mat[e.mat];
             const bool inel = (type == 1);
             const float tv = table2d_get(inel ? m.in_icdf : m.el_icdf, logE, u01(r0.z));
-            const V3 n = normalised(make_normal_vec(nd, u01(r0.w)));
+            const V3 n = approx::normalised(approx::make_normal_vec(nd, u01(r0.w)));
             if (!inel) {
                 elastic_finish(m, e, tv, nd, n);
                 *event = kEvElastic;
