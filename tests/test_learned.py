@@ -182,10 +182,17 @@ def test_learned_mode_disabled_equals_plain(inputs):
     b = nb.setup(inputs["grating_small"], [inputs["si"]], device=0, seed=55)
     b.build_surface_map([-100, -100, -40], [100, 100, 70], 1.0, 20.0)
     b.mlp_set_params(M.init_params(0))
-    s, se_l, bse_l, sw, bw = _run(b, recs, "learned", rr_threshold=0.0, split_threshold=2.0)
+    # thresholds the network's answer can never cross: it is evaluated for
+    # every newborn (on the tensor cores) and nothing changes
+    s, se_l, bse_l, sw, bw = _run(b, recs, "learned", rr_threshold=1e-30, split_threshold=0.99999)
     assert s["inferences"] > 0 and s["roulette_killed"] == 0 and s["splits"] == 0
     assert np.array_equal(se_p, se_l) and np.array_equal(bse_p, bse_l)
     assert np.array_equal(sw, se_l.astype(np.float32)) and np.array_equal(bw, bse_l.astype(np.float32))
+    # thresholds under which no decision is possible: the network is not
+    # consulted at all, with the same result
+    s, se_l, bse_l, sw, bw = _run(b, recs, "learned", rr_threshold=0.0, split_threshold=2.0)
+    assert s["inferences"] == 0 and s["roulette_killed"] == 0 and s["splits"] == 0
+    assert np.array_equal(se_p, se_l) and np.array_equal(bse_p, bse_l)
     b.close()
 
 
