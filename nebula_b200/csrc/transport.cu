@@ -14,6 +14,7 @@
 // push).  Detections are tallied per primary tag on the device; detected
 // records are optional.
 #include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
 
 #include <algorithm>
 #include <mutex>
@@ -733,6 +734,9 @@ __global__ void step_query_kernel(const dev::Physics P, ElectronRecord* el, uint
 
 // se_w / bse_w (learned mode): per-tag weighted detections used instead of
 // the counts, so the sums are of per-primary weighted yields and their squares.
+// Tags of a scan are usually numbered pixel by pixel, so the lanes of a warp
+// mostly share a pixel: they are grouped by pixel and each group adds its
+// sums with one set of atomics.
 __global__ void pixel_yields_kernel(const uint32_t* se, const uint32_t* bse, const float* se_w, const float* bse_w,
                                     const uint32_t* pixel_of_tag, uint64_t n_tags, uint64_t n_pixels, double* out) {
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n_tags;
@@ -740,15 +744,23 @@ __global__ void pixel_yields_kernel(const uint32_t* se, const uint32_t* bse, con
         const uint32_t p = pixel_of_tag[i];
         if (p >= n_pixels) continue;
         const double s = se_w ? double(se_w[i]) : double(se[i]), b = bse_w ? double(bse_w[i]) : double(bse[i]);
-        double* o = out + 5 * size_t(p);
-        atomicAdd(o + 0, 1.0);
-        if (s != 0) {
-            atomicAdd(o + 1, s);
-            atomicAdd(o + 2, s * s);
-        }
-        if (b != 0) {
-            atomicAdd(o + 3, b);
-            atomicAdd(o + 4, b * b);
+        const cg::coalesced_group grp = cg::labeled_partition(cg::coalesced_threads(), p);
+        const double n_sum = cg::reduce(grp, 1.0, cg::plus<double>());
+        const double s_sum = cg::reduce(grp, s, cg::plus<double>());
+        const double s2_sum = cg::reduce(grp, s * s, cg::plus<double>());
+        const double b_sum = cg::reduce(grp, b, cg::plus<double>());
+        const double b2_sum = cg::reduce(grp, b * b, cg::plus<double>());
+        if (grp.thread_rank() == 0) {
+            double* o = out + 5 * size_t(p);
+            atomicAdd(o + 0, n_sum);
+            if (s_sum != 0) {
+                atomicAdd(o + 1, s_sum);
+                atomicAdd(o + 2, s2_sum);
+            }
+            if (b_sum != 0) {
+                atomicAdd(o + 3, b_sum);
+                atomicAdd(o + 4, b2_sum);
+            }
         }
     }
 }
