@@ -852,6 +852,10 @@ int nbx_run(nbx_ctx* ctx) {
             a.n_ranges = uint32_t(ctx->sms);
         }
 
+        // electrons lost to a full overflow queue before this run (the
+        // counter is cumulative until nbx_reset_tallies)
+        unsigned long long ovf_before = 0;
+        to_host(ctx, &ovf_before, ctx->counters.p + nbx::kCntOverflow, 8, "D2H");
         ck(cudaEventRecord(ctx->ev0, ctx->stream), "event");
         int g = 0;
         bool done = false;
@@ -886,7 +890,7 @@ int nbx_run(nbx_ctx* ctx) {
         ctx->n_queued = 0;
         unsigned long long ovf = 0;
         to_host(ctx, &ovf, ctx->counters.p + nbx::kCntOverflow, 8, "D2H");
-        if (ovf) throw ApiError(NBX_ERR_CAPACITY, "secondary queue overflow: electrons lost");
+        if (ovf > ovf_before) throw ApiError(NBX_ERR_CAPACITY, "secondary queue overflow: electrons lost");
         return NBX_OK;
     });
 }
@@ -1265,11 +1269,18 @@ int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* ta
     // Time the sample with the context's current settings (its mode
     // included): twice on the same random streams, the first pass also
     // paying one-time costs (module load, buffer growth); the second is kept.
+    // A setting whose run loses electrons to a full overflow queue (a stack
+    // too shallow for the sample's cascades) is not a candidate.
     auto time_it = [&](double* ms) {
         for (int rep = 0; rep < 2; ++rep) {
             ctx->uid_next = uid_save;
             int rc = nbx_push(ctx, particles, tags, n, nullptr);
             if (rc == NBX_OK) rc = nbx_run(ctx);
+            if (rc == NBX_ERR_CAPACITY) {
+                *ms = 1e300;
+                ctx->err.clear();
+                return NBX_OK;
+            }
             if (rc != NBX_OK) return rc;
         }
         *ms = ctx->last_run_ms;

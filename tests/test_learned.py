@@ -189,7 +189,8 @@ def test_learned_mode_disabled_equals_plain(inputs):
     assert np.array_equal(se_p, se_l) and np.array_equal(bse_p, bse_l)
     assert np.array_equal(sw, se_l.astype(np.float32)) and np.array_equal(bw, bse_l.astype(np.float32))
     # thresholds under which no decision is possible: the network is not
-    # consulted at all, with the same result
+    # consulted at all, with the same result (same random streams)
+    b.set_uid_base(0)
     s, se_l, bse_l, sw, bw = _run(b, recs, "learned", rr_threshold=0.0, split_threshold=2.0)
     assert s["inferences"] == 0 and s["roulette_killed"] == 0 and s["splits"] == 0
     assert np.array_equal(se_p, se_l) and np.array_equal(bse_p, bse_l)
