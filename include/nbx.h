@@ -328,8 +328,7 @@ int nbx_autotune(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* ta
  * [out][in] with inputs padded to 16 and the output to 8:
  * W1[64][16] b1[64] W2[64][64] b2[64] W3[8][64] b3[8] (padding forced to 0).
  * Features (6 per sample): log(E/eV) scaled, distance to the nearest surface
- * scaled, direction cosine toward that surface's outward normal, material
- * one-hot (3). */
+ * scaled, direction cosine toward that surface, material one-hot (3). */
 #define NBX_MLP_PARAMS 5768
 
 /* Transport modes.  PLAIN: analogue transport (the reference's method).
@@ -389,9 +388,11 @@ int nbx_set_learned_cost(nbx_ctx* ctx, const float* mean_cost, int32_t n_materia
  * automatically when the parameters change (nbx_mlp_set_params,
  * nbx_mlp_train). */
 int nbx_set_importance_table(nbx_ctx* ctx, int32_t n_energy, int32_t n_distance, int32_t n_cosine);
-/* Nearest-triangle map over the box [lo, hi) with the given cell size (nm);
- * surfaces farther than d_max (nm) count as "far".  Needed for the distance
- * and cosine features. */
+/* Surface map over the box [lo, hi) with the given cell size (nm): per cell
+ * the distance from its centre to the nearest material surface and the unit
+ * vector from that surface point to the centre; a point of the cell takes
+ * the first-order distance from them.  Surfaces farther than d_max (nm) count
+ * as "far".  Needed for the distance and cosine features. */
 int nbx_build_surface_map(nbx_ctx* ctx, const float lo[3], const float hi[3], float cell, float d_max);
 int nbx_set_sample_capacity(nbx_ctx* ctx, uint64_t capacity);
 /* Copy out (and clear) the recorded samples: features n x 6, labels n and,

@@ -1,14 +1,17 @@
 // Input features of the escape-probability network (no reference
 // counterpart): log energy, distance to the nearest surface, direction
-// cosine toward that surface's outward normal, material one-hot.
+// cosine toward that surface, material one-hot.
 //
-// The nearest surface comes from a nearest-triangle map: a regular grid over
-// a region of interest whose cells store the triangle closest to the cell
-// centre (or -1 when none lies within d_max).  At run time the electron's
-// cell gives a candidate triangle and the exact point-triangle distance and
-// normal are computed from it, so the feature is exact wherever the cell's
-// nearest triangle is the point's nearest triangle and within one cell
-// diagonal of it elsewhere.
+// The nearest surface comes from a surface map: a regular grid over a region
+// of interest whose cells store, for the cell centre c, the distance d_c to
+// the nearest point q of any material triangle and the unit vector
+// g = (c - q) / d_c from that point to the centre (the gradient of the
+// distance field), or d_c < 0 when no triangle lies within d_max.  At a point
+// p of the cell the distance is taken to first order, d_c + g . (p - c):
+// exact where p and c see the same face of the nearest triangle, and within
+// the cell's extent of the true distance elsewhere (both lie between
+// d_c - |p - c| and |p - q|).  The cosine toward the surface is -g . dir.  A
+// feature lookup is one 16-byte gather.
 #pragma once
 
 #include <cstdint>
@@ -19,9 +22,9 @@ namespace nbx {
 namespace dev {
 
 struct SurfaceMap {
-    const int32_t* cell_tri;   // nullptr: no map (distance feature saturates)
+    const float4* cell;   // per cell (g.x, g.y, g.z, d_c); nullptr: no map (distance feature saturates)
     float lox, loy, loz;
-    float inv_cell;
+    float cell_size, inv_cell;
     int nx, ny, nz;
     float d_max;
 };
@@ -88,17 +91,31 @@ __device__ __forceinline__ float dist2_to_triangle(const float4* tri, int ti, fl
     return (px - qx) * (px - qx) + (py - qy) * (py - qy) + (pz - qz) * (pz - qz);
 }
 
-// Distance from p to the surface map's nearest triangle for p's cell, or
-// d_max where the map has none within d_max or p lies outside the map.
-__device__ __forceinline__ float surface_distance(const Geometry& g, const SurfaceMap& S, float px, float py, float pz) {
-    if (!S.cell_tri) return S.d_max;
+// The surface-map cell of p: its record, and the offset of p from the cell
+// centre; false when p lies outside the map or the cell has no surface within
+// d_max.
+__device__ __forceinline__ bool surface_cell(const SurfaceMap& S, float px, float py, float pz, float4* rec,
+                                             float* ox, float* oy, float* oz) {
+    if (!S.cell) return false;
     const int ix = int(floorf((px - S.lox) * S.inv_cell));
     const int iy = int(floorf((py - S.loy) * S.inv_cell));
     const int iz = int(floorf((pz - S.loz) * S.inv_cell));
-    if (ix < 0 || iy < 0 || iz < 0 || ix >= S.nx || iy >= S.ny || iz >= S.nz) return S.d_max;
-    const int ti = __ldg(S.cell_tri + (size_t(iz) * S.ny + iy) * S.nx + ix);
-    if (ti < 0) return S.d_max;
-    return fminf(sqrtf(dist2_to_triangle(g.tri, ti, px, py, pz)), S.d_max);
+    if (ix < 0 || iy < 0 || iz < 0 || ix >= S.nx || iy >= S.ny || iz >= S.nz) return false;
+    *rec = __ldg(S.cell + (size_t(iz) * S.ny + iy) * S.nx + ix);
+    if (!(rec->w >= 0.0f)) return false;
+    *ox = px - (S.lox + (float(ix) + 0.5f) * S.cell_size);
+    *oy = py - (S.loy + (float(iy) + 0.5f) * S.cell_size);
+    *oz = pz - (S.loz + (float(iz) + 0.5f) * S.cell_size);
+    return true;
+}
+
+// Distance from p to the nearest surface (first order in the map cell),
+// clamped to [0, d_max]; d_max outside the map or with no surface within d_max.
+__device__ __forceinline__ float surface_distance(const SurfaceMap& S, float px, float py, float pz) {
+    float4 r;
+    float ox, oy, oz;
+    if (!surface_cell(S, px, py, pz, &r, &ox, &oy, &oz)) return S.d_max;
+    return fminf(fmaxf(r.w + r.x * ox + r.y * oy + r.z * oz, 0.0f), S.d_max);
 }
 
 // Feature scaling: log E over [log 12 eV, log 8 keV] -> about [0, 1]; the
@@ -106,39 +123,21 @@ __device__ __forceinline__ float surface_distance(const Geometry& g, const Surfa
 constexpr float kLogEOffset = 2.5f;
 constexpr float kLogEScale = 1.0f / 6.5f;
 
-// f[6] for an electron at p with unit direction d in material `mat` (>= 0);
-// tri: the geometry's triangle records (Geometry::tri).
-__device__ __forceinline__ void electron_features(const float4* tri, const SurfaceMap& S, float px, float py, float pz,
-                                                  float dx, float dy, float dz, float logE, int mat, float f[6]) {
+// f[6] for an electron at p with unit direction d in material `mat` (>= 0).
+__device__ __forceinline__ void electron_features(const SurfaceMap& S, float px, float py, float pz, float dx,
+                                                  float dy, float dz, float logE, int mat, float f[6]) {
     f[0] = (logE - kLogEOffset) * kLogEScale;
     f[1] = 1.0f;
     f[2] = 0.0f;
     f[3] = mat == 0 ? 1.0f : 0.0f;
     f[4] = mat == 1 ? 1.0f : 0.0f;
     f[5] = mat == 2 ? 1.0f : 0.0f;
-    if (!S.cell_tri) return;
-    const int ix = int(floorf((px - S.lox) * S.inv_cell));
-    const int iy = int(floorf((py - S.loy) * S.inv_cell));
-    const int iz = int(floorf((pz - S.loz) * S.inv_cell));
-    if (ix < 0 || iy < 0 || iz < 0 || ix >= S.nx || iy >= S.ny || iz >= S.nz) return;
-    const int ti = __ldg(S.cell_tri + (size_t(iz) * S.ny + iy) * S.nx + ix);
-    if (ti < 0) return;
-    const float4 a = __ldg(tri + 3 * ti), b = __ldg(tri + 3 * ti + 1), c = __ldg(tri + 3 * ti + 2);
-    float qx, qy, qz;
-    closest_point_on_triangle(px, py, pz, a, b, c, &qx, &qy, &qz);
-    const float dist = sqrtf((px - qx) * (px - qx) + (py - qy) * (py - qy) + (pz - qz) * (pz - qz));
-    // outward normal: the triangle normal e1 x e2 points from material_in to
-    // material_out; leaving the electron's material means following it when
-    // the electron is on the material_in side.
-    float nx = b.y * c.z - b.z * c.y, ny = b.z * c.x - b.x * c.z, nz = b.x * c.y - b.y * c.x;
-    const float inv = rsqrtf(nx * nx + ny * ny + nz * nz + 1e-30f);
-    const float sgn = (__float_as_int(a.w) == mat) ? 1.0f : -1.0f;
-    f[1] = fminf(dist, S.d_max) / S.d_max;
-    f[2] = sgn * (nx * dx + ny * dy + nz * dz) * inv;
-}
-__device__ __forceinline__ void electron_features(const Geometry& g, const SurfaceMap& S, float px, float py, float pz,
-                                                  float dx, float dy, float dz, float logE, int mat, float f[6]) {
-    electron_features(g.tri, S, px, py, pz, dx, dy, dz, logE, mat, f);
+    float4 r;
+    float ox, oy, oz;
+    if (!surface_cell(S, px, py, pz, &r, &ox, &oy, &oz)) return;
+    const float dist = fminf(fmaxf(r.w + r.x * ox + r.y * oy + r.z * oz, 0.0f), S.d_max);
+    f[1] = dist / S.d_max;
+    f[2] = -(r.x * dx + r.y * dy + r.z * dz);
 }
 #endif
 

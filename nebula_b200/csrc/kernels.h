@@ -158,16 +158,17 @@ int transport_max_blocks_per_sm(int block, int variant, int mode = kModePlain);
 // Per-triangle face records (normal e1 x e2 and packed materials) for
 // Geometry::tri_face; materials must fit in 16 bits.
 cudaError_t launch_triangle_faces(const float4* tri, float4* face, int n, cudaStream_t s);
-// Nearest-triangle map over [lo, lo + n * cell): each cell searches the
-// candidate list of its brick of `brick`^3 cells (brick_tris[brick_start[b]
-// .. brick_start[b + 1]), bricks x-fastest over nbx x nby x ...); cells
-// farther than d_max from all candidates get -1.
+// Surface map over [lo, lo + n * cell): each cell searches the candidate
+// list of its brick of `brick`^3 cells (brick_tris[brick_start[b] ..
+// brick_start[b + 1]), bricks x-fastest over nbx x nby x ...) for the nearest
+// triangle and stores (unit vector from its nearest point to the cell
+// centre, distance); cells farther than d_max from all candidates get
+// distance -1.
 cudaError_t launch_build_surface_map(const float4* tri, const uint32_t* brick_start, const int32_t* brick_tris,
-                                     int nbx, int nby, int brick, int32_t* map, float lox, float loy, float loz,
+                                     int nbx, int nby, int brick, float4* map, float lox, float loy, float loz,
                                      float cell, int nx, int ny, int nz, float d_max, cudaStream_t s);
 // Features of n electrons (56-byte nbx_electron records) for testing.
-cudaError_t launch_features(const dev::Geometry& g, const dev::SurfaceMap& S, const void* electrons, uint64_t n,
-                            float* out, cudaStream_t s);
+cudaError_t launch_features(const dev::SurfaceMap& S, const void* electrons, uint64_t n, float* out, cudaStream_t s);
 
 cudaError_t launch_ray_query(const dev::Geometry& g, const float* pos, const float* dir, const float* dist,
                              const int32_t* ignore_tri, const int32_t* ignore_mat, uint64_t n, float* out_dist,

@@ -140,7 +140,7 @@ struct nbx_ctx {
     DevBuf<float> cost_table;      // cost-aware survival (nbx_set_learned_cost)
     int cost_bins = 0, cost_materials = 0;
     float cost_log_e_min = 0, cost_inv_width = 0, value_per_cost = 0;
-    DevBuf<int32_t> smap_cells;
+    DevBuf<float4> smap_cells;
     nbx::dev::SurfaceMap smap{};
     DevBuf<float> sample_feat, sample_label, sample_cost;
     DevBuf<uint32_t> sample_count;
@@ -1475,10 +1475,11 @@ int nbx_build_surface_map(nbx_ctx* ctx, const float lo[3], const float hi[3], fl
         ck(nbx::launch_build_surface_map(ctx->tris.p, dstart.p, dlist.p, nb[0], nb[1], kBrick, ctx->smap_cells.p, lo[0],
                                          lo[1], lo[2], cell, n[0], n[1], n[2], d_max, ctx->stream), "surface map");
         ck(cudaStreamSynchronize(ctx->stream), "surface map");
-        ctx->smap.cell_tri = ctx->smap_cells.p;
+        ctx->smap.cell = ctx->smap_cells.p;
         ctx->smap.lox = lo[0];
         ctx->smap.loy = lo[1];
         ctx->smap.loz = lo[2];
+        ctx->smap.cell_size = cell;
         ctx->smap.inv_cell = 1.0f / cell;
         ctx->smap.nx = n[0];
         ctx->smap.ny = n[1];
@@ -1546,7 +1547,7 @@ int nbx_features_query(nbx_ctx* ctx, const nbx_electron* electrons, uint64_t n, 
         e.alloc(56 * n);
         f.alloc(6 * n);
         ck(cudaMemcpyAsync(e.p, electrons, 56 * n, cudaMemcpyHostToDevice, ctx->stream), "H2D");
-        ck(nbx::launch_features(ctx->phys.geo, ctx->smap, e.p, n, f.p, ctx->stream), "features");
+        ck(nbx::launch_features(ctx->smap, e.p, n, f.p, ctx->stream), "features");
         ck(cudaMemcpyAsync(out, f.p, 24 * n, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
         ck(cudaStreamSynchronize(ctx->stream), "sync");
         return NBX_OK;

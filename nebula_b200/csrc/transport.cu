@@ -86,15 +86,15 @@ __shared__ __align__(16) LearnedSmem g_lsm;
 // feature tile and one m-tile (up to 16 candidates) or two go through the
 // tensor cores.  Called by the whole warp.  Not inlined, so the network's
 // register demand does not raise the transport loop's.
-__device__ __noinline__ float birth_logit(unsigned m, bool cand, const float4* tri, const dev::SurfaceMap S, float px,
-                                          float py, float pz, float dx, float dy, float dz, float E, int mat) {
+__device__ __noinline__ float birth_logit(unsigned m, bool cand, const dev::SurfaceMap S, float px, float py, float pz,
+                                          float dx, float dy, float dz, float E, int mat) {
     const int lane = threadIdx.x & 31;
     const int rank = __popc(m & ((1u << lane) - 1u));
     __nv_bfloat16* xs = g_lsm.xs + (threadIdx.x >> 5) * 32 * mlp::kIn;
     if (cand) {
         float f[6];
         const dev::V3 d = dev::normalised(dev::V3{dx, dy, dz});
-        dev::electron_features(tri, S, px, py, pz, d.x, d.y, d.z, logf(E), mat, f);
+        dev::electron_features(S, px, py, pz, d.x, d.y, d.z, logf(E), mat, f);
         __nv_bfloat16* row = xs + rank * mlp::kIn;
 #pragma unroll
         for (int k = 0; k < mlp::kIn; ++k) row[k] = __float2bfloat16_rn(k < 6 ? f[k] : 0.0f);
@@ -220,10 +220,10 @@ __device__ __forceinline__ int birth_decision(const TransportArgs& a, float p, i
 
 // The network's importance of a newborn from the importance table: its
 // features at birth, each clamped into the table's range, select the cell.
-__device__ __forceinline__ float table_importance(const TransportArgs& a, const float4* tri, const dev::Electron& se) {
+__device__ __forceinline__ float table_importance(const TransportArgs& a, const dev::Electron& se) {
     float f[6];
-    const dev::V3 d = dev::normalised(dev::V3{se.dx, se.dy, se.dz});
-    dev::electron_features(tri, a.smap, se.px, se.py, se.pz, d.x, d.y, d.z, __logf(se.E), se.mat, f);
+    const dev::V3 d = dev::approx::normalised(dev::V3{se.dx, se.dy, se.dz});
+    dev::electron_features(a.smap, se.px, se.py, se.pz, d.x, d.y, d.z, __logf(se.E), se.mat, f);
     const int m = se.mat < 0 ? 0 : (se.mat >= a.imp_materials ? a.imp_materials - 1 : se.mat);
     const int ie = min(max(int(floorf(f[0] * float(a.imp_ne))), 0), a.imp_ne - 1);
     const int id = min(max(int(floorf(f[1] * float(a.imp_nd))), 0), a.imp_nd - 1);
@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                 if (slot < a.sample_capacity) {
                     float f[6];
                     const dev::V3 d = dev::normalised(dev::V3{e.dx, e.dy, e.dz});
-                    dev::electron_features(P.geo, a.smap, e.px, e.py, e.pz, d.x, d.y, d.z, logf(e.E), e.mat, f);
+                    dev::electron_features(a.smap, e.px, e.py, e.pz, d.x, d.y, d.z, logf(e.E), e.mat, f);
 #pragma unroll
                     for (int k = 0; k < 6; ++k) a.sample_feat[size_t(slot) * 6 + k] = f[k];
                     ex.rec = int(slot);
@@ -426,20 +426,20 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                 // roulette up to the rule's weight 2^rule_k: a newborn that
                 // already carries it (its ancestor survived the rule) is kept
                 if (cand && wexp < rule_k && se.E < a.birth_max_energy &&
-                    dev::surface_distance(P.geo, a.smap, se.px, se.py, se.pz) >= a.birth_min_distance)
+                    dev::surface_distance(a.smap, se.px, se.py, se.pz) >= a.birth_min_distance)
                     bk = rule_k - wexp;
             } else if (use_net) {
                 if constexpr (kNet) {
                     const unsigned m = __ballot_sync(0xffffffffu, cand);
                     if (m) {
-                        const float logit = birth_logit(m, cand, P.geo.tri, a.smap, se.px, se.py, se.pz, se.dx,
-                                                        se.dy, se.dz, se.E, se.mat);
+                        const float logit =
+                            birth_logit(m, cand, a.smap, se.px, se.py, se.pz, se.dx, se.dy, se.dz, se.E, se.mat);
                         if ((threadIdx.x & 31) == 0) ++c_inf;
                         if (cand) bk = birth_decision(a, mlp::sigmoid(logit), wexp, se.E, se.mat);
                     }
                 } else if (cand) {
                     ++c_inf;
-                    bk = birth_decision(a, table_importance(a, P.geo.tri, se), wexp, se.E, se.mat);
+                    bk = birth_decision(a, table_importance(a, se), wexp, se.E, se.mat);
                 }
             }
             if (bk > 0) {
@@ -907,7 +907,7 @@ int transport_max_blocks_per_sm(int block, int variant, int mode) {
 
 namespace {
 __global__ void build_surface_map_kernel(const float4* tri, const uint32_t* brick_start, const int32_t* brick_tris,
-                                         int nbx, int nby, int brick, int32_t* map, float lox, float loy, float loz,
+                                         int nbx, int nby, int brick, float4* map, float lox, float loy, float loz,
                                          float cell, int nx, int ny, int nz, float d_max) {
     const uint64_t n = uint64_t(nx) * ny * nz;
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
@@ -924,17 +924,34 @@ __global__ void build_surface_map_kernel(const float4* tri, const uint32_t* bric
                 bi = ti;
             }
         }
-        map[i] = bi;
+        float4 rec = make_float4(0.0f, 0.0f, 0.0f, -1.0f);   // no surface within d_max
+        if (bi >= 0) {
+            // distance to the nearest point q and the unit vector from q to
+            // the centre; at a centre on the surface, the triangle's normal
+            const float4 a = tri[3 * bi], e1 = tri[3 * bi + 1], e2 = tri[3 * bi + 2];
+            float qx, qy, qz;
+            dev::closest_point_on_triangle(px, py, pz, a, e1, e2, &qx, &qy, &qz);
+            const float gx = px - qx, gy = py - qy, gz = pz - qz;
+            const float d = sqrtf(gx * gx + gy * gy + gz * gz);
+            if (d > 0.0f) {
+                rec = make_float4(gx / d, gy / d, gz / d, d);
+            } else {
+                const float nxv = e1.y * e2.z - e1.z * e2.y, nyv = e1.z * e2.x - e1.x * e2.z,
+                            nzv = e1.x * e2.y - e1.y * e2.x;
+                const float inv = rsqrtf(nxv * nxv + nyv * nyv + nzv * nzv + 1e-30f);
+                rec = make_float4(nxv * inv, nyv * inv, nzv * inv, 0.0f);
+            }
+        }
+        map[i] = rec;
     }
 }
 
-__global__ void features_kernel(const dev::Geometry g, const dev::SurfaceMap S, const ElectronRecord* el, uint64_t n,
-                                float* out) {
+__global__ void features_kernel(const dev::SurfaceMap S, const ElectronRecord* el, uint64_t n, float* out) {
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
         const ElectronRecord& r = el[i];
         const dev::V3 d = dev::normalised(dev::V3{r.dir[0], r.dir[1], r.dir[2]});
         float f[6];
-        dev::electron_features(g, S, r.pos[0], r.pos[1], r.pos[2], d.x, d.y, d.z, logf(r.E), r.mat, f);
+        dev::electron_features(S, r.pos[0], r.pos[1], r.pos[2], d.x, d.y, d.z, logf(r.E), r.mat, f);
         for (int k = 0; k < 6; ++k) out[6 * i + k] = f[k];
     }
 }
@@ -947,7 +964,7 @@ cudaError_t launch_triangle_faces(const float4* tri, float4* face, int n, cudaSt
 }
 
 cudaError_t launch_build_surface_map(const float4* tri, const uint32_t* brick_start, const int32_t* brick_tris,
-                                     int nbx, int nby, int brick, int32_t* map, float lox, float loy, float loz,
+                                     int nbx, int nby, int brick, float4* map, float lox, float loy, float loz,
                                      float cell, int nx, int ny, int nz, float d_max, cudaStream_t s) {
     const uint64_t n = uint64_t(nx) * ny * nz;
     if (n == 0) return cudaSuccess;
@@ -956,10 +973,9 @@ cudaError_t launch_build_surface_map(const float4* tri, const uint32_t* brick_st
     return cudaGetLastError();
 }
 
-cudaError_t launch_features(const dev::Geometry& g, const dev::SurfaceMap& S, const void* electrons, uint64_t n,
-                            float* out, cudaStream_t s) {
+cudaError_t launch_features(const dev::SurfaceMap& S, const void* electrons, uint64_t n, float* out, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
-    features_kernel<<<grid_for(n, 128), 128, 0, s>>>(g, S, static_cast<const ElectronRecord*>(electrons), n, out);
+    features_kernel<<<grid_for(n, 128), 128, 0, s>>>(S, static_cast<const ElectronRecord*>(electrons), n, out);
     return cudaGetLastError();
 }
 

@@ -96,8 +96,11 @@ def test_features_vs_bruteforce(inputs, ctx):
         best = np.minimum(best, _pt_tri_dist(P, a, b, c))
     dist = np.minimum(best, 20.0) / 20.0
     err = np.abs(f[:, 1] - dist) * 20.0
-    assert np.mean(err < 1e-3) > 0.9, np.mean(err < 1e-3)
-    assert np.max(err) < 0.9                         # at most about one cell
+    # the map's first-order distance is exact where the point and its cell
+    # centre see the same face of the nearest triangle, and within the cell
+    # (1 nm here) elsewhere
+    assert np.mean(err < 1e-2) > 0.95, np.mean(err < 1e-2)
+    assert np.max(err) < 0.9, np.max(err)
     assert np.allclose(f[:, 0], (np.log(100.0) - 2.5) / 6.5, atol=1e-5)
     assert np.all(f[:, 3] == 1) and np.all(f[:, 4:] == 0)
     assert np.all(np.abs(f[:, 2]) <= 1 + 1e-5)
