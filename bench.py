@@ -467,8 +467,10 @@ def learned_fom(args, tris, mats, local, rank, prim, tags, plain, tmp, tune_samp
         # the cost-aware survival runs without splitting: a split adds
         # near-surface work, the most expensive steps of the scan
         split = 2.0 if policy == "cost" else args.split_threshold
-        ctx.set_mode("learned", rr_threshold=args.rr_threshold, split_threshold=split,
-                     max_roulette_exp=args.max_roulette_exp)
+        # roulette floor: 2^-4 for the cost-aware survival (a deeper floor lets
+        # the rare heavy survivors dominate the variance), 2^-6 for the window
+        max_k = args.max_roulette_exp or (4 if policy == "cost" else 6)
+        ctx.set_mode("learned", rr_threshold=args.rr_threshold, split_threshold=split, max_roulette_exp=max_k)
         if args.birth_rr:
             ctx.set_birth_roulette(*[float(v) for v in args.birth_rr.split(",")])
         cost_info = None
@@ -495,7 +497,7 @@ def learned_fom(args, tris, mats, local, rank, prim, tags, plain, tmp, tune_samp
         ctx.set_birth_roulette(0.0, 0.0, 0.0)
         ctx.set_learned_cost(None, 0.0, 1.0, 1.0)
         # decisions off, network (or table) still consulted for every newborn
-        ctx.set_mode("learned", rr_threshold=1e-30, split_threshold=0.99999, max_roulette_exp=args.max_roulette_exp)
+        ctx.set_mode("learned", rr_threshold=1e-30, split_threshold=0.99999, max_roulette_exp=max_k)
         ctx.reset_tallies()
         ctx.push(prim, tags)
         ctx.run()
@@ -521,7 +523,7 @@ def learned_fom(args, tris, mats, local, rank, prim, tags, plain, tmp, tune_samp
                                   "ns_per_step": 1e6 * s_off["last_run_ms"] / max(s_off["steps"], 1),
                                   "inferences": s_off["inferences"]},
                 "rr_threshold": args.rr_threshold, "split_threshold": split,
-                "max_roulette_exp": args.max_roulette_exp,
+                "max_roulette_exp": max_k,
                 "autotuned": tuned,
                 "inferences": s["inferences"], "roulette_killed": s["roulette_killed"], "splits": s["splits"],
                 "steps": s["steps"], "train_on": list(L["train_on"]), "train_samples": int(len(y)),
@@ -562,8 +564,9 @@ def main():
                     help="learned leg: importance below which a newborn secondary plays roulette")
     ap.add_argument("--split-threshold", type=float, default=0.5,
                     help="learned leg: importance above which a newborn secondary splits in two")
-    ap.add_argument("--max-roulette-exp", type=int, default=6,
-                    help="learned leg: lowest roulette survival is 2^-this")
+    ap.add_argument("--max-roulette-exp", type=int, default=0,
+                    help="learned leg: lowest roulette survival is 2^-this (0: 4 for the cost-aware survival, "
+                         "6 for the weight window)")
     ap.add_argument("--learned-eval", default="table", choices=["table", "fused"],
                     help="learned leg: network tabulated once over its inputs (table) or evaluated on the tensor "
                          "cores for every newborn (fused)")

@@ -319,18 +319,20 @@ def test_learned_fom_gain_on_rough_slab(inputs):
 
     The network is trained on sample-mode records of the slab's scan (one
     primary per pixel, its own seed), tabulated, and drives the cost-aware
-    survival at birth (no splitting).  The fixed rule (born 10 nm or more
-    below the surface under 200 eV: target weight 64) is the comparison.
-    FOM = 1 / (sigma^2 t) of the mean weighted SE yield, sigma^2 the
-    per-primary variance of one run, t its device time; the plain variance
-    is the mean of two runs.
+    survival at birth (no splitting, survival at least 1/16).  The fixed
+    rule (born 10 nm or more below the surface under 200 eV: target weight
+    64) is the comparison.  FOM = 1 / (sigma^2 t) of the mean weighted SE
+    yield, sigma^2 the per-primary variance of one run, t its device time;
+    the plain variance is the mean of two runs.
 
     Checked: both weighted estimates within 3 sigma of the analogue SE and
     BSE yields; both FOM gains above 1.3 in device time; and the network's
-    gain above the rule's when the cost is counted in transport steps (it
-    removes more work at a small variance price).  In device time the two
-    are about equal (1.7-1.9x): the extra steps the network removes are deep
-    ones, which cost a quarter of a near-surface step."""
+    gain above the rule's, in device time and with the cost counted in
+    transport steps (measured: 2.17x against 1.87x in time, 5.8x against
+    4.1x in steps; the seeds are fixed, so only the timing varies from run
+    to run).  The gain in time stays well below the one in steps because
+    the work removed is deep, cheap steps: a near-surface step, which
+    carries the signal, costs three to four times as much."""
     w = g.SCANS["rough"]
     tris = w["geometry"]()
     recs = g.scan_beam(w["nx"], w["ny"], w["per_pixel"], w["energy"], spacing=w["spacing"], origin=w["origin"],
@@ -374,7 +376,7 @@ def test_learned_fom_gain_on_rough_slab(inputs):
     table, lo, hi = nb.fit_cost_table(f, cost)
     ctx.set_importance_table(48, 32, 16)
     ctx.set_learned_cost(table, lo, hi, (steps_p / n) / var_p)
-    net = run("learned", rr_threshold=0.05, split_threshold=2.0)
+    net = run("learned", rr_threshold=0.05, split_threshold=2.0, max_roulette_exp=4)
     ctx.set_importance_table(0, 0, 0)
     ctx.set_learned_cost(None, 0.0, 1.0, 1.0)
     ctx.set_birth_roulette(10.0, 200.0, 1.0 / 64)
@@ -388,4 +390,5 @@ def test_learned_fom_gain_on_rough_slab(inputs):
             assert abs(z) < 3, (name, z)
         gains[name] = ((var_p * ms_p) / (se.var() * s["last_run_ms"]), (var_p * steps_p) / (se.var() * s["steps"]))
     assert gains["network"][0] > 1.3 and gains["rule"][0] > 1.3, gains
+    assert gains["network"][0] > gains["rule"][0], gains
     assert gains["network"][1] > gains["rule"][1], gains
