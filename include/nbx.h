@@ -249,6 +249,19 @@ int nbx_add_material(nbx_ctx* ctx, const nbx_material* mat);
 int nbx_set_tag_range(nbx_ctx* ctx, uint64_t n_tags);
 /* Queue primaries (host buffers).  *accepted <= n is how many fit. */
 int nbx_push(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n, uint64_t* accepted);
+/* Staged push (no counterpart in the reference, whose frame loop copies the
+ * next frame's primaries from pinned buffers while a frame runs,
+ * gpu_driver.inl:167-306): nbx_stage starts copying a batch (host arrays as
+ * for nbx_push) to the device on the context's copy stream and returns at
+ * once, so the copy can overlap a following nbx_run; nbx_push_staged then
+ * queues it on the device (tags checked there) exactly as nbx_push would
+ * have, with the random-stream index running on from the primaries pushed
+ * before it.  The host arrays must stay unchanged until nbx_push_staged
+ * returns; the copy overlaps only from page-locked host memory.  One batch
+ * at a time: nbx_stage with a batch still staged returns NBX_ERR_STATE;
+ * nbx_push_staged with nothing staged queues nothing (*accepted = 0). */
+int nbx_stage(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n);
+int nbx_push_staged(nbx_ctx* ctx, uint64_t* accepted);
 /* Random-stream index of the next pushed primary (default: running count of
  * pushed primaries).  Replicas on several GPUs set it to the global index of
  * their first primary so the combined result does not depend on sharding. */

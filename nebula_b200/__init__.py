@@ -170,6 +170,8 @@ def lib():
         "nbx_mlp_predict": (C.c_int, [_vp, _vp, C.c_uint64, _vp]),
         "nbx_autotune": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.POINTER(Tuning)]),
         "nbx_set_tuning": (C.c_int, [_vp, C.POINTER(Tuning)]),
+        "nbx_stage": (C.c_int, [_vp, _vp, _vp, C.c_uint64]),
+        "nbx_push_staged": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
         "nbx_set_learned_cost": (C.c_int, [_vp, _vp, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float]),
         "nbx_set_importance_table": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32]),
         "nbx_get_tuning": (C.c_int, [_vp, C.POINTER(Tuning)]),
@@ -334,6 +336,20 @@ class Context:
         t = np.ascontiguousarray(tags, np.uint32)
         acc = C.c_uint64()
         self._ck(self.L.nbx_push(self.h, _ptr(p), _ptr(t), len(t), C.byref(acc)))
+        return acc.value
+
+    def stage(self, particles: np.ndarray, tags: np.ndarray):
+        """Start copying a batch to the device (nbx_stage); keep the arrays
+        alive and unchanged until push_staged() returns."""
+        p = np.ascontiguousarray(particles, np.float32).reshape(-1, 7)
+        t = np.ascontiguousarray(tags, np.uint32)
+        self._staged = (p, t)
+        self._ck(self.L.nbx_stage(self.h, _ptr(p), _ptr(t), len(t)))
+
+    def push_staged(self) -> int:
+        acc = C.c_uint64()
+        self._ck(self.L.nbx_push_staged(self.h, C.byref(acc)))
+        self._staged = None
         return acc.value
 
     def push_records(self, recs: np.ndarray, first_tag=0) -> int:

@@ -112,6 +112,15 @@ struct nbx_ctx {
     uint64_t uid_next = 0;
     DevBuf<float> stage_p;
     DevBuf<uint32_t> stage_t;
+    // staged batch (nbx_stage): copied on its own stream while a run may be
+    // in flight, queued by nbx_push_staged
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t staged_ev = nullptr;
+    DevBuf<float> staged_p;
+    DevBuf<uint32_t> staged_t;
+    DevBuf<uint32_t> staged_max;
+    uint64_t staged_n = 0;
+    bool staged_pending = false;
     DevBuf<uint32_t> ctl;       // head[G], tail[G], n_primary
     // tallies
     DevBuf<uint32_t> se_count, bse_count;
@@ -171,6 +180,8 @@ struct nbx_ctx {
         for (auto* t : tables) delete t;
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (staged_ev) cudaEventDestroy(staged_ev);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -553,6 +564,7 @@ int nbx_create(nbx_ctx** out, const nbx_config* cfg) {
 void nbx_destroy(nbx_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->cfg.device);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     delete ctx;
 }
@@ -646,6 +658,28 @@ int nbx_set_tag_range(nbx_ctx* ctx, uint64_t n_tags) {
     });
 }
 
+namespace {
+// Room for n more primaries in the primary queue (grown, keeping the queued ones).
+void ensure_primary_room(nbx_ctx* ctx, uint64_t n) {
+    if (ctx->prim.cap >= ctx->n_queued + n) return;
+    QueueBuf nq;
+    nq.ensure(std::max<uint64_t>(ctx->n_queued + n, 2 * ctx->prim.cap));
+    if (ctx->n_queued) {
+        ck(cudaMemcpyAsync(nq.a.p, ctx->prim.a.p, 16 * ctx->n_queued, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+        ck(cudaMemcpyAsync(nq.b.p, ctx->prim.b.p, 16 * ctx->n_queued, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+        ck(cudaMemcpyAsync(nq.c.p, ctx->prim.c.p, 16 * ctx->n_queued, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+        ck(cudaStreamSynchronize(ctx->stream), "sync");
+    }
+    std::swap(ctx->prim.a.p, nq.a.p);
+    std::swap(ctx->prim.a.n, nq.a.n);
+    std::swap(ctx->prim.b.p, nq.b.p);
+    std::swap(ctx->prim.b.n, nq.b.n);
+    std::swap(ctx->prim.c.p, nq.c.p);
+    std::swap(ctx->prim.c.n, nq.c.n);
+    std::swap(ctx->prim.cap, nq.cap);
+}
+}  // namespace
+
 int nbx_push(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n, uint64_t* accepted) {
     if (!ctx || (n && (!particles || !tags))) return NBX_ERR_ARG;
     return guarded(ctx, [&] {
@@ -655,24 +689,7 @@ int nbx_push(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, 
         uint32_t max_tag = 0;
         for (uint64_t i = 0; i < n; ++i) max_tag = std::max(max_tag, tags[i]);
         ensure_tags(ctx, uint64_t(max_tag) + 1);
-        if (ctx->prim.cap < ctx->n_queued + n) {
-            // grow, keeping queued primaries
-            QueueBuf nq;
-            nq.ensure(std::max<uint64_t>(ctx->n_queued + n, 2 * ctx->prim.cap));
-            if (ctx->n_queued) {
-                ck(cudaMemcpyAsync(nq.a.p, ctx->prim.a.p, 16 * ctx->n_queued, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
-                ck(cudaMemcpyAsync(nq.b.p, ctx->prim.b.p, 16 * ctx->n_queued, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
-                ck(cudaMemcpyAsync(nq.c.p, ctx->prim.c.p, 16 * ctx->n_queued, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
-                ck(cudaStreamSynchronize(ctx->stream), "sync");
-            }
-            std::swap(ctx->prim.a.p, nq.a.p);
-            std::swap(ctx->prim.a.n, nq.a.n);
-            std::swap(ctx->prim.b.p, nq.b.p);
-            std::swap(ctx->prim.b.n, nq.b.n);
-            std::swap(ctx->prim.c.p, nq.c.p);
-            std::swap(ctx->prim.c.n, nq.c.n);
-            std::swap(ctx->prim.cap, nq.cap);
-        }
+        ensure_primary_room(ctx, n);
         ctx->stage_p.ensure(7 * n);
         ctx->stage_t.ensure(n);
         ck(cudaMemcpyAsync(ctx->stage_p.p, particles, sizeof(float) * 7 * n, cudaMemcpyHostToDevice, ctx->stream), "H2D");
@@ -732,6 +749,57 @@ int nbx_set_importance_table(nbx_ctx* ctx, int32_t n_energy, int32_t n_distance,
         ctx->imp_nd = n_distance;
         ctx->imp_nc = n_cosine;
         build_importance_table(ctx);
+        return NBX_OK;
+    });
+}
+
+int nbx_stage(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n) {
+    if (!ctx || (n && (!particles || !tags))) return NBX_ERR_ARG;
+    if (ctx->staged_pending) return fail(ctx, NBX_ERR_STATE, "nbx_stage: a staged batch waits for nbx_push_staged");
+    return guarded(ctx, [&] {
+        if (!ctx->copy_stream) {
+            ck(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "stream");
+            ck(cudaEventCreateWithFlags(&ctx->staged_ev, cudaEventDisableTiming), "event");
+        }
+        ctx->staged_p.ensure(std::max<uint64_t>(7 * n, 1));
+        ctx->staged_t.ensure(std::max<uint64_t>(n, 1));
+        if (n) {
+            ck(cudaMemcpyAsync(ctx->staged_p.p, particles, sizeof(float) * 7 * n, cudaMemcpyHostToDevice,
+                               ctx->copy_stream), "H2D");
+            ck(cudaMemcpyAsync(ctx->staged_t.p, tags, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, ctx->copy_stream),
+               "H2D");
+        }
+        ck(cudaEventRecord(ctx->staged_ev, ctx->copy_stream), "event");
+        ctx->staged_n = n;
+        ctx->staged_pending = true;
+        return NBX_OK;
+    });
+}
+
+int nbx_push_staged(nbx_ctx* ctx, uint64_t* accepted) {
+    if (!ctx) return NBX_ERR_ARG;
+    if (accepted) *accepted = 0;
+    if (!ctx->staged_pending) return NBX_OK;
+    return guarded(ctx, [&] {
+        const uint64_t n = ctx->staged_n;
+        ck(cudaStreamWaitEvent(ctx->stream, ctx->staged_ev, 0), "wait");
+        ctx->staged_pending = false;
+        if (n == 0) return NBX_OK;
+        if (ctx->n_queued + n > 0xFFFFFFF0ull) throw ApiError(NBX_ERR_CAPACITY, "primary queue limited to 2^32 entries");
+        ctx->staged_max.ensure(1);
+        ck(cudaMemsetAsync(ctx->staged_max.p, 0, 4, ctx->stream), "memset");
+        ck(nbx::launch_max_tag(ctx->staged_t.p, n, ctx->staged_max.p, ctx->stream), "max tag");
+        uint32_t max_tag = 0;
+        to_host(ctx, &max_tag, ctx->staged_max.p, 4, "D2H");
+        ensure_tags(ctx, uint64_t(max_tag) + 1);
+        ensure_primary_room(ctx, n);
+        ck(nbx::launch_fill_queue(ctx->prim.q(), ctx->staged_p.p, ctx->staged_t.p, ctx->uid_next, n, ctx->n_queued,
+                                  ctx->stream), "fill");
+        ck(cudaStreamSynchronize(ctx->stream), "sync");
+        ctx->uid_next += n;
+        ctx->n_queued += n;
+        ctx->pushed += n;
+        if (accepted) *accepted = n;
         return NBX_OK;
     });
 }

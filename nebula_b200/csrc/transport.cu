@@ -789,6 +789,16 @@ __global__ void fill_queue_kernel(Queue q, const float* particles, const uint32_
     }
 }
 
+// Largest of n tags into *out (zeroed by the caller).
+__global__ void max_tag_kernel(const uint32_t* v, uint64_t n, uint32_t* out) {
+    uint32_t m = 0;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+        m = max(m, v[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
 int grid_for(uint64_t n, int block) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -1023,6 +1033,12 @@ cudaError_t launch_pixel_yields(const uint32_t* se, const uint32_t* bse, const f
     if (n_tags == 0) return cudaSuccess;
     pixel_yields_kernel<<<grid_for(n_tags, 256), 256, 0, s>>>(se, bse, se_w, bse_w, pixel_of_tag, n_tags, n_pixels,
                                                               out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_max_tag(const uint32_t* tags, uint64_t n, uint32_t* out, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    max_tag_kernel<<<grid_for(n, 256), 256, 0, s>>>(tags, n, out);
     return cudaGetLastError();
 }
 

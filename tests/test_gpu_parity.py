@@ -501,3 +501,49 @@ def test_learned_pixel_yields_are_weighted(inputs):
     np.add.at(ref[:, 4], pix, bse.astype(float) ** 2)
     assert np.allclose(w, ref)
     ctx.close()
+
+
+def test_staged_push_equals_push(inputs):
+    """nbx_stage + nbx_push_staged queue a batch exactly as nbx_push: the
+    same per-tag counts and event totals for the same random streams, with a
+    run in between them (the copy then overlaps it) and with tags beyond the
+    range tallied so far (the tag range is checked on the device).  A second
+    nbx_stage before nbx_push_staged is refused; nbx_push_staged with nothing
+    staged queues nothing."""
+    recs = g.scan_beam(32, 32, 20, 500.0, origin=(-16.0, -16.0), seed=17)
+    n = len(recs)
+    prim = np.zeros((n, 7), np.float32)
+    prim[:, 0:3] = recs["pos"]
+    prim[:, 3:6] = recs["dir"]
+    prim[:, 6] = recs["E"]
+    half = n // 2
+    tags = np.arange(n, dtype=np.uint32)
+
+    a = nb.setup(inputs["grating_small"], [inputs["si"]], device=0, seed=71)
+    a.set_tag_range(half)
+    a.push(prim[:half], tags[:half])
+    a.run()
+    a.push(prim[half:], tags[half:])
+    a.run()
+    sa = a.stats()
+    se_a, bse_a = a.tag_counts(0, n)
+    a.close()
+
+    b = nb.setup(inputs["grating_small"], [inputs["si"]], device=0, seed=71)
+    b.set_tag_range(half)
+    assert b.push_staged() == 0
+    b.stage(prim[:half], tags[:half])
+    with pytest.raises(nb.NbxError) as e:
+        b.stage(prim[half:], tags[half:])
+    assert e.value.code == -6
+    assert b.push_staged() == half
+    b.stage(prim[half:], tags[half:])     # copied while the first half runs
+    b.run()
+    assert b.push_staged() == n - half    # tags beyond the first half's range
+    b.run()
+    sb = b.stats()
+    se_b, bse_b = b.tag_counts(0, n)
+    b.close()
+    assert np.array_equal(se_a, se_b) and np.array_equal(bse_a, bse_b)
+    for k in ("primaries_done", "steps", "events_elastic", "events_inelastic", "events_boundary", "detected"):
+        assert sa[k] == sb[k], k
