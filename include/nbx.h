@@ -3,7 +3,8 @@
  * C ABI of the drop-in hot path.  Plain pointers and sizes only; no C++ types
  * or exceptions cross it.  Every call returns NBX_OK (0) or a negative
  * NBX_ERR_* code; nbx_last_error() gives a message for the last failing call
- * on a context.  One context per GPU, driven by one host thread (the
+ * on a context, and nbx_last_error(NULL) the message of the calling thread's
+ * last failing call that takes no context (material loading, octree build).  One context per GPU, driven by one host thread (the
  * reference's worker_thread model, source/gpu_main.cu:77-218); a context is
  * not re-entrant.
  *

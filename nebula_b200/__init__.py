@@ -188,7 +188,7 @@ def lib():
 
 def _check(rc, ctx=None):
     if rc != NBX_OK:
-        msg = lib().nbx_last_error(ctx).decode() if ctx else ""
+        msg = lib().nbx_last_error(ctx).decode()
         raise NbxError(rc, msg)
 
 

@@ -188,14 +188,19 @@ struct nbx_ctx {
 
 namespace {
 
+// Calls without a context (file loaders, octree build) keep their message
+// per host thread; nbx_last_error(NULL) returns it.
+thread_local std::string g_thread_err;
+
 int fail(nbx_ctx* ctx, int code, const std::string& msg) {
-    if (ctx) ctx->err = msg;
+    (ctx ? ctx->err : g_thread_err) = msg;
     return code;
 }
 
 template <typename F>
 int guarded(nbx_ctx* ctx, F&& f) {
     try {
+        if (!ctx) g_thread_err.clear();
         if (ctx) {
             ctx->err.clear();
             if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return fail(ctx, NBX_ERR_CUDA, "cudaSetDevice failed");
@@ -569,7 +574,7 @@ void nbx_destroy(nbx_ctx* ctx) {
     delete ctx;
 }
 
-const char* nbx_last_error(nbx_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+const char* nbx_last_error(nbx_ctx* ctx) { return ctx ? ctx->err.c_str() : g_thread_err.c_str(); }
 
 int nbx_set_geometry(nbx_ctx* ctx, const nbx_octree* o) {
     if (!ctx || !o || !o->octree_data || o->n_octree < 8 || !o->triangles) return NBX_ERR_ARG;
