@@ -74,7 +74,7 @@ WORKLOADS = {
     "holes": dict(rows=64, tune_row=8, cpu_sample=204800, ref_sample=102400,
                   # the map covers the default 64 pixel rows (y up to -1121 nm)
                   learned=dict(map_lo=(-1290, -1290, -170), map_hi=(1290, -1100, 25), cell=2.0, d_max=10.0,
-                               train_per_pixel=1, train_rows=64, train_on=("holes",), policy="cost"),
+                               train_per_pixel=8, train_rows=64, train_on=("holes",), policy="cost"),
                   desc="contact holes: 32x32 holes (40 nm diameter, 100 nm deep, +-2 nm edge roughness) in a "
                        "SiO2-like film over W-like plugs on a Si-like substrate, 2,506,772 triangles over "
                        "2.56 um; 1024x1024 px at 2.5 nm x 200 primaries at 1 keV, one step = %d pixel rows "
