@@ -182,7 +182,7 @@ typedef struct {
     uint64_t record_capacity;  /* detected records held on the device; 0 = auto */
     int32_t block_size;        /* threads per block of the transport kernel; 0 = 256 */
     int32_t blocks_per_sm;     /* transport variant: 2, 3 or 4 resident 256-thread blocks per SM, or 7
-                                  128-thread blocks (block_size capped at 128); 0 = 3 */
+                                  128-thread blocks (block_size capped at 128); 0 = 4 (64 registers) */
     int32_t inelastic_model;   /* NBX_INELASTIC_KIEFT (0, default) or NBX_INELASTIC_FULL_PENN */
     int32_t record_deposits;   /* keep energy-deposit records (plain mode; cpu_energydep.cpp) */
     uint64_t deposit_capacity; /* deposit records held on the device; 0 = 2^27 (3.2 GB) */
@@ -263,6 +263,12 @@ int nbx_push(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, 
  * nbx_push_staged with nothing staged queues nothing (*accepted = 0). */
 int nbx_stage(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags, uint64_t n);
 int nbx_push_staged(nbx_ctx* ctx, uint64_t* accepted);
+/* Page-locked host memory for nbx_stage's arrays (no counterpart in the
+ * reference, which pins its frame buffers inside the driver): usable by
+ * every context of the process.  NBX_ERR_OOM (and *out = NULL) when the
+ * allocation fails; nbx_host_free(NULL) does nothing. */
+int nbx_host_alloc(uint64_t bytes, void** out);
+void nbx_host_free(void* p);
 /* Random-stream index of the next pushed primary (default: running count of
  * pushed primaries).  Replicas on several GPUs set it to the global index of
  * their first primary so the combined result does not depend on sharding. */
@@ -280,7 +286,11 @@ int nbx_get_stats(nbx_ctx* ctx, nbx_stats* out);
  * record_deposits; runs whose records overflow deposit_capacity count the
  * lost ones in nbx_stats.deposits_dropped. */
 int nbx_flush_deposits(nbx_ctx* ctx, nbx_deposit* out, uint64_t capacity, uint64_t* n);
-/* Copy out (and remove) up to cap detected electrons. */
+/* Copy out (and remove) up to cap detected electrons, oldest first; call
+ * again until *n comes back 0.  The device keeps them in this struct's
+ * layout, so a call is one device-to-host copy straight into `out` (a DMA
+ * when `out` is page-locked, nbx_host_alloc).  A run while records are
+ * still pending appends to them. */
 int nbx_flush_detected(nbx_ctx* ctx, nbx_detected* out, uint64_t cap, uint64_t* n);
 /* Detections per primary tag below / at-or-above 50 eV. */
 int nbx_get_tag_counts(nbx_ctx* ctx, uint64_t first_tag, uint64_t n, uint32_t* se, uint32_t* bse);

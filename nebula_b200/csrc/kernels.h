@@ -60,8 +60,8 @@ struct TransportArgs {
     uint32_t* bse_count;        // per-tag detections at or above 50 eV
     uint64_t n_tags;
     unsigned long long* counters;
-    float4* rec_a;              // detected records: (pos, E), (dir, tag bits)
-    float4* rec_b;
+    float4* rec;                // detected records in nbx_detected's layout, two float4 each:
+                                //   (pos, dir.x), (dir.y, dir.z, E, tag bits)
     uint32_t* rec_count;
     uint32_t rec_capacity;
     unsigned long long* hist;   // detected-energy histogram

@@ -12,9 +12,11 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <iostream>
 #include <map>
 #include <mutex>
@@ -188,6 +190,62 @@ struct PriSource {
     }
 };
 
+// Hand-off of buffers between threads: pop() waits for an item; once the
+// queue is closed it returns what is left, then nullptr.
+template <typename T>
+class Handoff {
+public:
+    void push(T* x) {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            q_.push_back(x);
+        }
+        cv_.notify_one();
+    }
+    T* pop() {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return !q_.empty() || closed_; });
+        if (q_.empty()) return nullptr;
+        T* x = q_.front();
+        q_.pop_front();
+        return x;
+    }
+    void close() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            closed_ = true;
+        }
+        cv_.notify_all();
+    }
+
+private:
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<T*> q_;
+    bool closed_ = false;
+};
+
+// One batch of primaries on the host: the particles and batch-relative tags
+// in page-locked memory (so nbx_stage's copy overlaps a running batch) and
+// each primary's pixel, which its detected records carry.
+struct HostBatch {
+    uint64_t first = 0, n = 0;
+    nbx_particle* part = nullptr;
+    uint32_t* tags = nullptr;
+    std::vector<int32_t> px, py;
+};
+
+// Detected records of one batch on their way to the output: read back from
+// the device into page-locked memory (the library's layout; the rare records
+// beyond `cap` into `more`) and turned into the reference's 36-byte records
+// by the writer thread, with the pixel of the primary each one came from.
+struct OutBatch {
+    nbx_detected* det = nullptr;
+    uint64_t cap = 0, n = 0;
+    std::vector<nbx_detected> more;
+    HostBatch* src = nullptr;
+};
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -201,7 +259,7 @@ int main(int argc, char** argv) {
     p.add("seed", "Random seed", std::to_string(0x78c7e39b));
     p.add("sort-primaries", "Sort primary electrons before simulation", "0");
     p.add("device", "CUDA device ordinal", "0");
-    p.add("streams", "Device contexts working on batches at once (one with --energy-deposit)", "4");
+    p.add("streams", "Device contexts, each with its own pipeline of batches (one with --energy-deposit)", "1");
     p.add("inelastic", "Inelastic model: kieft (Kieft & Bosch) or penn (full Penn, the reference's stock build)",
           "kieft");
     p.add("energy-deposit", "Also write energy deposits, as the reference's nebula_cpu_energydep", "0");
@@ -338,8 +396,8 @@ int main(int argc, char** argv) {
     cfg.record_detected = 1;
     cfg.record_capacity = 1ull << 24;
     cfg.record_deposits = energy_deposit ? 1 : 0;
-    // Several contexts on the one device: while one drains the last long
-    // cascades of its batch, the next batch's kernel fills the freed SMs.
+    // --streams contexts on the one device, each running its own pipeline
+    // of batches (below); one keeps the device busy already.
     const int n_ctx = energy_deposit ? 1 : streams;
     std::vector<nbx_ctx*> ctxs;
     for (int k = 0; k < n_ctx; ++k) {
@@ -377,13 +435,13 @@ int main(int argc, char** argv) {
     static_assert(sizeof(DepositRecord) == 28, "deposit record layout");
     const uint64_t dep_capacity = uint64_t(1) << 27;   // nbx_config default
 
-    // Worker threads, one per context, claim the next batch of the file (in
-    // order, under a lock), read it with a positional read, run it and write
-    // its records (under a second lock).  A batch's primaries keep their
-    // global index as the uid of their random streams, so the records do not
-    // depend on the number of workers or on which worker ran a batch; only
-    // their order in the output does, as with the reference's worker threads.
-    // Tags are batch-relative.
+    // Energy-deposit mode: one worker claims the next batch of the file, reads
+    // it with a positional read, runs it and writes its records, then sizes
+    // the next batch from the deposits per primary seen so far.  In every
+    // mode a batch's primaries keep their global index as the uid of their
+    // random streams, so the records depend neither on the batch size nor on
+    // the number of contexts; only their order in the output does, as with
+    // the reference's worker threads.  Tags are batch-relative.
     struct Batch {
         uint64_t first = 0, n = 0;
         std::vector<nbx_record> pri;
@@ -491,12 +549,159 @@ int main(int argc, char** argv) {
             std::fprintf(stderr, " \rProgress %.2f%%", 100.0 * double(done) / double(n_pri));
         }
     };
+
+    // Plain mode: a pipeline that keeps the device busy.  A reader thread
+    // reads batches ahead of the device into page-locked buffers.  Each
+    // context's thread starts the copy of its next batch (nbx_stage) before it
+    // runs the current one, so the copy overlaps the run (the reference's
+    // frame loop overlaps its copies the same way, gpu_driver.inl:167-306);
+    // after the run it collects the batch's records and queues the next batch
+    // (nbx_push_staged).  A writer thread writes the records in the order the
+    // batches finish.  The device only waits for the record read-back and the
+    // queueing between two runs.
+    Handoff<HostBatch> ready, free_batches;
+    Handoff<OutBatch> written, free_out;
+    std::vector<HostBatch> host_batches(energy_deposit ? 0 : size_t(2 * n_ctx + 3));
+    std::vector<OutBatch> out_batches(energy_deposit ? 0 : size_t(2 * n_ctx + 2));
+    auto close_all = [&] {
+        ready.close();
+        free_batches.close();
+        written.close();
+        free_out.close();
+    };
+    // Page-locked buffers are allocated where they are first needed, off the
+    // device's critical path: the reader's on first use, the read-back
+    // buffers by the writer thread as it starts.
+    const uint64_t buf_n = std::min(batch, n_pri);
+    auto reader = [&] {
+        std::vector<nbx_record> raw;
+        for (uint64_t first = 0; first < n_pri; first += batch) {
+            HostBatch* b = free_batches.pop();
+            if (!b) return;
+            if (!b->part) {
+                void* p = nullptr;
+                void* t = nullptr;
+                if (nbx_host_alloc(sizeof(nbx_particle) * buf_n, &p) != NBX_OK ||
+                    nbx_host_alloc(sizeof(uint32_t) * buf_n, &t) != NBX_OK) {
+                    nbx_host_free(p);
+                    fail_with(nullptr, NBX_ERR_OOM, "page-locked batch buffers (lower --capacity)");
+                    return close_all();
+                }
+                b->part = static_cast<nbx_particle*>(p);
+                b->tags = static_cast<uint32_t*>(t);
+            }
+            b->first = first;
+            b->n = std::min(batch, n_pri - first);
+            raw.resize(b->n);
+            if (!src.read(first, b->n, raw.data())) {
+                std::fprintf(stderr, "Error: could not read primary electrons!\n");
+                fail_with(nullptr, NBX_ERR_FORMAT, "primaries");
+                return close_all();
+            }
+            if (!sort_primaries) warn.add(raw.data(), b->n);
+            b->px.resize(b->n);
+            b->py.resize(b->n);
+            for (uint64_t i = 0; i < b->n; ++i) {
+                std::memcpy(b->part[i].pos, raw[i].pos, 12);
+                std::memcpy(b->part[i].dir, raw[i].dir, 12);
+                b->part[i].E = raw[i].E;
+                b->tags[i] = uint32_t(i);
+                b->px[i] = raw[i].px;
+                b->py[i] = raw[i].py;
+            }
+            ready.push(b);
+        }
+        for (int k = 0; k < n_ctx; ++k) ready.push(nullptr);   // one end mark per context
+    };
+    auto pipeline = [&](nbx_ctx* c) {
+        auto failed = [&](int code, const char* what) {
+            fail_with(c, code, what);
+            close_all();
+        };
+        HostBatch* cur = ready.pop();
+        if (!cur) return;
+        int r;
+        if ((r = nbx_set_uid_base(c, cur->first)) != NBX_OK) return failed(r, "uid base");
+        if ((r = nbx_stage(c, cur->part, cur->tags, cur->n)) != NBX_OK) return failed(r, "stage");
+        if ((r = nbx_push_staged(c, nullptr)) != NBX_OK) return failed(r, "push");
+        for (;;) {
+            HostBatch* next = ready.pop();
+            if (next && (r = nbx_stage(c, next->part, next->tags, next->n)) != NBX_OK) return failed(r, "stage");
+            if ((r = nbx_run(c)) != NBX_OK) return failed(r, "run");
+            OutBatch* o = free_out.pop();
+            if (!o) return;
+            o->n = 0;
+            o->more.clear();
+            o->src = cur;
+            for (;;) {
+                uint64_t got = 0;
+                if (o->n < o->cap) {
+                    if ((r = nbx_flush_detected(c, o->det + o->n, o->cap - o->n, &got)) != NBX_OK)
+                        return failed(r, "flush");
+                    o->n += got;
+                } else {
+                    const size_t base = o->more.size();
+                    o->more.resize(base + (1u << 20));
+                    if ((r = nbx_flush_detected(c, o->more.data() + base, 1u << 20, &got)) != NBX_OK)
+                        return failed(r, "flush");
+                    o->more.resize(base + got);
+                }
+                if (got == 0) break;
+            }
+            written.push(o);
+            if (!next) return;
+            if ((r = nbx_set_uid_base(c, next->first)) != NBX_OK) return failed(r, "uid base");
+            if ((r = nbx_push_staged(c, nullptr)) != NBX_OK) return failed(r, "push");
+            cur = next;
+        }
+    };
+    auto writer = [&] {
+        for (OutBatch& o : out_batches) {
+            void* d = nullptr;
+            if (nbx_host_alloc(sizeof(nbx_detected) * buf_n, &d) != NBX_OK) {
+                fail_with(nullptr, NBX_ERR_OOM, "page-locked record buffers (lower --capacity)");
+                return close_all();
+            }
+            o.det = static_cast<nbx_detected*>(d);
+            o.cap = buf_n;
+            free_out.push(&o);
+        }
+        std::vector<nbx_record> out;
+        for (;;) {
+            OutBatch* o = written.pop();
+            if (!o) return;
+            const HostBatch* b = o->src;
+            out.resize(o->n + o->more.size());
+            for (size_t i = 0; i < out.size(); ++i) {
+                const nbx_detected& d = i < o->n ? o->det[i] : o->more[i - o->n];
+                nbx_record& rec = out[i];
+                std::memcpy(rec.pos, d.pos, 12);
+                std::memcpy(rec.dir, d.dir, 12);
+                rec.E = d.E;
+                rec.px = b->px[d.tag];
+                rec.py = b->py[d.tag];
+            }
+            if (!out.empty()) std::fwrite(out.data(), sizeof(nbx_record), out.size(), detect_out);
+            done += b->n;
+            std::fprintf(stderr, " \rProgress %.2f%%", 100.0 * double(done) / double(n_pri));
+            free_batches.push(o->src);
+            free_out.push(o);
+        }
+    };
+
     timer.start();
-    {
+    if (energy_deposit) {
+        worker(ctxs[0], warns[0]);
+        warn.merge(warns[0]);
+    } else {
+        for (HostBatch& b : host_batches) free_batches.push(&b);
+        std::thread out_thread(writer);
         std::vector<std::thread> threads;
-        for (size_t k = 0; k < ctxs.size(); ++k) threads.emplace_back(worker, ctxs[k], std::ref(warns[k]));
+        threads.emplace_back(reader);
+        for (nbx_ctx* c : ctxs) threads.emplace_back(pipeline, c);
         for (auto& t : threads) t.join();
-        for (const auto& w : warns) warn.merge(w);
+        written.close();   // every context has handed over its last batch
+        out_thread.join();
     }
     if (failed_rc != NBX_OK) {
         const int r = die(failed_ctx, failed_rc, failed_what.c_str());
@@ -530,6 +735,11 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "\n\n");
     timer.print();
     for (nbx_ctx* c : ctxs) nbx_destroy(c);
+    for (HostBatch& b : host_batches) {
+        nbx_host_free(b.part);
+        nbx_host_free(b.tags);
+    }
+    for (OutBatch& o : out_batches) nbx_host_free(o.det);
     for (auto* m : mats) nbx_material_free(m);
     nbx_octree_free(oct);
     return 0;

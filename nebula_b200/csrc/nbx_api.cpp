@@ -127,7 +127,7 @@ struct nbx_ctx {
     uint64_t n_tags = 0;
     DevBuf<unsigned long long> counters;
     DevBuf<unsigned long long> hist;
-    DevBuf<float4> rec_a, rec_b;
+    DevBuf<float4> rec;   // detected records, two float4 each in nbx_detected's layout
     DevBuf<uint32_t> rec_count;
     // escape-probability network: FP32 master parameters, Adam moments, gradient
     DevBuf<float> mlp_params, mlp_m, mlp_v, mlp_grad, mlp_loss;
@@ -165,6 +165,7 @@ struct nbx_ctx {
     float spec_width = 0;
     DevBuf<double> yield_out;
     uint64_t rec_cap = 0;
+    uint64_t rec_read = 0;   // records [0, rec_read) already flushed
     // stats
     uint64_t pushed = 0, generations = 0;
     double last_run_ms = 0, last_kernel_ms = 0;
@@ -232,12 +233,6 @@ static void to_device(nbx_ctx* ctx, void* dst, const void* src, size_t bytes, co
 static void to_host(nbx_ctx* ctx, void* dst, const void* src, size_t bytes, const char* what) {
     if (!bytes) return;
     ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream), what);
-    ck(cudaStreamSynchronize(ctx->stream), what);
-}
-
-static void on_device(nbx_ctx* ctx, void* dst, const void* src, size_t bytes, const char* what) {
-    if (!bytes) return;
-    ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, ctx->stream), what);
     ck(cudaStreamSynchronize(ctx->stream), what);
 }
 
@@ -534,8 +529,9 @@ int nbx_create(nbx_ctx** out, const nbx_config* cfg) {
         if (ctx->block % 32 != 0 || ctx->block > 256) throw ApiError(NBX_ERR_ARG, "block_size must be a multiple of 32, <= 256");
         // Kernel variant = resident blocks per SM it was register-limited for:
         // 2, 3 or 4 blocks of 256 threads, or 7 blocks of 128 (72 registers;
-        // block size capped at 128); default 3 (80 registers).
-        ctx->variant = ((c.blocks_per_sm >= 2 && c.blocks_per_sm <= 4) || c.blocks_per_sm == 7) ? c.blocks_per_sm : 3;
+        // block size capped at 128); default 4 (64 registers: the
+        // autotuner's choice on most workloads).
+        ctx->variant = ((c.blocks_per_sm >= 2 && c.blocks_per_sm <= 4) || c.blocks_per_sm == 7) ? c.blocks_per_sm : 4;
         if (ctx->variant == 7 && ctx->block > 128) ctx->block = 128;
         ctx->bpsm = nbx::transport_max_blocks_per_sm(ctx->block, ctx->variant);
         if (c.record_deposits) {
@@ -546,8 +542,7 @@ int nbx_create(nbx_ctx** out, const nbx_config* cfg) {
         }
         if (c.record_detected) {
             ctx->rec_cap = c.record_capacity ? c.record_capacity : (1ull << 24);
-            ctx->rec_a.alloc(ctx->rec_cap);
-            ctx->rec_b.alloc(ctx->rec_cap);
+            ctx->rec.alloc(2 * ctx->rec_cap);
         }
         ctx->phys.seed = c.seed;
         ctx->phys.min_energy = c.energy_threshold;
@@ -781,6 +776,22 @@ int nbx_stage(nbx_ctx* ctx, const nbx_particle* particles, const uint32_t* tags,
     });
 }
 
+int nbx_host_alloc(uint64_t bytes, void** out) {
+    if (!out) return NBX_ERR_ARG;
+    *out = nullptr;
+    if (bytes == 0) return NBX_ERR_ARG;
+    if (cudaHostAlloc(out, bytes, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return NBX_ERR_OOM;
+    }
+    return NBX_OK;
+}
+
+void nbx_host_free(void* p) {
+    if (p) cudaFreeHost(p);
+}
+
 int nbx_push_staged(nbx_ctx* ctx, uint64_t* accepted) {
     if (!ctx) return NBX_ERR_ARG;
     if (accepted) *accepted = 0;
@@ -843,8 +854,7 @@ int nbx_run(nbx_ctx* ctx) {
         a.bse_count = ctx->bse_count.p;
         a.n_tags = ctx->n_tags;
         a.counters = ctx->counters.p;
-        a.rec_a = ctx->rec_a.p;
-        a.rec_b = ctx->rec_b.p;
+        a.rec = ctx->rec.p;
         a.rec_count = ctx->rec_count.p;
         a.rec_capacity = uint32_t(std::min<uint64_t>(ctx->rec_cap, 0xFFFFFFF0ull));
         a.hist = ctx->hist.p;
@@ -1010,35 +1020,19 @@ int nbx_flush_detected(nbx_ctx* ctx, nbx_detected* out, uint64_t cap, uint64_t* 
     if (!ctx || !n || (cap && !out)) return NBX_ERR_ARG;
     return guarded(ctx, [&] {
         *n = 0;
-        if (!ctx->rec_a.p) return NBX_OK;
+        if (!ctx->rec.p) return NBX_OK;
         uint32_t cnt = 0;
         to_host(ctx, &cnt, ctx->rec_count.p, 4, "D2H");
         const uint64_t have = std::min<uint64_t>(cnt, ctx->rec_cap);
-        const uint64_t take = std::min<uint64_t>(have, cap);
-        if (take) {
-            std::vector<float4> a(take), b(take);
-            to_host(ctx, a.data(), ctx->rec_a.p, 16 * take, "D2H");
-            to_host(ctx, b.data(), ctx->rec_b.p, 16 * take, "D2H");
-            for (uint64_t i = 0; i < take; ++i) {
-                out[i].pos[0] = a[i].x;
-                out[i].pos[1] = a[i].y;
-                out[i].pos[2] = a[i].z;
-                out[i].E = a[i].w;
-                out[i].dir[0] = b[i].x;
-                out[i].dir[1] = b[i].y;
-                out[i].dir[2] = b[i].z;
-                std::memcpy(&out[i].tag, &b[i].w, 4);
-            }
-        }
-        if (take < have) {
-            // keep the remainder at the front
-            const uint64_t rest = have - take;
-            on_device(ctx, ctx->rec_a.p, ctx->rec_a.p + take, 16 * rest, "D2D");
-            on_device(ctx, ctx->rec_b.p, ctx->rec_b.p + take, 16 * rest, "D2D");
-            const uint32_t r = uint32_t(rest);
-            to_device(ctx, ctx->rec_count.p, &r, 4, "H2D");
-        } else {
+        const uint64_t take = std::min<uint64_t>(have - std::min(ctx->rec_read, have), cap);
+        // the device already holds the records in the caller's layout: one copy
+        static_assert(sizeof(nbx_detected) == 2 * sizeof(float4), "record layout");
+        to_host(ctx, out, ctx->rec.p + 2 * ctx->rec_read, sizeof(nbx_detected) * take, "D2H");
+        ctx->rec_read += take;
+        if (ctx->rec_read >= have) {
+            // everything read: the next records start at the front again
             zero(ctx, ctx->rec_count.p, 4, "memset");
+            ctx->rec_read = 0;
         }
         *n = take;
         return NBX_OK;
@@ -1136,6 +1130,7 @@ int nbx_reset_tallies(nbx_ctx* ctx) {
         ck(cudaMemsetAsync(ctx->counters.p, 0, 8 * nbx::kNumCounters, ctx->stream), "memset");
         ck(cudaMemsetAsync(ctx->hist.p, 0, 8ull * kHistBins, ctx->stream), "memset");
         ck(cudaMemsetAsync(ctx->rec_count.p, 0, 4, ctx->stream), "memset");
+        ctx->rec_read = 0;
         if (ctx->spec_pixels)
             ck(cudaMemsetAsync(ctx->pix_spec.p, 0, sizeof(float) * ctx->spec_pixels * uint64_t(ctx->spec_bins),
                                ctx->stream), "memset");

@@ -565,11 +565,11 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                 const int bin = dev::floor_to_int(e.E * a.pix_inv_width);
                 if (px < a.n_pixels && bin >= 0 && bin < a.pix_bins) atomicAdd(a.pix_spec + size_t(px) * a.pix_bins + bin, wt);
             }
-            if (a.rec_a) {
+            if (a.rec) {
                 const uint32_t slot = atomicAdd(a.rec_count, 1u);
                 if (slot < a.rec_capacity) {
-                    a.rec_a[slot] = make_float4(e.px, e.py, e.pz, e.E);
-                    a.rec_b[slot] = make_float4(e.dx, e.dy, e.dz, __uint_as_float(e.tag));
+                    a.rec[2 * size_t(slot)] = make_float4(e.px, e.py, e.pz, e.dx);
+                    a.rec[2 * size_t(slot) + 1] = make_float4(e.dy, e.dz, e.E, __uint_as_float(e.tag));
                 } else {
                     atomicAdd(a.counters + kCntRecordsDropped, 1ull);
                 }

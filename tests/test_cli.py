@@ -2,8 +2,8 @@
 nebula_cpu_mt: same inputs (.tri, .pri, .mat), 36-byte detected records on
 stdout.
 
-* Primaries are streamed from the .pri file in --capacity batches, run by
-  --streams device contexts at once; every primary keeps its own random
+* Primaries are streamed from the .pri file in --capacity batches through
+  --streams pipelines (device contexts); every primary keeps its own random
   stream, so the detected records depend on neither (byte-identical record
   sets).
 * Against the reference's own cpu_mt_main program (oracle/_ref, Kieft and
