@@ -73,6 +73,16 @@ constexpr int kMinWeightExp = -4;   // at least 1/16 (a chain of splits)
 // triangle): kWeightTag | uint8(wexp); no real triangle index has these bits.
 constexpr uint32_t kWeightTag = 0xFFFFFE00u;
 
+// Words per thread of the transport kernel's dynamic shared memory: the leaf
+// cache, then the event counters.  Counter slots 0-3 are indexed by the event
+// type (dev::kEvNone .. dev::kEvBoundary; slot 0 is never read).
+constexpr int kLeafCacheWords = 13;
+constexpr int kSlotSteps = 4, kSlotSecondaries = 5, kSlotDetectedSE = 6, kSlotDetectedBSE = 7, kSlotTerminated = 8,
+              kSlotPopped = 9;
+constexpr int kCounterSlots = 10;
+static_assert(dev::kEvNone == 0 && dev::kEvInelastic == 1 && dev::kEvElastic == 2 && dev::kEvBoundary == 3,
+              "event types index counter slots 0-3");
+
 struct LearnedSmem {
     mlp::Weights w;
     __nv_bfloat16 xs[8 * 32 * mlp::kIn];   // one 32 x 16 feature tile per warp
@@ -245,14 +255,22 @@ __device__ __forceinline__ float table_importance(const TransportArgs& a, const 
 // scattering event).
 template <int MinBlocks, int Mode, bool Penn>
 __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transport_kernel(const dev::Physics P, const TransportArgs a) {
-    // Leaf cache: 13 words per thread in dynamic shared memory sized by the
-    // launch (13 * 4 * blockDim.x bytes), so a 128-thread block does not hold
-    // a 256-thread allocation and the rest of the SM's L1 stays with the
-    // cascade stacks.
+    // Dynamic shared memory sized by the launch (transport_smem_bytes), per
+    // thread and strided by the block size: the leaf cache (13 words), then
+    // the thread's event counters (kCounterSlots words), so a 128-thread
+    // block does not hold a 256-thread allocation and the rest of the SM's
+    // L1 stays with the cascade stacks.  The counters live there rather than
+    // in registers, which the octree walk needs: a shared-memory atomic add
+    // per event costs one instruction, as a register increment does.
     extern __shared__ float leaf_cache[];
     const dev::LeafCache cache{leaf_cache + threadIdx.x, int(blockDim.x)};
     cache.f(0) = 0.0f;   // location 0: empty
     cache.f(1) = 0.0f;
+    uint32_t* const cnt = reinterpret_cast<uint32_t*>(leaf_cache + kLeafCacheWords * blockDim.x) + threadIdx.x;
+    const int cs = int(blockDim.x);
+#pragma unroll
+    for (int k = 0; k < kCounterSlots; ++k) cnt[k * cs] = 0u;
+    auto bump = [&](int slot) { atomicAdd(cnt + slot * cs, 1u); };
     constexpr bool kExtra = (Mode == kModeSample);
     constexpr bool kNet = (Mode == kModeLearned);                   // tensor-core inference at birth
     constexpr bool kW = (Mode == kModeLearned || Mode == kModeWeighted);   // weighted electrons
@@ -290,10 +308,10 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
     uint32_t probe = 0;   // ranges this thread has found used up (range_cursor)
     uint32_t carry_hit = 0;
     // Per-thread tallies in 32 bits (a thread would need 2^32 steps in one
-    // launch to wrap); rare ones (dropped records, queue overflow) go straight
-    // to the global counters.
-    uint32_t c_steps = 0, c_el = 0, c_inel = 0, c_bd = 0, c_se = 0, c_dse = 0, c_dbse = 0, c_term = 0, c_pop = 0,
-             c_inf = 0, c_kill = 0, c_split = 0, c_smp = 0, c_dep = 0, c_dep_drop = 0;
+    // launch to wrap): the frequent ones in the shared-memory slots above,
+    // the weighted, sample and deposit modes' own in registers; rare ones
+    // (dropped records, queue overflow) go straight to the global counters.
+    uint32_t c_inf = 0, c_kill = 0, c_split = 0, c_smp = 0, c_dep = 0, c_dep_drop = 0;
     // Deposit mode: this thread's current chunk [dep_pos, dep_end) of the
     // record buffer, taken kDepositChunk records at a time with one atomic.
     unsigned long long dep_pos = 0, dep_end = 0;
@@ -375,7 +393,7 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                         ex.flags = 0;
                         carry_hit = 0;
                     }
-                    ++c_pop;
+                    bump(kSlotPopped);
                     alive = true;
                 }
             }
@@ -399,7 +417,7 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
 #pragma unroll
                     for (int k = 0; k < 6; ++k) a.sample_feat[size_t(slot) * 6 + k] = f[k];
                     ex.rec = int(slot);
-                    ex.c0 = c_steps;
+                    ex.c0 = cnt[kSlotSteps * cs];
                     ++c_smp;
                 }
             }
@@ -411,7 +429,7 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
         [[maybe_unused]] const float E_before = e.E;
         if (!kNet || alive) {
             st = dev::step<Penn>(P, e, &ev, &se, &has_se, cache);
-            ++c_steps;
+            bump(kSlotSteps);
         }
         // Learned mode: birth decision for every newborn secondary of the warp
         // (k > 0 roulette at survival 2^-k, -1 split, 0 keep; drop = lost the
@@ -483,20 +501,18 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
                 }
             }
         }
-        c_el += (ev == dev::kEvElastic);
-        c_inel += (ev == dev::kEvInelastic);
-        c_bd += (ev == dev::kEvBoundary);
+        bump(ev);   // slots 1-3 count the event types; slot 0 (no event) is not read
         if (has_se) {
             // an inelastic step never ends its electron: st == kAlive here
-            ++c_se;
+            bump(kSlotSecondaries);
             if (drop) {
                 ++c_kill;   // the secondary's sub-cascade is not simulated
             } else if (dev::ends_at_init(P, se)) {
                 // The secondary's first step would only terminate it (about a
                 // quarter of them start below the barrier): tally that step
                 // here instead of parking the parent for it.
-                ++c_steps;
-                ++c_term;
+                bump(kSlotSteps);
+                bump(kSlotTerminated);
             } else {
                 // the newborn's weight exponent: roulette survivors gain bk,
                 // both halves of a split lose one
@@ -536,19 +552,18 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
             if (!dev::ends_at_init(P, e)) continue;
             // The next init pass would only end the electron (energy below
             // the barrier, or it left the domain): tally that step now.
-            ++c_steps;
+            bump(kSlotSteps);
             st = dev::kTerminated;
         }
         alive = false;
         uint32_t hit = 0;
         if (st == dev::kTerminated) {
-            ++c_term;
+            bump(kSlotTerminated);
         } else {
             // detected
             const bool is_se = e.E < 50;
             hit = is_se ? 1u : 0u;
-            c_dse += is_se;
-            c_dbse += !is_se;
+            bump(is_se ? kSlotDetectedSE : kSlotDetectedBSE);
             [[maybe_unused]] const float wt = kW ? ldexpf(1.0f, wexp) : 1.0f;
             if (e.tag < a.n_tags) {
                 atomicAdd(is_se ? a.se_count + e.tag : a.bse_count + e.tag, 1u);
@@ -579,7 +594,7 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
             const uint32_t sub = (ex.flags | hit) & 1u;
             if (ex.rec >= 0) {
                 a.sample_label[ex.rec] = float(sub);
-                if (a.sample_cost) a.sample_cost[ex.rec] = float(c_steps - ex.c0);
+                if (a.sample_cost) a.sample_cost[ex.rec] = float(cnt[kSlotSteps * cs] - ex.c0);
             }
             carry_hit = sub;
         }
@@ -590,18 +605,18 @@ __global__ void __launch_bounds__(MinBlocks == 7 ? 128 : 256, MinBlocks) transpo
     }
     // Counters: one atomic per warp per counter.
     unsigned long long v[kNumCounters];
-    v[kCntSteps] = c_steps;
-    v[kCntElastic] = c_el;
-    v[kCntInelastic] = c_inel;
-    v[kCntBoundary] = c_bd;
-    v[kCntSecondaries] = c_se;
-    v[kCntDetected] = c_dse + c_dbse;
-    v[kCntDetectedSE] = c_dse;
-    v[kCntDetectedBSE] = c_dbse;
-    v[kCntTerminated] = c_term;
+    v[kCntSteps] = cnt[kSlotSteps * cs];
+    v[kCntElastic] = cnt[dev::kEvElastic * cs];
+    v[kCntInelastic] = cnt[dev::kEvInelastic * cs];
+    v[kCntBoundary] = cnt[dev::kEvBoundary * cs];
+    v[kCntSecondaries] = cnt[kSlotSecondaries * cs];
+    v[kCntDetected] = cnt[kSlotDetectedSE * cs] + cnt[kSlotDetectedBSE * cs];
+    v[kCntDetectedSE] = cnt[kSlotDetectedSE * cs];
+    v[kCntDetectedBSE] = cnt[kSlotDetectedBSE * cs];
+    v[kCntTerminated] = cnt[kSlotTerminated * cs];
     v[kCntRecordsDropped] = 0;
     v[kCntOverflow] = 0;
-    v[kCntPopped] = c_pop;
+    v[kCntPopped] = cnt[kSlotPopped * cs];
     v[kCntInferences] = c_inf;
     v[kCntRouletteKilled] = c_kill;
     v[kCntSplit] = c_split;
@@ -810,8 +825,11 @@ int grid_for(uint64_t n, int block) {
 
 }  // namespace
 
-// Dynamic shared memory of transport_kernel: the per-thread leaf cache.
-static size_t leaf_cache_bytes(int block) { return size_t(13) * sizeof(float) * size_t(block); }
+// Dynamic shared memory of transport_kernel: per thread, the leaf cache and
+// the event counters.
+static size_t transport_smem_bytes(int block) {
+    return size_t(kLeafCacheWords + kCounterSlots) * sizeof(float) * size_t(block);
+}
 
 // Shared-memory carveout that just fits the blocks the registers allow on an
 // SM, so the rest of the unified L1 caches what the transport gathers
@@ -831,7 +849,7 @@ static void fit_carveout(Kernel kernel, int block) {
     for (const auto& d : done)
         if (d.first == key && d.second == tag) return;
     done.emplace_back(key, tag);
-    const size_t dyn = leaf_cache_bytes(block);
+    const size_t dyn = transport_smem_bytes(block);
     int before = 0, after = 0, smem_sm = 0;
     cudaFuncAttributes fa{};
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&before, kernel, block, dyn) != cudaSuccess ||
@@ -859,7 +877,7 @@ template <int Mode, bool Penn>
 static cudaError_t launch_mode(const dev::Physics& P, const TransportArgs& a, int grid, int block, int variant,
                                cudaStream_t s) {
     if (block <= 0 || block > (variant == 7 ? 128 : 256)) return cudaErrorInvalidValue;
-    const size_t sm = leaf_cache_bytes(block);
+    const size_t sm = transport_smem_bytes(block);
     switch (variant) {
     case 2: fit_carveout(transport_kernel<2, Mode, Penn>, block); break;
     case 4: fit_carveout(transport_kernel<4, Mode, Penn>, block); break;
@@ -895,7 +913,7 @@ template <int Mode>
 static int max_blocks_mode(int block, int variant) {
     int n = 0;
     cudaError_t e;
-    const size_t sm = leaf_cache_bytes(block);
+    const size_t sm = transport_smem_bytes(block);
     switch (variant) {
     // both models share launch bounds and shared memory, hence occupancy
     case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_kernel<2, Mode, false>, block, sm); break;
