@@ -119,3 +119,23 @@ def test_documented_caller_compiles_and_reports_nodev(tmp_path):
         # g.tri is absent in the temporary directory: the loader fails first
         r = subprocess.run([str(exe)], capture_output=True, text=True, cwd=str(tmp_path), timeout=60)
         assert r.returncode == 1
+
+
+def test_streaming_example_compiles_and_reports_nodev(tmp_path, inputs):
+    """The streaming C++ caller (examples/nbx_stream.cpp: page-locked
+    buffers, nbx_stage / nbx_push_staged) compiles and links; without a GPU
+    it loads its inputs and fails cleanly at nbx_create (exit status 1)."""
+    src = os.path.join(ROOT, "examples", "nbx_stream.cpp")
+    exe = tmp_path / "stream"
+    libdir = os.path.dirname(nb.LIB_PATH)
+    r = subprocess.run(["g++", "-std=c++17", "-I" + os.path.join(ROOT, "include"), src, "-L" + libdir, "-lnbx",
+                        "-Wl,-rpath," + libdir, "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    import torch
+    if not torch.cuda.is_available():
+        from nebula_b200 import formats, generators as g
+        pri = str(tmp_path / "p.pri")
+        formats.write_pri(pri, g.point_beam(100, 1000.0, pos=(0.0, 0.0, 1.0)))
+        r = subprocess.run([str(exe), inputs["cube_tri"], pri, inputs["si"]], capture_output=True, text=True,
+                           timeout=60)
+        assert r.returncode == 1 and "no CUDA device" in r.stderr

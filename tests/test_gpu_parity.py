@@ -547,3 +547,39 @@ def test_staged_push_equals_push(inputs):
     assert np.array_equal(se_a, se_b) and np.array_equal(bse_a, bse_b)
     for k in ("primaries_done", "steps", "events_elastic", "events_inelastic", "events_boundary", "detected"):
         assert sa[k] == sb[k], k
+
+
+def test_streaming_example_equals_one_push(inputs, tmp_path):
+    """examples/nbx_stream.cpp streams a .pri file through page-locked
+    buffers in uneven batches (nbx_stage before each run, nbx_push_staged
+    after it, the uid base set to each batch's first index): its SE and BSE
+    totals equal those of one push of the whole file through the Python
+    binding, on the same random streams."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = tmp_path / "stream"
+    libdir = os.path.dirname(nb.LIB_PATH)
+    r = subprocess.run(["g++", "-std=c++17", "-I" + os.path.join(root, "include"),
+                        os.path.join(root, "examples", "nbx_stream.cpp"), "-L" + libdir, "-lnbx",
+                        "-Wl,-rpath," + libdir, "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    recs = g.scan_beam(32, 32, 20, 500.0, origin=(-16.0, -16.0), seed=23)
+    pri = str(tmp_path / "scan.pri")
+    formats.write_pri(pri, recs)
+    r = subprocess.run([str(exe), inputs["grating_tri"], pri, inputs["si"], "7000"], capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = r.stdout.strip().splitlines()
+    assert len(lines) == 4 and lines[-1].startswith("total:")          # 3 batches of 20,480
+    n_tot, se_tot, bse_tot = [int(w) for w in lines[-1].replace(",", " ").split() if w.isdigit()]
+    assert n_tot == len(recs)
+    ctx = nb.setup(inputs["grating"], [inputs["si"]], device=0)
+    try:
+        ctx.set_uid_base(0)
+        ctx.push_records(recs)
+        ctx.run()
+        s = ctx.stats()
+    finally:
+        ctx.close()
+    assert (se_tot, bse_tot) == (s["detected_se"], s["detected_bse"])
+    assert se_tot > 1000
