@@ -198,6 +198,8 @@ int run_transport_noalloc(const dev::Physics& P, int grid, int block, int varian
                           uint64_t n_tags, uint64_t counts[4], const char** err);
 cudaError_t launch_fill_queue(Queue q, const float* particles, const uint32_t* tags, uint64_t uid_base,
                               uint64_t n, uint64_t offset, cudaStream_t s);
+// *p = v on the device, in stream order.
+cudaError_t launch_set_word(uint32_t* p, uint32_t v, cudaStream_t s);
 // The largest of n tags into *out (which the caller zeroes first).
 cudaError_t launch_max_tag(const uint32_t* tags, uint64_t n, uint32_t* out, cudaStream_t s);
 

@@ -522,7 +522,7 @@ int nbx_create(nbx_ctx** out, const nbx_config* cfg) {
         zero(ctx, ctx->counters.p, sizeof(unsigned long long) * nbx::kNumCounters, "memset");
         ctx->hist.alloc(kHistBins);
         zero(ctx, ctx->hist.p, sizeof(unsigned long long) * kHistBins, "memset");
-        ctx->ctl.alloc(2 * kMaxGenerations + 2);
+        ctx->ctl.alloc(2 * kMaxGenerations + 4);   // + the overflow snapshot (8-byte aligned)
         ctx->rec_count.alloc(1);
         zero(ctx, ctx->rec_count.p, 4, "memset");
         ctx->block = c.block_size > 0 ? c.block_size : 256;
@@ -830,12 +830,15 @@ int nbx_run(nbx_ctx* ctx) {
         // Overflow-queue capacity (secondaries of cascades deeper than the
         // per-thread stack): explicit, else one per queued primary (at least
         // 1M), bounded by a quarter of the free device memory.
-        size_t free_b = 0, total_b = 0;
-        ck(cudaMemGetInfo(&free_b, &total_b), "meminfo");
         uint64_t want = ctx->cfg.capacity ? ctx->cfg.capacity : std::max<uint64_t>(1ull << 20, ctx->n_queued);
-        const uint64_t budget = (free_b / 4) / (2 * 48);
-        want = std::min<uint64_t>(want, std::max<uint64_t>(budget, 1ull << 16));
         want = std::min<uint64_t>(want, 0xFFFFFFF0ull);
+        if (ctx->qa.cap < want) {
+            // the memory budget only matters when the queues would grow
+            size_t free_b = 0, total_b = 0;
+            ck(cudaMemGetInfo(&free_b, &total_b), "meminfo");
+            const uint64_t budget = (free_b / 4) / (2 * 48);
+            want = std::min<uint64_t>(want, std::max<uint64_t>(budget, 1ull << 16));
+        }
         if (ctx->qa.cap < want) {
             ctx->qa.a.release(); ctx->qa.b.release(); ctx->qa.c.release(); ctx->qa.cap = 0;
             ctx->qb.a.release(); ctx->qb.b.release(); ctx->qb.c.release(); ctx->qb.cap = 0;
@@ -846,8 +849,15 @@ int nbx_run(nbx_ctx* ctx) {
         ctx->queue_capacity = cap;
         uint32_t* ctl = ctx->ctl.p;
         ck(cudaMemsetAsync(ctl, 0, sizeof(uint32_t) * (2 * kMaxGenerations + 2), ctx->stream), "memset");
-        const uint32_t nq = uint32_t(ctx->n_queued);
-        ck(cudaMemcpyAsync(ctl + 2 * kMaxGenerations, &nq, 4, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+        static_assert((2 * kMaxGenerations + 2) % 2 == 0, "overflow snapshot alignment");
+        // Nothing before the first launch waits on the host or on a copy
+        // engine: the queue length is set by a one-thread kernel (a small
+        // host-to-device copy could queue behind a staged batch's copy), and
+        // the overflow counter is snapshotted on the device.
+        ck(nbx::launch_set_word(ctl + 2 * kMaxGenerations, uint32_t(ctx->n_queued), ctx->stream), "set");
+        unsigned long long* const ovf_snapshot = reinterpret_cast<unsigned long long*>(ctl + 2 * kMaxGenerations + 2);
+        ck(cudaMemcpyAsync(ovf_snapshot, ctx->counters.p + nbx::kCntOverflow, 8, cudaMemcpyDeviceToDevice,
+                           ctx->stream), "D2D");
 
         nbx::TransportArgs a{};
         a.se_count = ctx->se_count.p;
@@ -935,10 +945,6 @@ int nbx_run(nbx_ctx* ctx) {
             a.n_ranges = uint32_t(ctx->sms);
         }
 
-        // electrons lost to a full overflow queue before this run (the
-        // counter is cumulative until nbx_reset_tallies)
-        unsigned long long ovf_before = 0;
-        to_host(ctx, &ovf_before, ctx->counters.p + nbx::kCntOverflow, 8, "D2H");
         ck(cudaEventRecord(ctx->ev0, ctx->stream), "event");
         int g = 0;
         bool done = false;
@@ -971,7 +977,10 @@ int nbx_run(nbx_ctx* ctx) {
         ctx->last_kernel_ms = ms;
         ctx->generations = uint64_t(g);
         ctx->n_queued = 0;
-        unsigned long long ovf = 0;
+        // electrons lost to a full overflow queue in this run (the counter is
+        // cumulative until nbx_reset_tallies)
+        unsigned long long ovf = 0, ovf_before = 0;
+        to_host(ctx, &ovf_before, ovf_snapshot, 8, "D2H");
         to_host(ctx, &ovf, ctx->counters.p + nbx::kCntOverflow, 8, "D2H");
         if (ovf > ovf_before) throw ApiError(NBX_ERR_CAPACITY, "secondary queue overflow: electrons lost");
         return NBX_OK;

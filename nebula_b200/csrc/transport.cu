@@ -804,6 +804,11 @@ __global__ void fill_queue_kernel(Queue q, const float* particles, const uint32_
     }
 }
 
+// One word set on the device: a run's queue length goes into its control
+// block this way rather than by a host-to-device copy, which could wait
+// behind a staged batch's copy on the same copy engine.
+__global__ void set_word_kernel(uint32_t* p, uint32_t v) { *p = v; }
+
 // Largest of n tags into *out (zeroed by the caller).
 __global__ void max_tag_kernel(const uint32_t* v, uint64_t n, uint32_t* out) {
     uint32_t m = 0;
@@ -1054,6 +1059,11 @@ cudaError_t launch_pixel_yields(const uint32_t* se, const uint32_t* bse, const f
     return cudaGetLastError();
 }
 
+cudaError_t launch_set_word(uint32_t* p, uint32_t v, cudaStream_t s) {
+    set_word_kernel<<<1, 1, 0, s>>>(p, v);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_max_tag(const uint32_t* tags, uint64_t n, uint32_t* out, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     max_tag_kernel<<<grid_for(n, 256), 256, 0, s>>>(tags, n, out);
@@ -1144,7 +1154,7 @@ int run_transport_noalloc(const dev::Physics& P, int grid, int block, int varian
         return cudaStreamSynchronize(s) == cudaSuccess ? 0 : fail("stream synchronisation failed");
     }
     const uint32_t n_prim = n;
-    if (cudaMemcpyAsync(ctl + 2 * kNoAllocGenerations, &n_prim, 4, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    if (launch_set_word(ctl + 2 * kNoAllocGenerations, n_prim, s) != cudaSuccess)
         return fail("writing the primary count failed");
     fill_queue_kernel<<<grid_for(n, 256), 256, 0, s>>>(prim, d_particles, d_tags, uid_base, n, 0);
     if (cudaGetLastError() != cudaSuccess) return fail("queue fill launch failed");
