@@ -39,6 +39,10 @@ struct Material {
     float phonon_loss, recoil_const;
     float fermi, band_gap;
     Table1D el_imfp, in_imfp;
+    // The two log-IMFP tables interleaved per interval, (in[i], in[i+1],
+    // el[i], el[i+1]), when both share one energy axis (else null): a step's
+    // two free-path lookups then take one index and one 16-byte gather.
+    const float4* imfp_pair;
     Table2D el_icdf, in_icdf, ion;
     Table3D q, ion3;
 };

@@ -272,6 +272,27 @@ nbx::dev::Table3D upload3d(nbx_ctx* ctx, const nbx_table3d& t) {
     return nbx::dev::Table3D{b->p, t.width, t.height, t.depth, t.x_min, t.x_step, t.y_min, t.y_step, t.z_min, t.z_step};
 }
 
+// The inelastic and elastic log-IMFP tables interleaved per interval,
+// (in[i], in[i+1], el[i], el[i+1]), when they share one axis (the same
+// point count and the same scale, bit for bit); null otherwise.
+const float4* upload_imfp_pair(nbx_ctx* ctx, const nbx_table1d& in, const nbx_table1d& el) {
+    if (in.n != el.n || in.n < 2 || std::memcmp(&in.x_min, &el.x_min, 4) != 0 ||
+        std::memcmp(&in.x_step, &el.x_step, 4) != 0)
+        return nullptr;
+    std::vector<float> v(4 * size_t(in.n - 1));
+    for (int i = 0; i + 1 < in.n; ++i) {
+        v[4 * size_t(i)] = in.data[i];
+        v[4 * size_t(i) + 1] = in.data[i + 1];
+        v[4 * size_t(i) + 2] = el.data[i];
+        v[4 * size_t(i) + 3] = el.data[i + 1];
+    }
+    auto* b = new DevBuf<float>();
+    ctx->tables.push_back(b);
+    b->alloc(v.size());
+    to_device(ctx, b->p, v.data(), sizeof(float) * v.size(), "table upload");
+    return reinterpret_cast<const float4*>(b->p);
+}
+
 void ensure_tags(nbx_ctx* ctx, uint64_t n_tags) {
     if (n_tags <= ctx->n_tags) return;
     DevBuf<uint32_t> s, b;
@@ -641,6 +662,7 @@ int nbx_add_material(nbx_ctx* ctx, const nbx_material* m) {
             d.in_icdf = upload2d(ctx, m->inelastic_icdf);
             d.ion = upload2d(ctx, m->ionisation);
         }
+        d.imfp_pair = upload_imfp_pair(ctx, ctx->phys.penn ? m->penn_imfp : m->inelastic_imfp, m->elastic_imfp);
         ctx->phys.mat[ctx->n_mat++] = d;
         ctx->phys.n_mat = ctx->n_mat;
         // cpu_material_manager::get_max_energy (core/cpu_material_manager.inl:43-55)

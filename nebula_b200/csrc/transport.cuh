@@ -684,6 +684,25 @@ __device__ __forceinline__ int boundary(const Physics& P, Electron& e, float u) 
     return kAlive;
 }
 
+// A step's two log-IMFP lookups (table_1D::get, common/util/table_1D.inl:
+// 66-80): from the interleaved pair table when both tables share one axis --
+// the same index, fraction and lerps as two table1d_get calls, so the same
+// values -- else one table1d_get each.
+__device__ __forceinline__ void imfp_pair_get(const Material& m, float logE, float& in_v, float& el_v) {
+    if (m.imfp_pair) {
+        const Table1D& t = m.in_imfp;
+        const float xi = (logE - t.x_min) * t.x_step;
+        const int lo = clampi(floor_to_int(xi), 0, t.n - 2);
+        const float4 v = __ldg(m.imfp_pair + lo);
+        const float f = xi - float(lo);
+        in_v = (1 - f) * v.x + f * v.y;
+        el_v = (1 - f) * v.z + f * v.w;
+    } else {
+        in_v = table1d_get(m.in_imfp, logE);
+        el_v = table1d_get(m.el_imfp, logE);
+    }
+}
+
 // The init pass's termination test (drivers/cpu/cpu_driver.inl:73-92): outside
 // the simulation domain, or inside a material with an energy outside
 // [barrier + min_energy, barrier + max_energy].  A step that ends here draws no
@@ -729,8 +748,10 @@ __device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, E
         // Mean free path exp(-log imfp) rather than 1 / exp(log imfp): the
         // same exponential sampling (scatter_list.h:106-132, random.h
         // exponential) without a division per mechanism.
+        float in_lg, el_lg;
+        imfp_pair_get(m, logE, in_lg, el_lg);
         {
-            const float mfp = __expf(-table1d_get(m.in_imfp, logE));
+            const float mfp = __expf(-in_lg);
             const float path = fmaxf(-mfp * __logf(u01(r0.x)), 0.0f);
             if (path < dist) {
                 type = 1;
@@ -738,7 +759,7 @@ __device__ __forceinline__ int step(const Physics& P, Electron& e, int* event, E
             }
         }
         {
-            const float mfp = __expf(-table1d_get(m.el_imfp, logE));
+            const float mfp = __expf(-el_lg);
             const float path = fmaxf(-mfp * __logf(u01(r0.y)), 0.0f);
             if (path < dist) {
                 type = 2;
