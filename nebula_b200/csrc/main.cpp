@@ -134,12 +134,6 @@ struct PriWarnings {
             dir0 += !(std::fabs(r.dir[0]) > eps || std::fabs(r.dir[1]) > eps || std::fabs(r.dir[2]) > eps);
         }
     }
-    void merge(const PriWarnings& o) {
-        outside += o.outside;
-        low += o.low;
-        high += o.high;
-        dir0 += o.dir0;
-    }
     void print() const {
         if (outside) std::fprintf(stderr, "WARNING: %llu primary electrons starting outside geometry.\n", (unsigned long long)outside);
         if (low) std::fprintf(stderr, "WARNING: %llu primary electrons starting with low kinetic energy.\n", (unsigned long long)low);
@@ -435,55 +429,50 @@ int main(int argc, char** argv) {
     static_assert(sizeof(DepositRecord) == 28, "deposit record layout");
     const uint64_t dep_capacity = uint64_t(1) << 27;   // nbx_config default
 
-    // Energy-deposit mode: one worker claims the next batch of the file, reads
-    // it with a positional read, runs it and writes its records, then sizes
-    // the next batch from the deposits per primary seen so far.  In every
-    // mode a batch's primaries keep their global index as the uid of their
-    // random streams, so the records depend neither on the batch size nor on
-    // the number of contexts; only their order in the output does, as with
-    // the reference's worker threads.  Tags are batch-relative.
+    // Energy-deposit mode: one context runs the batches in turn on this
+    // thread.  It reads each batch with a positional read, runs it, writes
+    // its records, then sizes the next batch from the deposits per primary
+    // seen so far.  In every mode a batch's primaries keep their global index
+    // as the uid of their random streams, so the records depend neither on
+    // the batch size nor on the number of contexts; only their order in the
+    // output does, as with the reference's worker threads.  Tags are
+    // batch-relative.
     struct Batch {
         uint64_t first = 0, n = 0;
         std::vector<nbx_record> pri;
         std::vector<nbx_particle> part;
         std::vector<uint32_t> tags;
     };
-    std::mutex in_mu, out_mu;
-    uint64_t next_first = 0, done = 0;
+    std::mutex fail_mu;
+    uint64_t done = 0;
     uint64_t batch = std::max<uint64_t>(capacity, 1);
     if (energy_deposit) batch = std::min<uint64_t>(batch, std::max<uint32_t>(prescan, 1));
     int failed_rc = NBX_OK;
     std::string failed_what;
     nbx_ctx* failed_ctx = nullptr;
     auto fail_with = [&](nbx_ctx* c, int code, const char* what) {
-        std::lock_guard<std::mutex> lk(in_mu);
+        std::lock_guard<std::mutex> lk(fail_mu);
         if (failed_rc == NBX_OK) {
             failed_rc = code;
             failed_what = what;
             failed_ctx = c;
         }
     };
-    std::vector<PriWarnings> warns(ctxs.size(), PriWarnings{oct, max_energy});
-    auto worker = [&](nbx_ctx* c, PriWarnings& my_warn) {
+    auto deposit_loop = [&](nbx_ctx* c) {
         Batch b;
         std::vector<nbx_detected> det(1u << 20);
-        std::vector<nbx_deposit> dep(energy_deposit ? (1u << 20) : 0);
+        std::vector<nbx_deposit> dep(1u << 20);
         std::vector<nbx_record> out;
         std::vector<DepositRecord> dep_out;
-        for (;;) {
-            {
-                std::lock_guard<std::mutex> lk(in_mu);
-                if (failed_rc != NBX_OK || next_first >= n_pri) return;
-                b.first = next_first;
-                b.n = std::min(batch, n_pri - next_first);
-                next_first += b.n;
-            }
+        for (uint64_t first = 0; first < n_pri; first += b.n) {
+            b.first = first;
+            b.n = std::min(batch, n_pri - first);
             b.pri.resize(b.n);
             if (!src.read(b.first, b.n, b.pri.data())) {
                 std::fprintf(stderr, "Error: could not read primary electrons!\n");
                 return fail_with(c, NBX_ERR_FORMAT, "primaries");
             }
-            if (!sort_primaries) my_warn.add(b.pri.data(), b.n);
+            if (!sort_primaries) warn.add(b.pri.data(), b.n);
             b.part.resize(b.n);
             b.tags.resize(b.n);
             for (uint64_t i = 0; i < b.n; ++i) {
@@ -514,35 +503,30 @@ int main(int argc, char** argv) {
                 }
             }
             dep_out.clear();
-            if (energy_deposit) {
-                for (;;) {
-                    uint64_t got = 0;
-                    if ((r = nbx_flush_deposits(c, dep.data(), dep.size(), &got)) != NBX_OK)
-                        return fail_with(c, r, "flush deposits");
-                    if (got == 0) break;
-                    const size_t base = dep_out.size();
-                    dep_out.resize(base + got);
-                    for (uint64_t i = 0; i < got; ++i) {
-                        const nbx_deposit& d = dep[i];
-                        const nbx_record& rec = b.pri[d.tag];
-                        dep_out[base + i] = {d.pos[0], d.pos[1], d.pos[2], d.E, d.dE, rec.px, rec.py};
-                    }
+            for (;;) {
+                uint64_t got = 0;
+                if ((r = nbx_flush_deposits(c, dep.data(), dep.size(), &got)) != NBX_OK)
+                    return fail_with(c, r, "flush deposits");
+                if (got == 0) break;
+                const size_t base = dep_out.size();
+                dep_out.resize(base + got);
+                for (uint64_t i = 0; i < got; ++i) {
+                    const nbx_deposit& d = dep[i];
+                    const nbx_record& rec = b.pri[d.tag];
+                    dep_out[base + i] = {d.pos[0], d.pos[1], d.pos[2], d.E, d.dE, rec.px, rec.py};
                 }
-                nbx_stats st;
-                nbx_get_stats(c, &st);
-                if (st.deposits_dropped) {
-                    std::fprintf(stderr, "\nError: %llu energy deposits did not fit the device buffer; lower --batch-factor\n",
-                                 (unsigned long long)st.deposits_dropped);
-                    return fail_with(c, NBX_ERR_CAPACITY, "deposit buffer");
-                }
-                // size the next batches from the deposits per primary seen so
-                // far (one context in this mode, so batches run in turn)
-                const double per_primary = double(dep_out.size()) / double(b.n);
-                const double fit = batch_factor * double(dep_capacity) / std::max(per_primary, 1.0);
-                std::lock_guard<std::mutex> lk(in_mu);
-                batch = std::max<uint64_t>(1, std::min<uint64_t>(std::max<uint64_t>(capacity, 1), uint64_t(fit)));
             }
-            std::lock_guard<std::mutex> lk(out_mu);
+            nbx_stats st;
+            nbx_get_stats(c, &st);
+            if (st.deposits_dropped) {
+                std::fprintf(stderr, "\nError: %llu energy deposits did not fit the device buffer; lower --batch-factor\n",
+                             (unsigned long long)st.deposits_dropped);
+                return fail_with(c, NBX_ERR_CAPACITY, "deposit buffer");
+            }
+            // size the next batches from the deposits per primary seen so far
+            const double per_primary = double(dep_out.size()) / double(b.n);
+            const double fit = batch_factor * double(dep_capacity) / std::max(per_primary, 1.0);
+            batch = std::max<uint64_t>(1, std::min<uint64_t>(std::max<uint64_t>(capacity, 1), uint64_t(fit)));
             if (!out.empty()) std::fwrite(out.data(), sizeof(nbx_record), out.size(), detect_out);
             if (!dep_out.empty()) std::fwrite(dep_out.data(), sizeof(DepositRecord), dep_out.size(), deposit_out);
             done += b.n;
@@ -691,8 +675,7 @@ int main(int argc, char** argv) {
 
     timer.start();
     if (energy_deposit) {
-        worker(ctxs[0], warns[0]);
-        warn.merge(warns[0]);
+        deposit_loop(ctxs[0]);
     } else {
         for (HostBatch& b : host_batches) free_batches.push(&b);
         std::thread out_thread(writer);
