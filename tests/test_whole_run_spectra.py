@@ -7,7 +7,7 @@ the exit polar-angle spectrum of the detected electrons.
   Kieft inelastic model and the stock full Penn model.
 * Rough slab (526,334 triangles) with the mixed {0.3, 1, 3, 5} keV beam: a
   32 x 32-pixel subsample of the 512 x 512 scan (20,480 primaries), checked
-  per beam energy.
+  per beam energy, Kieft and full Penn.
 
 Each detected record carries the electron's position, direction and energy
 (cpu_mt_main.cpp:182-189 on the CPU; the GPU's nbx_flush_detected); the
@@ -195,12 +195,17 @@ def rough_full(tmp_path_factory):
     return tris, p
 
 
-def test_rough_slab_mixed_beam_per_energy(inputs, oracle_built, tmp_path, rough_full):
+@pytest.mark.parametrize("model", ["kieft", "penn"])
+def test_rough_slab_mixed_beam_per_energy(inputs, oracle_built, tmp_path, rough_full, model):
     """Rough slab with the mixed-energy beam: every 16th pixel row and column
     of the 512 x 512 scan (32 x 32 pixels x 20 primaries, energies drawn from
-    {300, 1000, 3000, 5000} eV).  Per-pixel SE/BSE chi-square over the 1,024
-    pixels, and for each beam energy: SE and BSE yields, exit-energy and
-    exit-angle spectra; events per primary over the whole sample."""
+    {300, 1000, 3000, 5000} eV), Kieft model and the stock full Penn model.
+    Per-pixel SE/BSE chi-square over the 1,024 pixels, and for each beam
+    energy: SE and BSE yields, exit-energy and exit-angle spectra; events per
+    primary over the whole sample."""
+    penn = model == "penn"
+    if penn and not oracle.have_ref(penn=True):
+        pytest.skip("reference full Penn build unavailable")
     tris, tri_path = rough_full
     w = g.SCANS["rough"]
     recs = g.scan_beam(w["nx"], w["ny"], w["per_pixel"], w["energy"], spacing=w["spacing"], origin=w["origin"],
@@ -208,19 +213,20 @@ def test_rough_slab_mixed_beam_per_energy(inputs, oracle_built, tmp_path, rough_
     recs = recs[recs["px"] % 16 == 0]
     n = len(recs)
     assert n == 32 * 32 * 20
-    gpu, ref = _run_both(tris, tri_path, [inputs["si"]], recs, tmp_path, gpu_seed=103, ref_seed=11)
+    gpu, ref = _run_both(tris, tri_path, [inputs["si"]], recs, tmp_path, gpu_seed=103, ref_seed=11, penn=penn)
     pixel = (recs["py"].astype(np.int64) // 16) * 32 + recs["px"] // 16
     energy = recs["E"]
     for key in ("se", "bse"):
         chi2, dof = _pixel_chi2(gpu[key], ref[key], pixel, 1024, strata=energy)
-        assert _chi2_ok(chi2, dof), (key, "pixels", chi2, dof)
+        assert _chi2_ok(chi2, dof), (model, key, "pixels", chi2, dof)
     gpu_tag_E = energy[gpu["det"]["tag"]]
     ref_tag_E = energy[ref["det"]["px"]]
     for e0 in w["energies"]:
         sel = energy == np.float32(e0)
         assert sel.sum() > 4000
         for key in ("se", "bse"):
-            assert abs(_z(gpu[key][sel], ref[key][sel])) < 3, (e0, key, gpu[key][sel].mean(), ref[key][sel].mean())
+            assert abs(_z(gpu[key][sel], ref[key][sel])) < 3, (model, e0, key, gpu[key][sel].mean(),
+                                                               ref[key][sel].mean())
         _check_spectra(gpu["det"][gpu_tag_E == np.float32(e0)], ref["det"][ref_tag_E == np.float32(e0)], e0,
-                       "%g eV" % e0)
+                       "%s %g eV" % (model, e0))
     assert abs(gpu["ev"] - ref["ev"]) / ref["ev"] < 0.05, (gpu["ev"], ref["ev"])
