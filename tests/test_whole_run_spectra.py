@@ -8,6 +8,8 @@ the exit polar-angle spectrum of the detected electrons.
 * Rough slab (526,334 triangles) with the mixed {0.3, 1, 3, 5} keV beam: a
   32 x 32-pixel subsample of the 512 x 512 scan (20,480 primaries), checked
   per beam energy, Kieft and full Penn.
+* Contact holes (three materials): a 16 x 16-pixel patch over the middle
+  hole of the 3 x 3 array at 1 keV (20,480 primaries), Kieft and full Penn.
 
 Each detected record carries the electron's position, direction and energy
 (cpu_mt_main.cpp:182-189 on the CPU; the GPU's nbx_flush_detected); the
@@ -229,4 +231,30 @@ def test_rough_slab_mixed_beam_per_energy(inputs, oracle_built, tmp_path, rough_
                                                                ref[key][sel].mean())
         _check_spectra(gpu["det"][gpu_tag_E == np.float32(e0)], ref["det"][ref_tag_E == np.float32(e0)], e0,
                        "%s %g eV" % (model, e0))
+    assert abs(gpu["ev"] - ref["ev"]) / ref["ev"] < 0.05, (gpu["ev"], ref["ev"])
+
+
+@pytest.mark.parametrize("model", ["kieft", "penn"])
+def test_contact_holes_patch_yields_and_spectra(inputs, oracle_built, tmp_path, model):
+    """Three materials (SiO2-like film, W-like plugs, Si-like substrate) on
+    the 3 x 3 contact-hole array: a 16 x 16-pixel patch at 5 nm spacing over
+    the middle hole (walls, floor and the film around it), 80 primaries per
+    pixel at 1 keV, Kieft and full Penn.  Per-pixel SE/BSE chi-square over
+    the 256 pixels, total yields, exit-energy and exit-angle spectra, events
+    per primary."""
+    penn = model == "penn"
+    if penn and not oracle.have_ref(penn=True):
+        pytest.skip("reference full Penn build unavailable")
+    recs = g.scan_beam(16, 16, 80, 1000.0, spacing=5.0, origin=(-37.5, -37.5), z_start=10.0, seed=47)
+    n = len(recs)
+    assert n == 16 * 16 * 80
+    mats = [inputs["sio2"], inputs["w"], inputs["si"]]
+    gpu, ref = _run_both(inputs["holes"], inputs["holes_tri"], mats, recs, tmp_path, gpu_seed=107, ref_seed=13,
+                         penn=penn)
+    pixel = recs["py"].astype(np.int64) * 16 + recs["px"]
+    for key in ("se", "bse"):
+        chi2, dof = _pixel_chi2(gpu[key], ref[key], pixel, 256)
+        assert _chi2_ok(chi2, dof), (model, key, "pixels", chi2, dof)
+        assert abs(_z(gpu[key], ref[key])) < 3, (model, key, gpu[key].mean(), ref[key].mean())
+    _check_spectra(gpu["det"], ref["det"], 1000.0, "contact holes " + model)
     assert abs(gpu["ev"] - ref["ev"]) / ref["ev"] < 0.05, (gpu["ev"], ref["ev"])
