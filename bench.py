@@ -64,7 +64,9 @@ WORKLOADS = {
     "grating": dict(rows=256, cpu_sample=409600, ref_sample=102400, desc=WORKLOAD,
                     # config 4 as written: weight window 0.05, splitting above 0.5
                     learned=dict(map_lo=(-180, -180, -60), map_hi=(180, 180, 60), cell=1.0, d_max=20.0,
-                                 train_per_pixel=2, train_on=("grating", "rough"), policy="window")),
+                                 train_per_pixel=2, train_on=("grating", "rough"), policy="window",
+                                 # survival floor 2^-3 (config 4 leaves it open): fewer heavy weights
+                                 max_roulette_exp=3)),
     "rough": dict(rows=512, cpu_sample=163840, ref_sample=40960,
                   learned=dict(map_lo=(-500, -500, -40), map_hi=(500, 500, 30), cell=2.0, d_max=10.0,
                                train_per_pixel=1, train_on=("grating", "rough"), policy="cost"),
@@ -470,9 +472,11 @@ def learned_fom(args, tris, mats, local, rank, prim, tags, plain, tmp, tune_samp
         # the cost-aware survival runs without splitting: a split adds
         # near-surface work, the most expensive steps of the scan
         split = 2.0 if policy == "cost" else args.split_threshold
-        # roulette floor: 2^-4 for the cost-aware survival (a deeper floor lets
-        # the rare heavy survivors dominate the variance), 2^-6 for the window
-        max_k = args.max_roulette_exp or (4 if policy == "cost" else 6)
+        # roulette floor (a deeper floor lets the rare heavy survivors dominate
+        # the variance): the flag, else the workload's own for its own policy,
+        # else 2^-4 for the cost-aware survival and 2^-6 for the window
+        max_k = args.max_roulette_exp or (L.get("max_roulette_exp") if policy == L["policy"] else None) or \
+            (4 if policy == "cost" else 6)
         ctx.set_mode("learned", rr_threshold=args.rr_threshold, split_threshold=split, max_roulette_exp=max_k)
         if args.birth_rr:
             ctx.set_birth_roulette(*[float(v) for v in args.birth_rr.split(",")])
@@ -568,8 +572,8 @@ def main():
     ap.add_argument("--split-threshold", type=float, default=0.5,
                     help="learned leg: importance above which a newborn secondary splits in two")
     ap.add_argument("--max-roulette-exp", type=int, default=0,
-                    help="learned leg: lowest roulette survival is 2^-this (0: 4 for the cost-aware survival, "
-                         "6 for the weight window)")
+                    help="learned leg: lowest roulette survival is 2^-this (0: the workload's default for its "
+                         "policy, else 4 for the cost-aware survival and 6 for the weight window)")
     ap.add_argument("--learned-eval", default="table", choices=["table", "fused"],
                     help="learned leg: network tabulated once over its inputs (table) or evaluated on the tensor "
                          "cores for every newborn (fused)")
