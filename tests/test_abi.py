@@ -139,3 +139,14 @@ def test_streaming_example_compiles_and_reports_nodev(tmp_path, inputs):
         r = subprocess.run([str(exe), inputs["cube_tri"], pri, inputs["si"]], capture_output=True, text=True,
                            timeout=60)
         assert r.returncode == 1 and "no CUDA device" in r.stderr
+
+
+def test_host_alloc_arguments():
+    """nbx_host_alloc refuses a null result pointer or a zero size
+    (NBX_ERR_ARG, result left null), and nbx_host_free(NULL) does nothing."""
+    L = nb.lib()
+    p = C.c_void_p(1)
+    assert L.nbx_host_alloc(C.c_uint64(0), C.byref(p)) == -1
+    assert not p.value
+    assert L.nbx_host_alloc(C.c_uint64(16), None) == -1
+    L.nbx_host_free(None)
