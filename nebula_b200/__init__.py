@@ -198,6 +198,34 @@ def device_count():
     return n.value
 
 
+class _HostBlock:
+    """Page-locked host memory from nbx_host_alloc, freed with the object."""
+
+    def __init__(self, nbytes):
+        self.p = C.c_void_p()
+        _check(lib().nbx_host_alloc(C.c_uint64(nbytes), C.byref(self.p)))
+
+    def __del__(self):
+        if getattr(self, "p", None) and self.p.value:
+            lib().nbx_host_free(self.p)
+            self.p = None
+
+
+def host_empty(shape, dtype=np.float32) -> np.ndarray:
+    """An uninitialised numpy array in page-locked host memory
+    (nbx_host_alloc), freed when the last view of it goes away.
+    Context.stage copies from such arrays asynchronously, so the copy
+    overlaps a run; from ordinary (pageable) arrays it works too, but the
+    call then waits for the copy.  Needs a CUDA device."""
+    dtype = np.dtype(dtype)
+    n = int(np.prod(shape, dtype=np.int64))
+    nbytes = max(n * dtype.itemsize, 1)
+    block = _HostBlock(nbytes)
+    raw = (C.c_char * nbytes).from_address(block.p.value)
+    raw._nbx_block = block          # the array's base keeps the allocation alive
+    return np.frombuffer(raw, dtype=dtype, count=n).reshape(shape)
+
+
 # ---------------------------------------------------------------------------
 # Host-side helpers
 # ---------------------------------------------------------------------------

@@ -583,3 +583,42 @@ def test_streaming_example_equals_one_push(inputs, tmp_path):
         ctx.close()
     assert (se_tot, bse_tot) == (s["detected_se"], s["detected_bse"])
     assert se_tot > 1000
+
+
+def test_host_empty_stages_like_push(inputs):
+    """Arrays from nebula_b200.host_empty (page-locked memory) stage a batch
+    that runs exactly as the same batch pushed from ordinary arrays (same
+    per-tag counts and event totals), and the memory goes away with the
+    arrays."""
+    import gc
+    recs = g.scan_beam(16, 16, 20, 500.0, origin=(-8.0, -8.0), seed=19)
+    n = len(recs)
+    prim = np.zeros((n, 7), np.float32)
+    prim[:, 0:3] = recs["pos"]
+    prim[:, 3:6] = recs["dir"]
+    prim[:, 6] = recs["E"]
+    tags = np.arange(n, dtype=np.uint32)
+    a = nb.setup(inputs["grating_small"], [inputs["si"]], device=0, seed=5)
+    a.set_tag_range(n)
+    a.push(prim, tags)
+    a.run()
+    sa = a.stats()
+    se_a, bse_a = a.tag_counts(0, n)
+    a.close()
+    b = nb.setup(inputs["grating_small"], [inputs["si"]], device=0, seed=5)
+    hp = nb.host_empty((n, 7), np.float32)
+    ht = nb.host_empty(n, np.uint32)
+    hp[:] = prim
+    ht[:] = tags
+    b.set_tag_range(n)
+    b.stage(hp, ht)
+    assert b.push_staged() == n
+    b.run()
+    sb = b.stats()
+    se_b, bse_b = b.tag_counts(0, n)
+    b.close()
+    assert np.array_equal(se_a, se_b) and np.array_equal(bse_a, bse_b)
+    for k in ("steps", "events_elastic", "events_inelastic", "events_boundary", "detected"):
+        assert sa[k] == sb[k], k
+    del hp, ht
+    gc.collect()
