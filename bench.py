@@ -604,15 +604,10 @@ def main():
     prim[:, 6] = recs["E"]
     tags = np.arange(n, dtype=np.uint32)
     pixel_of_tag = (recs["py"].astype(np.uint32) * NX + recs["px"].astype(np.uint32))
-    try:
-        import torch
-        pin_p = torch.empty((n, 7), dtype=torch.float32, pin_memory=True).numpy()
-        pin_t = torch.empty((n,), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
-        pinned = True
-    except Exception:
-        pin_p = np.empty((n, 7), np.float32)
-        pin_t = np.empty((n,), np.uint32)
-        pinned = False
+    # the library's own page-locked host buffers (nbx_host_alloc)
+    pin_p = nb.host_empty((n, 7), np.float32)
+    pin_t = nb.host_empty(n, np.uint32)
+    pinned = True
     pin_p[:] = prim
     pin_t[:] = tags
     ctx.set_tag_range(n)
@@ -696,11 +691,7 @@ def main():
     # tag -> pixel map is given once, like the geometry (setup, untimed).
     ctx.set_pixel_map(pixel_of_tag)
     n_pix = args.rows * NX
-    try:
-        import torch
-        pin_y = torch.empty((n_pix, 5), dtype=torch.float64, pin_memory=True).numpy()
-    except Exception:
-        pin_y = np.empty((n_pix, 5), np.float64)
+    pin_y = nb.host_empty((n_pix, 5), np.float64)
     # Pipelined like a scan that streams its frames: each step starts the copy
     # of the next step's primaries (nbx_stage, on the library's copy stream)
     # and runs its own while that copy is in flight, reads its per-pixel
