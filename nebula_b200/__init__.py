@@ -139,6 +139,8 @@ def lib():
         "nbx_set_tag_range": (C.c_int, [_vp, C.c_uint64]),
         "nbx_push": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.POINTER(C.c_uint64)]),
         "nbx_run": (C.c_int, [_vp]),
+        "nbx_host_alloc": (C.c_int, [C.c_uint64, C.POINTER(_vp)]),
+        "nbx_host_free": (None, [_vp]),
         "nbx_get_running_count": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
         "nbx_get_stats": (C.c_int, [_vp, C.POINTER(Stats)]),
         "nbx_flush_detected": (C.c_int, [_vp, _vp, C.c_uint64, C.POINTER(C.c_uint64)]),
@@ -202,12 +204,13 @@ class _HostBlock:
     """Page-locked host memory from nbx_host_alloc, freed with the object."""
 
     def __init__(self, nbytes):
+        self._L = lib()     # kept, so the free also works while the interpreter shuts down
         self.p = C.c_void_p()
-        _check(lib().nbx_host_alloc(C.c_uint64(nbytes), C.byref(self.p)))
+        _check(self._L.nbx_host_alloc(C.c_uint64(nbytes), C.byref(self.p)))
 
     def __del__(self):
         if getattr(self, "p", None) and self.p.value:
-            lib().nbx_host_free(self.p)
+            self._L.nbx_host_free(self.p)
             self.p = None
 
 
@@ -258,8 +261,9 @@ class HostOctree:
     def __init__(self, triangles: np.ndarray):
         tri = np.ascontiguousarray(triangles)
         assert tri.dtype.itemsize == 44
+        self._L = lib()     # kept, so the free also works while the interpreter shuts down
         self._p = C.POINTER(Octree)()
-        _check(lib().nbx_octree_build(_ptr(tri), len(tri), C.byref(self._p)))
+        _check(self._L.nbx_octree_build(_ptr(tri), len(tri), C.byref(self._p)))
         o = self._p.contents
         self.octree_data = np.ctypeslib.as_array(o.octree_data, (o.n_octree,)).copy()
         raw = C.string_at(o.triangles, 44 * o.n_triangles)
@@ -271,7 +275,7 @@ class HostOctree:
 
     def __del__(self):
         if getattr(self, "_p", None):
-            lib().nbx_octree_free(self._p)
+            self._L.nbx_octree_free(self._p)
             self._p = None
 
 
@@ -279,8 +283,9 @@ class HostMaterial:
     """A .mat file loaded and transformed by the library's host loader."""
 
     def __init__(self, path):
+        self._L = lib()     # kept, so the free also works while the interpreter shuts down
         self._p = C.POINTER(Material)()
-        _check(lib().nbx_material_load(str(path).encode(), C.byref(self._p)))
+        _check(self._L.nbx_material_load(str(path).encode(), C.byref(self._p)))
         m = self._p.contents
         self.barrier, self.fermi, self.band_gap = m.barrier, m.fermi, m.band_gap
         self.phonon_loss, self.recoil_const, self.max_energy = m.phonon_loss, m.recoil_const, m.max_energy
@@ -309,7 +314,7 @@ class HostMaterial:
 
     def __del__(self):
         if getattr(self, "_p", None):
-            lib().nbx_material_free(self._p)
+            self._L.nbx_material_free(self._p)
             self._p = None
 
 
